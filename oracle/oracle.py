@@ -1,0 +1,311 @@
+"""ctypes wrapper of the oracle library -- TEST INFRASTRUCTURE ONLY.
+
+The oracle is a CPU f64 restatement of the galaxy reference's LBVH Barnes-Hut
+path (solvers/src/lbvh.rs, solvers/src/direct_sum.rs, solvers/src/potential.rs,
+core/src/integrator.rs, core/src/diagnostics.rs) in ``lbvh_oracle.cpp``.  Only
+``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
+it, always as the checker or the timed CPU baseline; the product library
+``libgalaxy_b200.so`` never calls it.
+
+Parity pinning: the Morton bit-spreading is pinned by the reference's
+known-answer tests (solvers/src/lbvh.rs:691-726, in tests/golden/); the rest by
+the reference's invariant tests (solvers/tests/lbvh.rs:88-312). Bitwise identity
+with the Rust binary is unpinned beyond those (no Rust toolchain here).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liblbvh_oracle.so")
+_lib = None
+
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+
+
+def build() -> None:
+    """Compile the oracle with its Makefile (g++, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        sz, d, u64, i = C.c_size_t, C.c_double, C.c_uint64, C.c_int
+        sig = {
+            "or_expand10": (C.c_uint32, [C.c_uint32]),
+            "or_morton3": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32]),
+            "or_reference_morton": (i, [sz, _f64p, C.c_void_p, _u32p, C.c_void_p]),
+            "or_reference_sort": (None, [sz, _u32p, _u32p]),
+            "or_reference_karras": (i, [sz, _u32p, _u32p, _u32p, _u32p]),
+            "or_reference_aggregate": (i, [sz, _u32p, _u32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]),
+            "or_quadrupole": (i, [sz, _u32p, _u32p, _f64p, _f64p, _f64p]),
+            "or_lbvh_flat": (i, [sz, _f64p, _f64p, _f64p, _u32p, _u32p]),
+            "or_lbvh_accelerations": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i, C.c_void_p]),
+            "or_lbvh_accelerations_subset": (i, [sz, _f64p, _f64p, d, d, d, sz, _u32p, _f64p, i]),
+            "or_lbvh_accelerations_quad": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i]),
+            "or_direct_sum": (None, [sz, _f64p, _f64p, d, d, _f64p]),
+            "or_direct_sum_targets": (None, [sz, _f64p, _f64p, d, d, sz, _u32p, _f64p, i]),
+            "or_potential_serial": (d, [sz, _f64p, _f64p, d, d]),
+            "or_potential_parallel": (d, [sz, _f64p, _f64p, d, d, i]),
+            "or_diagnostics": (None, [sz, _f64p, _f64p, _f64p, _f64p]),
+            "or_kdk_lbvh": (i, [sz, _f64p, _f64p, _f64p, _f64p, C.POINTER(C.c_int), d, d, d, d, u64, i]),
+            "or_fixture_cluster": (None, [u64, sz, _f64p, _f64p, _f64p]),
+            "or_fixture_cloud": (None, [u64, sz, d, d, d, d, _f64p]),
+            "or_fixture_masses": (None, [u64, sz, _f64p]),
+            "or_fixture_random_codes": (None, [u64, sz, _u32p]),
+            "or_openmp_max_threads": (i, []),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _pos(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(-1, 3)
+
+
+def max_threads() -> int:
+    return int(lib().or_openmp_max_threads())
+
+
+# ---- Morton / sort / Karras / aggregate (solvers/src/lbvh.rs) -------------------------
+def expand10(v: int) -> int:
+    return int(lib().or_expand10(v))
+
+
+def morton3(x: int, y: int, z: int) -> int:
+    return int(lib().or_morton3(x, y, z))
+
+
+def reference_morton(pos):
+    """Returns (lanes [n,3] u32, codes [n] u32, bounds dict)."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    lanes = np.zeros((n, 3), np.uint32)
+    codes = np.zeros(n, np.uint32)
+    b = np.zeros(5, np.float64)
+    rc = lib().or_reference_morton(n, pos.reshape(-1), lanes.ctypes.data, codes, b.ctypes.data)
+    if rc != 0:
+        raise ValueError("reference_morton requires a non-empty system")
+    return lanes, codes, {"bmin": b[:3].copy(), "size": float(b[3]), "scale": float(b[4])}
+
+
+def reference_sort(codes) -> np.ndarray:
+    codes = np.ascontiguousarray(codes, dtype=np.uint32)
+    order = np.zeros(codes.shape[0], np.uint32)
+    lib().or_reference_sort(codes.shape[0], codes, order)
+    return order
+
+
+def reference_karras(sorted_codes):
+    """Returns (left [n-1], right [n-1], parent [2n-1]) in the unified index space."""
+    sc = np.ascontiguousarray(sorted_codes, dtype=np.uint32)
+    n = sc.shape[0]
+    if n == 0:
+        raise ValueError("reference_karras requires a non-empty system")
+    left = np.zeros(max(n - 1, 1), np.uint32)
+    right = np.zeros(max(n - 1, 1), np.uint32)
+    parent = np.zeros(2 * n - 1, np.uint32)
+    lib().or_reference_karras(n, sc, left, right, parent)
+    return left[: n - 1], right[: n - 1], parent
+
+
+def reference_aggregate(left, right, sorted_pos, sorted_mass):
+    """Returns dict of aabb_min, aabb_max, com ([2n-1,3]) and mass ([2n-1])."""
+    sp = _pos(sorted_pos)
+    n = sp.shape[0]
+    sm = np.ascontiguousarray(sorted_mass, dtype=np.float64)
+    l = np.ascontiguousarray(left if n > 1 else [0], dtype=np.uint32)
+    r = np.ascontiguousarray(right if n > 1 else [0], dtype=np.uint32)
+    t = 2 * n - 1
+    mn, mx, com = (np.zeros((t, 3)) for _ in range(3))
+    mass = np.zeros(t)
+    lib().or_reference_aggregate(n, l, r, sp.reshape(-1), sm, mn.reshape(-1), mx.reshape(-1), com.reshape(-1), mass)
+    return {"aabb_min": mn, "aabb_max": mx, "com": com, "mass": mass}
+
+
+def quadrupole(left, right, com, mass):
+    n = (np.asarray(mass).shape[0] + 1) // 2
+    l = np.ascontiguousarray(left if n > 1 else [0], dtype=np.uint32)
+    r = np.ascontiguousarray(right if n > 1 else [0], dtype=np.uint32)
+    q = np.zeros((2 * n - 1, 6))
+    lib().or_quadrupole(n, l, r, np.ascontiguousarray(com, np.float64).reshape(-1),
+                        np.ascontiguousarray(mass, np.float64), q.reshape(-1))
+    return q
+
+
+def lbvh_flat(pos, mass):
+    """The DFS skip-pointer flat form (reference_flatten): (node_f64 [2n-1,11], node_u32 [2n-1,3], leaf_bodies)."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    nf = np.zeros((2 * n - 1, 11))
+    nu = np.zeros((2 * n - 1, 3), np.uint32)
+    lb = np.zeros(n, np.uint32)
+    lib().or_lbvh_flat(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), nf.reshape(-1), nu.reshape(-1), lb)
+    return nf, nu, lb
+
+
+# ---- solvers ------------------------------------------------------------------------
+def lbvh_accelerations(pos, mass, g, softening, theta, threads: int = 1, stats: bool = False):
+    """Lbvh::accelerations (solvers/src/lbvh.rs:662-676). Returns acc [n,3] (and stats)."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3))
+    st = np.zeros(3, np.uint64)
+    lib().or_lbvh_accelerations(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g, softening, theta,
+                                acc.reshape(-1), threads, st.ctypes.data if stats else None)
+    if stats:
+        return acc, {"leaf": int(st[0]), "far": int(st[1]), "open": int(st[2])}
+    return acc
+
+
+def lbvh_accelerations_subset(pos, mass, g, softening, theta, targets, threads: int = 1):
+    pos = _pos(pos)
+    t = np.ascontiguousarray(targets, dtype=np.uint32)
+    acc = np.zeros((t.shape[0], 3))
+    lib().or_lbvh_accelerations_subset(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g,
+                                       softening, theta, t.shape[0], t, acc.reshape(-1), threads)
+    return acc
+
+
+def lbvh_accelerations_quad(pos, mass, g, softening, theta, threads: int = 1):
+    pos = _pos(pos)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3))
+    lib().or_lbvh_accelerations_quad(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g, softening, theta,
+                                     acc.reshape(-1), threads)
+    return acc
+
+
+def direct_sum(pos, mass, g, softening):
+    """DirectSum::accelerations (solvers/src/direct_sum.rs:25-45), Newton-3 pairing."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3))
+    lib().or_direct_sum(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g, softening, acc.reshape(-1))
+    return acc
+
+
+def direct_sum_targets(pos, mass, g, softening, targets, threads: int = 0):
+    pos = _pos(pos)
+    t = np.ascontiguousarray(targets, dtype=np.uint32)
+    acc = np.zeros((t.shape[0], 3))
+    lib().or_direct_sum_targets(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g, softening,
+                                t.shape[0], t, acc.reshape(-1), threads or max_threads())
+    return acc
+
+
+def potential_serial(pos, mass, g, softening) -> float:
+    pos = _pos(pos)
+    return float(lib().or_potential_serial(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g,
+                                           softening))
+
+
+def potential_parallel(pos, mass, g, softening, threads: int = 0) -> float:
+    pos = _pos(pos)
+    return float(lib().or_potential_parallel(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                                             g, softening, threads or max_threads()))
+
+
+def diagnostics(pos, vel, mass):
+    """core/src/diagnostics.rs: kinetic energy, momentum, angular momentum."""
+    pos, vel = _pos(pos), _pos(vel)
+    out = np.zeros(7)
+    lib().or_diagnostics(pos.shape[0], pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64), out)
+    return {"kinetic": float(out[0]), "momentum": out[1:4].copy(), "angular_momentum": out[4:7].copy()}
+
+
+class LeapfrogKdkLbvh:
+    """LeapfrogKdk (core/src/integrator.rs:38-78) driving the Lbvh solver, in place on f64 arrays."""
+
+    def __init__(self, g, softening, theta, threads: int = 1):
+        self.g, self.softening, self.theta, self.threads = g, softening, theta, threads
+        self.acc = None
+        self.primed = C.c_int(0)
+
+    def step_many(self, pos, vel, mass, dt, steps):
+        n = pos.shape[0]
+        if self.acc is None or self.acc.shape[0] != n:
+            self.acc = np.zeros((n, 3))
+            self.primed = C.c_int(0)
+        lib().or_kdk_lbvh(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                          self.acc.reshape(-1), C.byref(self.primed), self.g, self.softening, self.theta, dt, steps,
+                          self.threads)
+
+
+# ---- reference test fixtures ---------------------------------------------------------
+def fixture_cluster(seed: int, n: int):
+    """solvers/tests/lbvh.rs:27-44: (pos, vel, mass)."""
+    pos, vel, mass = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+    lib().or_fixture_cluster(seed, n, pos.reshape(-1), vel.reshape(-1), mass)
+    return pos, vel, mass
+
+
+def fixture_cloud(seed: int, n: int, r: float, center=(0.0, 0.0, 0.0)):
+    """gpu/tests/lbvh_sort.rs:25-37."""
+    pos = np.zeros((n, 3))
+    lib().or_fixture_cloud(seed, n, r, float(center[0]), float(center[1]), float(center[2]), pos.reshape(-1))
+    return pos
+
+
+def fixture_masses(seed: int, n: int):
+    """gpu/tests/lbvh_tree.rs:47-58."""
+    m = np.zeros(n)
+    lib().or_fixture_masses(seed, n, m)
+    return m
+
+
+def fixture_random_codes(seed: int, n: int):
+    """gpu/tests/lbvh_sort.rs:41-51."""
+    c = np.zeros(n, np.uint32)
+    lib().or_fixture_random_codes(seed, n, c)
+    return c
+
+
+def cluster_with_coincident_knot():
+    """solvers/tests/lbvh.rs:249-261: cluster(3, 60) plus 8 coincident particles."""
+    pos, _, mass = fixture_cluster(3, 60)
+    knot = np.tile([0.25, -0.1, 0.4], (8, 1))
+    kmass = np.array([0.5 + 0.05 * k for k in range(8)])
+    pos = np.vstack([pos, knot])
+    mass = np.concatenate([mass, kmass])
+    return pos, np.zeros_like(pos), mass
+
+
+# ---- error metrics (solvers/tests/lbvh.rs:54-82) ---------------------------------------
+def rms_accel(a) -> float:
+    a = np.asarray(a)
+    return max(float(np.sqrt(np.sum(a * a) / a.shape[0])), 1e-300)
+
+
+def rms_rel_err(approx, exact) -> float:
+    d = np.asarray(approx) - np.asarray(exact)
+    return float(np.sqrt(np.sum(d * d) / d.shape[0])) / rms_accel(exact)
+
+
+def worst_rel_err(approx, exact) -> float:
+    d = np.asarray(approx) - np.asarray(exact)
+    return float(np.max(np.sqrt(np.sum(d * d, axis=1)))) / rms_accel(exact)
+
+
+def per_particle_rel_err(approx, exact) -> np.ndarray:
+    """|a - a_ref| / |a_ref| per particle (the parity metric for median/p99)."""
+    approx, exact = np.asarray(approx), np.asarray(exact)
+    num = np.sqrt(np.sum((approx - exact) ** 2, axis=1))
+    den = np.maximum(np.sqrt(np.sum(exact * exact, axis=1)), 1e-300)
+    return num / den
