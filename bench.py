@@ -1,0 +1,325 @@
+"""Benchmark of the LBVH Barnes-Hut gravity step on B200.
+
+Default workload (one line of JSON on rank 0): the two-galaxy collision, 2 x 524,288
+particles (halo 60% / exponential disk 35% / Hernquist bulge 5% per galaxy, mass
+ratio 1:1, parabolic orbit, pericentre 4 Rd, disks inclined 30 and 60 degrees),
+eps = 0.02, theta = 0.5, dt = 5e-4, FP32 walk with FP64 positions/velocities. A step
+is one resident KDK step (kick + drift + bbox, Morton, 4 sort passes, build +
+aggregation, tree walk). The state plus tree (~330 MB) is larger than the 126 MB
+L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config collision|plummer|batched]
+
+Under torchrun each rank steps its own replica (a single system does not shard:
+replicas only) and value = all ranks' particle-steps / max-over-ranks device time.
+--impl reference times the reference algorithm's CPU implementation (the oracle's
+C++ restatement of Lbvh + LeapfrogKdk; the Rust reference cannot be built here) on
+the host cores with all threads, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at theta=0.5 (resident KDK step, plain single-system path)"
+N_PER_GALAXY = 524_288
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.lines, self.proc = device, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1, 0
+    import torch
+    import torch.distributed as dist
+
+    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    from datetime import timedelta
+
+    dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return dist, rank, ws, local
+
+
+def _max_over_ranks(dist, v: float, local: int) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist, local):
+    if dist is not None:
+        import torch
+
+        if torch.cuda.is_available():
+            dist.barrier(device_ids=[local])
+        else:
+            dist.barrier()
+
+
+def workload(config: str, seed: int):
+    import galaxy_b200 as gb
+
+    if config == "plummer":
+        return gb.ic.plummer(16_384, seed), dict(eps=0.01, theta=0.5, dt=1e-3, name="plummer-16384")
+    st = gb.ic.collision(2 * N_PER_GALAXY, seed, mass_ratio=1.0, pericentre=4.0, incl1_deg=30.0, incl2_deg=60.0)
+    return st, dict(eps=0.02, theta=0.5, dt=5e-4, name="collision-2x524288")
+
+
+# ---- algorithmic work per launch (bytes / flops) ----------------------------------------
+def algorithmic(n: int, counts: dict) -> dict:
+    # Per-stage compulsory bytes (inputs read once, outputs written once):
+    #   kick+drift+bbox: pos, vel, acc read (72 B) + pos, vel written (48 B)      = 120 N
+    #   Morton + histograms: pos read (24 B) + code written (4 B)                  =  28 N
+    #   onesweep pass: (key, index) read + written                                 =  16 N per pass
+    #   build: sorted codes + order (8 B) + gathered pos/mass (32 B) read; leaf64 +
+    #          leafA/B (64 B), kids/parent (16 B), agg64 (80 B), node records (64 B)
+    #          written; sibling aggregate read (80 B)                              = 344 N
+    #   walk: node records + leaves read once (96 B), target leaves (48 B), acc (24 B)
+    # Walk FLOPs: 20 per leaf term, 24 per far term (Kahan), 18 per opened node.
+    flops = 20 * counts["leaf"] + 24 * counts["far"] + 18 * counts["open"]
+    return {"kick_bbox": 120 * n, "morton": 28 * n, "sort_pass": 16 * n, "build": 344 * n, "walk_bytes": 168 * n,
+            "walk_flops": flops}
+
+
+def cpu_sample_step(st, params, threads: int, n_targets: int, rng) -> float:
+    """Seconds for one CPU step estimated from a bounded sample: the oracle's full tree
+    build plus the walk of n_targets random targets, scaled to all N targets."""
+    from oracle import oracle
+
+    n = len(st)
+    t0 = time.perf_counter()
+    oracle.lbvh_accelerations_subset(st.pos, st.mass, 1.0, params["eps"], params["theta"], np.zeros(1, np.uint32),
+                                     threads=threads)
+    t_build = time.perf_counter() - t0
+    tg = rng.choice(n, n_targets, replace=False).astype(np.uint32)
+    t0 = time.perf_counter()
+    oracle.lbvh_accelerations_subset(st.pos, st.mass, 1.0, params["eps"], params["theta"], tg, threads=threads)
+    t_walk = time.perf_counter() - t0 - t_build
+    return t_build + max(t_walk, 0.0) * n / n_targets
+
+
+def run_reference(args):
+    dist, rank, ws, local = _dist()
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    st, p = workload(args.config, 0)
+    n = len(st)
+    rng = np.random.default_rng(1)
+    n_targets = min(n, 16_384)
+    for _ in range(args.warmup):
+        cpu_sample_step(st, p, threads, min(n_targets, 1024), rng)
+    times = [cpu_sample_step(st, p, threads, n_targets, rng) for _ in range(args.steps)]
+    t_step = statistics.mean(times)
+    value = n / t_step
+    sample = (f"per step: full {n}-particle tree build + walk of {n_targets} random targets with {threads} "
+              f"threads, scaled to all targets (C++ restatement of the reference Lbvh; the Rust crate "
+              f"cannot be built here)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": p["name"], "particles": n, "theta": p["theta"], "eps": p["eps"], "dt": p["dt"]},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    dist, rank, ws, local = _dist()
+    import galaxy_b200 as gb
+
+    st, p = workload(args.config, rank)
+    n = len(st)
+    dt = p["dt"]
+    peaks = _peaks()
+
+    # --- headline: resident steps, CUDA-graph replay, device time (CUDA events) ---
+    r = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], device=local)
+    r.upload(st)
+    r.step_many(dt, args.warmup)
+    clocks = ClockSampler(local)
+    clocks.start()
+    _barrier(dist, local)
+    ms = r.step_many_timed(dt, args.steps)
+    _barrier(dist, local)
+    clk = clocks.stop()
+    ms_max = _max_over_ranks(dist, ms, local)
+    value = n * ws * args.steps / (ms_max / 1e3)
+
+    # --- e2e: the reference-facing ForceSolver path (LeapfrogKdk on host arrays) ---
+    pinned = gb.PinnedState.from_state(st)
+    h = gb.GpuLbvh(1.0, p["eps"], p["theta"], device=local)
+    primed = h.kdk_step_host(pinned, dt, primed=False)  # prime + one step (warm-up)
+    k_e2e = max(1, min(args.steps, 10))
+    _barrier(dist, local)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        primed = h.kdk_step_host(pinned, dt, primed=primed)
+    t_e2e = time.perf_counter() - t0
+    _barrier(dist, local)
+    t_e2e = _max_over_ranks(dist, t_e2e, local)
+    e2e = {"value": n * ws * k_e2e / t_e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
+           "d2h_bytes_per_step": 24 * n, "steps": k_e2e,
+           "path": "LeapfrogKdk on pinned host f64 arrays, gx_accelerations per step (upload pos+mass, download acc)"}
+    del pinned
+
+    # --- per-stage device times (eager launches with CUDA events on the handle's stream) ---
+    rs = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], device=local, stage_times=True)
+    rs.upload(st)
+    stage = {"ms_bbox_morton": 0.0, "ms_sort": 0.0, "ms_build": 0.0, "ms_walk": 0.0}
+    k_st = max(1, min(args.steps, 10))
+    rs.step(dt)
+    for _ in range(k_st):
+        rs.step(dt)
+        s = rs.stats()
+        for k in stage:
+            stage[k] += s[k] / k_st
+    counts_h = gb.GpuLbvh(1.0, p["eps"], p["theta"], device=local, stats=True)
+    counts_h.accelerations(st)
+    c = counts_h.stats()
+    counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"]}
+    alg = algorithmic(n, counts)
+    walk_s = stage["ms_walk"] / 1e3
+    sm_clock = (clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved = alg["walk_flops"] / walk_s / 1e12
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    sort_gbs = 4 * alg["sort_pass"] / (stage["ms_sort"] / 1e3) / 1e9
+    build_gbs = alg["build"] / (stage["ms_build"] / 1e3) / 1e9
+    mort_gbs = (alg["kick_bbox"] + alg["morton"]) / (stage["ms_bbox_morton"] / 1e3) / 1e9
+    roofline = {"kernel": "k_walk (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm "
+                               "(MEASURED_PEAKS.json has no FP32 figure); no tensor-core work in this path",
+                "flops_per_launch": alg["walk_flops"], "ms_per_launch": stage["ms_walk"],
+                "interactions_per_particle": (counts["leaf"] + counts["far"]) / n,
+                "hbm_stages": {
+                    "sort (4 onesweep passes)": {"achieved_gbs": sort_gbs, "frac": sort_gbs / hbm,
+                                                 "ms": stage["ms_sort"], "bytes": 4 * alg["sort_pass"]},
+                    "build + aggregation": {"achieved_gbs": build_gbs, "frac": build_gbs / hbm,
+                                            "ms": stage["ms_build"], "bytes": alg["build"]},
+                    "kick/drift/bbox + Morton": {"achieved_gbs": mort_gbs, "frac": mort_gbs / hbm,
+                                                 "ms": stage["ms_bbox_morton"],
+                                                 "bytes": alg["kick_bbox"] + alg["morton"]},
+                    "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rng = np.random.default_rng(1)
+        t = statistics.mean(cpu_sample_step(st, p, threads, 8192, rng) for _ in range(2))
+        cpu = {"value": n / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"2 samples of: full {n}-particle tree build + walk of 8192 random targets, "
+                         f"{threads} threads, scaled to all targets (oracle C++ restatement of Lbvh)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": p["name"], "particles_per_gpu": n, "theta": p["theta"], "eps": p["eps"],
+                           "dt": p["dt"], "precision": "FP32 walk (Kahan), FP64 pos/vel and opening re-checks",
+                           "parallelism": "replicas" if ws > 1 else "single system",
+                           "l2": "working set ~330 B/particle > L2 (no flush needed)", "cuda_graph": True},
+                "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clk, "stage_ms": stage, "walk_counts": counts}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="collision", choices=["collision", "plummer"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

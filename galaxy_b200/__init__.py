@@ -1,0 +1,436 @@
+"""galaxy_b200 -- B200 (sm_100a) LBVH Barnes-Hut gravity step behind galaxy's solver API.
+
+Host-side mirror of the reference interfaces (paths relative to the reference
+project root), each a thin layer over the C ABI of ``libgalaxy_b200.so``:
+
+* :class:`State` -- ``core/src/state.rs:29`` (SoA f64 pos/vel/mass, time).
+* :class:`ForceSolver` -- ``core/src/traits.rs:24-157``: ``accelerations(state, acc)``
+  and ``potential_energy(state)``.
+* :class:`GpuLbvh` -- the drop-in GPU backend, ``gpu/src/gpu_lbvh_fused.rs:44-146``
+  (``Lbvh::new(g, softening, theta)`` semantics, ``solvers/src/lbvh.rs:643-683``).
+* :class:`LeapfrogKdk` -- ``core/src/integrator.rs:6-78``.
+* :class:`GpuResidentLeapfrog` -- ``gpu/src/gpu_resident.rs:1685-1960``
+  (upload / step / step_many / snapshot / time / len / submits).
+* :class:`Batch` -- many independent systems stepped by one launch per stage.
+* stage functions ``stage_morton`` / ``stage_sort`` / ``stage_build`` -- the
+  ``reference_*`` oracles' GPU counterparts (``solvers/src/lbvh.rs:105-348``).
+
+Errors follow the reference's conventions: constructors raise on a missing device
+(``GpuError``), a length mismatch raises like the reference's ``assert_eq!``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import (GX_FLAG_NO_KAHAN, GX_FLAG_STAGE_TIMES, GX_FLAG_STATS, GX_MULTIPOLE_MONO, GX_MULTIPOLE_QUAD,
+                   GX_PREC_F32, GX_PREC_F64, GxError, check, lib)
+
+__all__ = [
+    "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "GxError", "PinnedState",
+    "stage_morton",
+    "stage_sort", "stage_build", "device_info", "ic",
+]
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+@dataclass
+class State:
+    """core/src/state.rs:29 -- positions/velocities [n,3] f64, masses [n] f64, time."""
+
+    pos: np.ndarray
+    vel: np.ndarray
+    mass: np.ndarray
+    time: float = 0.0
+
+    def __post_init__(self):
+        self.pos = _f64(self.pos).reshape(-1, 3)
+        self.vel = _f64(self.vel).reshape(-1, 3)
+        self.mass = _f64(self.mass).reshape(-1)
+        n = self.pos.shape[0]
+        if self.vel.shape[0] != n or self.mass.shape[0] != n:
+            raise ValueError("vel/mass length must match pos")
+
+    def __len__(self):
+        return self.pos.shape[0]
+
+    def copy(self) -> "State":
+        return State(self.pos.copy(), self.vel.copy(), self.mass.copy(), self.time)
+
+
+class ForceSolver:
+    """core/src/traits.rs:24-157 (the gravity part of the trait)."""
+
+    def accelerations(self, state: State, acc: np.ndarray) -> None:
+        raise NotImplementedError
+
+    def potential_energy(self, state: State) -> float:
+        raise NotImplementedError
+
+
+def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: int, walk_block: int,
+             stage_times: bool = False):
+    o = _lib.Options()
+    o.struct_size = C.sizeof(_lib.Options)
+    o.precision = {"f32": GX_PREC_F32, "f64": GX_PREC_F64}[precision]
+    o.multipole = {"mono": GX_MULTIPOLE_MONO, "quad": GX_MULTIPOLE_QUAD}[multipole]
+    o.flags = ((0 if kahan else GX_FLAG_NO_KAHAN) | (GX_FLAG_STATS if stats else 0) |
+               (GX_FLAG_STAGE_TIMES if stage_times else 0))
+    o.device = device
+    o.walk_block = walk_block
+    return o
+
+
+class _Handle:
+    def __init__(self, g, softening, theta, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
+                 walk_block=0, stage_times=False):
+        self.g, self.softening, self.theta = float(g), float(softening), float(theta)
+        self._h = C.c_void_p()
+        o = _options(precision, multipole, kahan, stats, device, walk_block, stage_times)
+        rc = lib().gx_create(self.g, self.softening, self.theta, C.byref(o), C.byref(self._h))
+        if rc != 0:
+            check(rc, None)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().gx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        check(rc, self._h)
+
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        self._ck(lib().gx_get_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in s._fields_}
+
+
+class GpuLbvh(_Handle, ForceSolver):
+    """Drop-in GPU ForceSolver (gpu/src/gpu_lbvh_fused.rs:44-146) over libgalaxy_b200.
+
+    precision: "f32" (FP32 walk, Kahan-compensated, opening decisions guarded in
+    FP64) or "f64" (the reference's arithmetic, bit-identical to Lbvh on the CPU).
+    multipole: "mono" (the reference) or "quad" (adds node quadrupoles).
+    """
+
+    def accelerations(self, state, acc=None, mass=None):
+        """Fill acc[n,3] (or return a new array) with the acceleration of each particle.
+
+        Accepts a State, or positions [n,3] plus ``mass``.
+        """
+        if isinstance(state, State):
+            pos, m = state.pos, state.mass
+        else:
+            pos, m = _f64(state).reshape(-1, 3), _f64(mass).reshape(-1)
+        n = pos.shape[0]
+        out = acc if acc is not None else np.empty((n, 3))
+        if out.shape != (n, 3) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("acc length must match particle count (C-contiguous f64 [n,3])")
+        self._ck(lib().gx_accelerations(self._h, n, _ptr(pos), _ptr(m), _ptr(out)))
+        return out
+
+    def potential_energy(self, state, mass=None) -> float:
+        pos, m = (state.pos, state.mass) if isinstance(state, State) else (_f64(state).reshape(-1, 3), _f64(mass))
+        out = C.c_double()
+        self._ck(lib().gx_potential_energy(self._h, pos.shape[0], _ptr(pos), _ptr(m), C.byref(out)))
+        return out.value
+
+    def kdk_step_host(self, st: "PinnedState", dt: float, primed: bool) -> bool:
+        """One LeapfrogKdk step (core/src/integrator.rs:38-78) on host arrays, this solver
+        computing the accelerations. Returns the integrator's primed flag."""
+        p = C.c_int(1 if primed else 0)
+        self._ck(lib().gx_kdk_step_host(self._h, len(st), _ptr(st.pos), _ptr(st.vel), _ptr(st.mass), _ptr(st.acc),
+                                        C.byref(p), float(dt)))
+        st.time += dt
+        return bool(p.value)
+
+    def direct_sum_f64(self, pos, mass, targets=None):
+        """FP64 direct summation on the GPU (the large-N force oracle)."""
+        pos, mass = _f64(pos).reshape(-1, 3), _f64(mass)
+        t = None if targets is None else np.ascontiguousarray(targets, dtype=np.uint32)
+        nt = pos.shape[0] if t is None else t.shape[0]
+        out = np.empty((nt, 3))
+        self._ck(lib().gx_direct_sum_f64(self._h, pos.shape[0], _ptr(pos), _ptr(mass), nt, _ptr(t), _ptr(out)))
+        return out
+
+
+class LeapfrogKdk:
+    """core/src/integrator.rs:6-78 -- kick-drift-kick with cached accelerations (host arrays)."""
+
+    def __init__(self):
+        self.acc = np.zeros((0, 3))
+        self.primed = False
+
+    def reset(self):
+        self.acc = np.zeros((0, 3))
+        self.primed = False
+
+    def prime(self, state: State, solver: ForceSolver):
+        self.acc = np.zeros((len(state), 3))
+        solver.accelerations(state, self.acc)
+        self.primed = True
+
+    def step(self, state: State, solver: ForceSolver, dt: float):
+        n = len(state)
+        if self.acc.shape[0] != n:
+            self.acc = np.zeros((n, 3))
+            self.primed = False
+        if not self.primed:
+            solver.accelerations(state, self.acc)
+            self.primed = True
+        half = 0.5 * dt
+        state.vel += self.acc * half
+        state.pos += state.vel * dt
+        solver.accelerations(state, self.acc)
+        state.vel += self.acc * half
+        state.time += dt
+
+
+class GpuResidentLeapfrog(_Handle):
+    """gpu/src/gpu_resident.rs:1685-1960 -- state kept on the device across KDK steps."""
+
+    MAX_BATCH = 64  # the reference's submit cap; steps here are graph launches, not submits
+
+    def __init__(self, g, softening, theta, **kw):
+        super().__init__(g, softening, theta, **kw)
+        self._mass = np.zeros(0)
+
+    def upload(self, state: State):
+        self._mass = state.mass.copy()
+        self._ck(lib().gx_upload(self._h, len(state), _ptr(state.pos), _ptr(state.vel), _ptr(state.mass)))
+
+    def step(self, dt: float):
+        self._ck(lib().gx_step(self._h, float(dt)))
+
+    def step_many(self, dt: float, steps: int):
+        self._ck(lib().gx_step_many(self._h, float(dt), int(steps)))
+
+    def step_many_timed(self, dt: float, steps: int) -> float:
+        """Run steps and return their device time in ms (CUDA events on the handle's stream)."""
+        ms = C.c_float()
+        self._ck(lib().gx_step_many_timed(self._h, float(dt), int(steps), C.byref(ms)))
+        return ms.value
+
+    def step_many_async(self, dt: float, steps: int):
+        self._ck(lib().gx_step_many_async(self._h, float(dt), int(steps)))
+
+    def synchronize(self):
+        self._ck(lib().gx_synchronize(self._h))
+
+    def snapshot(self) -> State:
+        n = len(self)
+        pos, vel = np.empty((n, 3)), np.empty((n, 3))
+        self._ck(lib().gx_snapshot(self._h, _ptr(pos), _ptr(vel)))
+        return State(pos, vel, self._mass.copy(), self.time())
+
+    def accelerations(self) -> np.ndarray:
+        out = np.empty((len(self), 3))
+        self._ck(lib().gx_resident_accelerations(self._h, _ptr(out)))
+        return out
+
+    def diagnostics(self, with_potential: bool = True) -> dict:
+        out = np.zeros(8)
+        self._ck(lib().gx_diagnostics(self._h, int(with_potential), _ptr(out)))
+        return {"kinetic": out[0], "potential": out[1], "total": out[0] + out[1], "momentum": out[2:5].copy(),
+                "angular_momentum": out[5:8].copy()}
+
+    def time(self) -> float:
+        t = C.c_double()
+        self._ck(lib().gx_time(self._h, C.byref(t)))
+        return t.value
+
+    def __len__(self):
+        n = C.c_size_t()
+        self._ck(lib().gx_len(self._h, C.byref(n)))
+        return n.value
+
+    def submits(self) -> int:
+        v = C.c_uint64()
+        self._ck(lib().gx_launches(self._h, C.byref(v)))
+        return v.value
+
+
+class PinnedState:
+    """A State whose arrays live in page-locked host memory (gx_host_alloc), plus the
+    integrator's cached acceleration."""
+
+    def __init__(self, n: int):
+        self.n = n
+        self._bufs = []
+        self.pos = self._alloc((n, 3))
+        self.vel = self._alloc((n, 3))
+        self.mass = self._alloc((n,))
+        self.acc = self._alloc((n, 3))
+        self.time = 0.0
+
+    def _alloc(self, shape):
+        nbytes = int(np.prod(shape)) * 8
+        p = C.c_void_p()
+        check(lib().gx_host_alloc(max(nbytes, 8), C.byref(p)))
+        self._bufs.append(p)
+        buf = (C.c_double * max(int(np.prod(shape)), 1)).from_address(p.value)
+        return np.frombuffer(buf, dtype=np.float64, count=int(np.prod(shape))).reshape(shape)
+
+    @classmethod
+    def from_state(cls, st: State) -> "PinnedState":
+        p = cls(len(st))
+        p.pos[:] = st.pos
+        p.vel[:] = st.vel
+        p.mass[:] = st.mass
+        p.acc[:] = 0.0
+        p.time = st.time
+        return p
+
+    def __len__(self):
+        return self.n
+
+    def __del__(self):
+        try:
+            for b in self._bufs:
+                lib().gx_host_free(b)
+            self._bufs = []
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent systems, one launch per stage (see include/galaxy_b200.h)."""
+
+    def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
+                 walk_block=0):
+        self._b = C.c_void_p()
+        o = _options(precision, multipole, kahan, stats, device, walk_block)
+        rc = lib().gx_batch_create(int(budget_bytes), C.byref(o), C.byref(self._b))
+        if rc != 0:
+            check(rc, None)
+        self._mass = {}
+
+    def _ck(self, rc):
+        check(rc, self._b, "gx_batch_last_error")
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            lib().gx_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, state: State, g: float, softening: float, theta: float, dt: float) -> int:
+        sid = C.c_uint64()
+        self._ck(lib().gx_system_add(self._b, len(state), _ptr(state.pos), _ptr(state.vel), _ptr(state.mass), g,
+                                     softening, theta, dt, C.byref(sid)))
+        self._mass[sid.value] = state.mass.copy()
+        return sid.value
+
+    def remove(self, sid: int):
+        self._ck(lib().gx_system_remove(self._b, sid))
+        self._mass.pop(sid, None)
+
+    def system_bytes(self, n: int) -> int:
+        out = C.c_size_t()
+        self._ck(lib().gx_system_bytes(self._b, n, C.byref(out)))
+        return out.value
+
+    def step(self, steps: int = 1):
+        self._ck(lib().gx_batch_step(self._b, int(steps)))
+
+    def set_graph(self, enable: bool):
+        self._ck(lib().gx_batch_set_graph(self._b, int(enable)))
+
+    def snapshot(self, sid: int) -> State:
+        n = C.c_size_t()
+        self._ck(lib().gx_system_len(self._b, sid, C.byref(n)))
+        pos, vel, t = np.empty((n.value, 3)), np.empty((n.value, 3)), C.c_double()
+        self._ck(lib().gx_system_snapshot(self._b, sid, _ptr(pos), _ptr(vel), C.byref(t)))
+        return State(pos, vel, self._mass[sid].copy(), t.value)
+
+    def stats(self) -> dict:
+        s = _lib.BatchStats()
+        self._ck(lib().gx_batch_stats_get(self._b, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in s._fields_}
+
+
+# ---- stage entry points (parity tests) ------------------------------------------------
+def _stage_handle(h=None, **kw):
+    return h if h is not None else GpuLbvh(1.0, 0.0, 0.5, **kw)
+
+
+def stage_morton(pos, handle=None):
+    """reference_morton on the GPU: (lanes [n,3] u32, codes [n] u32, bounds dict)."""
+    h = _stage_handle(handle)
+    pos = _f64(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    lanes = np.empty((n, 3), np.uint32)
+    codes = np.empty(n, np.uint32)
+    b = np.empty(5)
+    h._ck(lib().gx_stage_morton(h._h, n, _ptr(pos), _ptr(lanes), _ptr(codes), _ptr(b)))
+    return lanes, codes, {"bmin": b[:3].copy(), "size": float(b[3]), "scale": float(b[4])}
+
+
+def stage_sort(codes, handle=None):
+    """reference_sort on the GPU: (order [n] u32, sorted_codes [n] u32)."""
+    h = _stage_handle(handle)
+    codes = np.ascontiguousarray(codes, dtype=np.uint32)
+    n = codes.shape[0]
+    order = np.empty(n, np.uint32)
+    sc = np.empty(n, np.uint32)
+    h._ck(lib().gx_stage_sort(h._h, n, _ptr(codes), _ptr(order), _ptr(sc)))
+    return order, sc
+
+
+def stage_build(sorted_codes, sorted_pos, sorted_mass, handle=None, quad=False):
+    """reference_karras + reference_aggregate on the GPU."""
+    h = _stage_handle(handle, multipole="quad" if quad else "mono")
+    sc = np.ascontiguousarray(sorted_codes, dtype=np.uint32)
+    sp = _f64(sorted_pos).reshape(-1, 3)
+    sm = _f64(sorted_mass)
+    n = sc.shape[0]
+    t = 2 * n - 1
+    left = np.empty(max(n - 1, 1), np.uint32)
+    right = np.empty(max(n - 1, 1), np.uint32)
+    parent = np.empty(t, np.uint32)
+    mn, mx, com = np.empty((t, 3)), np.empty((t, 3)), np.empty((t, 3))
+    mass = np.empty(t)
+    q = np.empty((t, 6)) if quad else None
+    h._ck(lib().gx_stage_build(h._h, n, _ptr(sc), _ptr(sp), _ptr(sm), _ptr(left), _ptr(right), _ptr(parent), _ptr(mn),
+                               _ptr(mx), _ptr(com), _ptr(mass), _ptr(q)))
+    out = {"left": left[: n - 1], "right": right[: n - 1], "parent": parent, "aabb_min": mn, "aabb_max": mx,
+           "com": com, "mass": mass}
+    if quad:
+        out["quad"] = q
+    return out
+
+
+def device_info(device: int = 0) -> dict:
+    name = C.create_string_buffer(256)
+    sm, ma, mi, mem = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+    rc = lib().gx_device_info(device, name, 256, C.byref(sm), C.byref(ma), C.byref(mi), C.byref(mem))
+    check(rc, None)
+    return {"name": name.value.decode(), "sm_count": sm.value, "cc": (ma.value, mi.value), "total_mem": mem.value}
+
+
+from . import ic  # noqa: E402  (uses the helpers above)

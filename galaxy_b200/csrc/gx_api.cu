@@ -1,0 +1,888 @@
+// gx_api.cu -- the C ABI of one system: ForceSolver-style calls, resident leapfrog
+// stepping, stage entry points and diagnostics (declared in include/galaxy_b200.h).
+//
+// Reference interfaces: core/src/traits.rs:24-157 (ForceSolver),
+// gpu/src/gpu_lbvh_fused.rs:44-146 (the drop-in GPU backend),
+// gpu/src/gpu_resident.rs:1685-1960 (upload / step / step_many / snapshot / time).
+// The closing half kick of a step is deferred into the next step's kick + drift
+// kernel (two separately rounded half kicks, as integrator.rs:61-73 applies them)
+// or into a snapshot, so it costs no extra pass over the state.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/galaxy_b200.h"
+#include "gx_kernels.h"
+#include "gx_runtime.h"
+
+using namespace gx;
+
+namespace gx {
+
+thread_local std::string g_global_err;
+
+void set_global_err(const std::string& s) { g_global_err = s; }
+const char* global_err() { return g_global_err.c_str(); }
+
+bool check_device(int device, std::string& err) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    err = std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
+    return false;
+  }
+  int dev = device;
+  if (dev < 0) {
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  }
+  if (dev >= count) {
+    err = "device ordinal out of range";
+    return false;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+    err = "cudaGetDeviceProperties failed";
+    return false;
+  }
+  if (p.major != 10) {
+    err = std::string("libgalaxy_b200 is built for sm_100a (B200); device is ") + p.name + " sm_" +
+          std::to_string(p.major) + std::to_string(p.minor);
+    return false;
+  }
+  return true;
+}
+
+// ---- Arena: one system's device buffers -------------------------------------------
+void Arena::release() {
+  for (void* p : allocs)
+    if (p) cudaFree(p);
+  allocs.clear();
+  bytes = 0;
+  b = StepBufs();
+  cap_n = 0;
+  cap_tiles = 0;
+  cap_items = 0;
+  cap_sys = 0;
+}
+
+cudaError_t Arena::alloc(void** p, size_t nbytes) {
+  nbytes = (nbytes + 255) & ~size_t(255);
+  if (nbytes == 0) nbytes = 256;
+  cudaError_t e = cudaMalloc(p, nbytes);
+  if (e == cudaSuccess) {
+    allocs.push_back(*p);
+    bytes += nbytes;
+  }
+  return e;
+}
+
+size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
+  const size_t tiles = n / kTile + nsys + 1;
+  size_t s = 0;
+  s += 3 * 3 * n * 8 + n * 8;                 // pos, vel, acc, mass
+  s += 4 * n * 4;                             // codes, keys_alt, order, vals_alt
+  s += n * (32 + 16 + 16);                    // leaf64, leafA, leafB
+  s += n * 8 + 2 * n * 4 + n * sizeof(Agg64); // kids, parent, agg64
+  s += 4 * n * 16;                            // nodeA..D
+  s += n * 8;                                 // slots
+  if (quad) s += 2 * n * 16 + 6 * n * 8;
+  if (f64rec) s += n * sizeof(Node64);
+  s += tiles * sizeof(TileDesc) + (n / 32 + nsys + 1) * sizeof(WalkItem);
+  s += nsys * (sizeof(SysDesc) + sizeof(Bounds) + 48 + kRadixPasses * kRadixBins * 4);
+  s += kRadixPasses * tiles * kRadixBins * 4 + 64;
+  s += (n / 256 + 1) * 8 * 8;  // diagnostic partials
+  return s + 64 * 256;         // alignment slack
+}
+
+cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int quad, int f64rec, cudaStream_t st) {
+  if (n <= cap_n && tiles <= cap_tiles && items <= cap_items && nsys <= cap_sys && quad <= cap_quad &&
+      f64rec <= cap_f64)
+    return cudaSuccess;
+  // Grow (never shrink), with headroom so a slowly growing N does not reallocate
+  // every call.
+  size_t nn = std::max(n, cap_n + cap_n / 4);
+  size_t nt = std::max(tiles, cap_tiles + cap_tiles / 4);
+  size_t ni = std::max(items, cap_items + cap_items / 4);
+  size_t ns = std::max(nsys, cap_sys);
+  int q = std::max(quad, cap_quad), f = std::max(f64rec, cap_f64);
+  cudaStreamSynchronize(st);
+  release();
+  cudaError_t e = cudaSuccess;
+#define GX_A(ptr, count, T)                                              \
+  do {                                                                   \
+    void* _p = nullptr;                                                  \
+    e = alloc(&_p, (size_t)(count) * sizeof(T));                         \
+    if (e != cudaSuccess) return e;                                      \
+    ptr = reinterpret_cast<decltype(ptr)>(_p);                           \
+  } while (0)
+  GX_A(b.pos, 3 * nn, double);
+  GX_A(b.vel, 3 * nn, double);
+  GX_A(b.acc, 3 * nn, double);
+  double* mass = nullptr;
+  GX_A(mass, nn, double);
+  b.mass = mass;
+  mass_rw = mass;
+  GX_A(b.codes, nn, uint32_t);
+  GX_A(b.keys_alt, nn, uint32_t);
+  GX_A(b.order, nn, uint32_t);
+  GX_A(b.vals_alt, nn, uint32_t);
+  GX_A(b.leaf64, nn, double4);
+  GX_A(b.leafA, nn, float4);
+  GX_A(b.leafB, nn, float4);
+  GX_A(b.kids, nn, uint2);
+  GX_A(b.parent, 2 * nn, uint32_t);
+  GX_A(b.agg64, nn, Agg64);
+  GX_A(b.nodeA, nn, float4);
+  GX_A(b.nodeB, nn, float4);
+  GX_A(b.nodeC, nn, float4);
+  GX_A(b.nodeD, nn, float4);
+  if (q) {
+    GX_A(b.nodeQ, 2 * nn, float4);
+    GX_A(b.q64, 6 * nn, double);
+  }
+  if (f) GX_A(b.node64, nn, Node64);
+  GX_A(b.slots, nn, unsigned long long);
+  TileDesc* tl = nullptr;
+  GX_A(tl, nt, TileDesc);
+  b.tiles = tl;
+  tiles_rw = tl;
+  WalkItem* it = nullptr;
+  GX_A(it, ni, WalkItem);
+  b.items = it;
+  items_rw = it;
+  SysDesc* sd = nullptr;
+  GX_A(sd, ns, SysDesc);
+  b.sys = sd;
+  sys_rw = sd;
+  GX_A(b.bounds, ns, Bounds);
+  // One zeroed region per step: bbox words, histograms, look-back status, counters.
+  const size_t z_bbox = 6 * ns * sizeof(unsigned long long);
+  const size_t z_hist = ns * kRadixPasses * kRadixBins * sizeof(uint32_t);
+  const size_t z_stat = (size_t)kRadixPasses * nt * kRadixBins * sizeof(uint32_t);
+  const size_t z_ctr = 16 * sizeof(uint32_t);
+  char* z = nullptr;
+  GX_A(z, z_bbox + z_hist + z_stat + z_ctr, char);
+  b.bbox_enc = reinterpret_cast<unsigned long long*>(z);
+  b.hist = reinterpret_cast<uint32_t*>(z + z_bbox);
+  b.sort_status = reinterpret_cast<uint32_t*>(z + z_bbox + z_hist);
+  b.counters = reinterpret_cast<uint32_t*>(z + z_bbox + z_hist + z_stat);
+  b.zero_begin = z;
+  b.zero_bytes = z_bbox + z_hist + z_stat + z_ctr;
+  GX_A(b.ctl, 1, DevCtl);
+  diag_cap = nn / 256 + 2;
+  GX_A(diag_partial, 8 * diag_cap, double);
+#undef GX_A
+  e = cudaMemsetAsync(b.slots, 0xFF, nn * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(b.ctl, 0, sizeof(DevCtl), st);
+  if (e != cudaSuccess) return e;
+  cap_n = nn;
+  cap_tiles = nt;
+  cap_items = ni;
+  cap_sys = ns;
+  cap_quad = q;
+  cap_f64 = f;
+  return cudaStreamSynchronize(st);
+}
+
+// Host-side tile and walk-item tables of a list of systems packed back to back.
+void make_tables(const std::vector<SysDesc>& in, std::vector<SysDesc>& sys, std::vector<TileDesc>& tiles,
+                 std::vector<WalkItem>& items) {
+  sys = in;
+  tiles.clear();
+  items.clear();
+  for (uint32_t s = 0; s < sys.size(); ++s) {
+    SysDesc& d = sys[s];
+    d.first_tile = static_cast<uint32_t>(tiles.size());
+    for (uint32_t b0 = 0; b0 < d.n; b0 += kTile) {
+      TileDesc t;
+      t.sys = s;
+      t.begin = d.off + b0;
+      t.end = d.off + std::min<uint32_t>(d.n, b0 + kTile);
+      t.pad = 0;
+      tiles.push_back(t);
+    }
+    d.ntiles = static_cast<uint32_t>(tiles.size()) - d.first_tile;
+    for (uint32_t b0 = 0; b0 < d.n; b0 += 32) items.push_back(WalkItem{d.off + b0, s});
+  }
+}
+
+}  // namespace gx
+
+// ===================================================================================
+struct gx_handle {
+  double g = 1.0, eps = 0.0, theta = 0.5;
+  gx_options opt{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  std::string err;
+  Arena ar;
+  // current layout
+  size_t n_layout = 0;
+  double dt_layout = 0.0;
+  // resident state
+  size_t n = 0;
+  double time = 0.0;
+  bool resident = false;
+  bool pending_kick = false;
+  uint64_t launches = 0;
+  gx_stats stats{};
+  // graph of one resident step (pending closing kick + opening kick, drift, force)
+  cudaGraphExec_t step_graph = nullptr;
+  size_t graph_n = 0;
+  double graph_dt = 0.0;
+};
+
+namespace {
+
+int fail(gx_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define GX_CK(h, call)                                                                        \
+  do {                                                                                        \
+    cudaError_t _e = (call);                                                                  \
+    if (_e != cudaSuccess)                                                                    \
+      return fail((h), GX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));      \
+  } while (0)
+
+WalkCfg walk_cfg(const gx_handle* h) {
+  WalkCfg c;
+  c.precision = h->opt.precision == GX_PREC_F64 ? 1 : 0;
+  c.quad = (h->opt.multipole == GX_MULTIPOLE_QUAD && c.precision == 0) ? 1 : 0;
+  c.kahan = (h->opt.flags & GX_FLAG_NO_KAHAN) ? 0 : 1;
+  c.stats = (h->opt.flags & GX_FLAG_STATS) ? 1 : 0;
+  c.inside_test = h->theta >= 0.57 ? 1 : 0;
+  c.block = h->opt.walk_block ? static_cast<int>(h->opt.walk_block) : 256;
+  return c;
+}
+
+// Lay out one system of n particles (tables + SysDesc) with step dt.
+int layout(gx_handle* h, size_t n, double dt) {
+  if (n > (1u << 30)) return fail(h, GX_ERR_INVALID_ARG, "N above 2^30 is not supported (30-bit look-back counts)");
+  if (n == h->n_layout && dt == h->dt_layout && h->ar.cap_n >= n) return GX_OK;
+  std::vector<SysDesc> in(1), sys;
+  in[0].off = 0;
+  in[0].n = static_cast<uint32_t>(n);
+  in[0].g = h->g;
+  in[0].eps = h->eps;
+  in[0].theta = h->theta;
+  in[0].dt = dt;
+  std::vector<TileDesc> tiles;
+  std::vector<WalkItem> items;
+  make_tables(in, sys, tiles, items);
+  const int quad = h->opt.multipole == GX_MULTIPOLE_QUAD;
+  const int f64 = h->opt.precision == GX_PREC_F64;
+  GX_CK(h, h->ar.ensure(n, tiles.size(), items.size(), 1, quad, f64, h->stream));
+  StepBufs& b = h->ar.b;
+  b.n = static_cast<uint32_t>(n);
+  b.nsys = 1;
+  b.ntiles = static_cast<uint32_t>(tiles.size());
+  b.nitems = static_cast<uint32_t>(items.size());
+  // The per-step zero region: bbox words, histograms, look-back status, counters.
+  b.zero_bytes = reinterpret_cast<char*>(b.counters) - reinterpret_cast<char*>(b.zero_begin) + 16 * sizeof(uint32_t);
+  GX_CK(h, cudaMemcpyAsync(h->ar.sys_rw, sys.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.tiles_rw, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice,
+                           h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.items_rw, items.data(), items.size() * sizeof(WalkItem), cudaMemcpyHostToDevice,
+                           h->stream));
+  GX_CK(h, cudaStreamSynchronize(h->stream));
+  h->n_layout = n;
+  h->dt_layout = dt;
+  if (h->step_graph) {
+    cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
+  return GX_OK;
+}
+
+// Enqueue bbox (+kick/drift) -> Morton -> sort -> build -> walk on b.
+void enqueue_force(gx_handle* h, const StepBufs& b, int kick, int pending, bool timed) {
+  cudaStream_t st = h->stream;
+  if (timed) cudaEventRecord(h->ev[0], st);
+  cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, st);
+  launch_kick_drift_bbox(b, kick, pending, st);
+  launch_morton_hist(b, nullptr, st);
+  if (timed) cudaEventRecord(h->ev[1], st);
+  launch_sort(b, st);
+  if (timed) cudaEventRecord(h->ev[2], st);
+  launch_build(b, h->opt.multipole == GX_MULTIPOLE_QUAD && h->opt.precision != GX_PREC_F64,
+               h->opt.precision == GX_PREC_F64, st);
+  if (timed) cudaEventRecord(h->ev[3], st);
+  launch_walk(b, walk_cfg(h), st);
+  if (timed) cudaEventRecord(h->ev[4], st);
+  h->launches += 1;
+}
+
+// Wait for the stream, then turn the device error word into a status.
+int finish(gx_handle* h, bool timed) {
+  GX_CK(h, cudaStreamSynchronize(h->stream));
+  GX_CK(h, cudaGetLastError());
+  DevCtl ctl;
+  GX_CK(h, cudaMemcpy(&ctl, h->ar.b.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost));
+  if (timed) {
+    cudaEventElapsedTime(&h->stats.ms_bbox_morton, h->ev[0], h->ev[1]);
+    cudaEventElapsedTime(&h->stats.ms_sort, h->ev[1], h->ev[2]);
+    cudaEventElapsedTime(&h->stats.ms_build, h->ev[2], h->ev[3]);
+    cudaEventElapsedTime(&h->stats.ms_walk, h->ev[3], h->ev[4]);
+    cudaEventElapsedTime(&h->stats.ms_total, h->ev[0], h->ev[4]);
+  }
+  h->stats.leaf_interactions = ctl.stats[0];
+  h->stats.far_interactions = ctl.stats[1];
+  h->stats.nodes_opened = ctl.stats[2];
+  h->stats.f64_rechecks = ctl.stats[3];
+  h->stats.warp_node_visits = ctl.stats[4];
+  if (ctl.err) {
+    // Re-arm the climb slots and clear the word so the handle stays usable.
+    cudaMemset(h->ar.b.slots, 0xFF, h->ar.cap_n * sizeof(unsigned long long));
+    cudaMemset(h->ar.b.ctl, 0, sizeof(DevCtl));
+    char buf[128];
+    snprintf(buf, sizeof buf, "device check tripped (error word 0x%x)", ctl.err);
+    return fail(h, GX_ERR_DEVICE_CHECK, buf);
+  }
+  if (h->opt.flags & GX_FLAG_STATS) cudaMemset(h->ar.b.ctl, 0, sizeof(DevCtl));
+  return GX_OK;
+}
+
+bool stats_on(const gx_handle* h) { return (h->opt.flags & GX_FLAG_STAGE_TIMES) != 0; }
+
+}  // namespace
+
+// ===================================================================================
+extern "C" {
+
+int gx_create(double g, double softening, double theta, const gx_options* opt, gx_handle** out) {
+  if (!out) return GX_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!(softening >= 0.0) || !(theta >= 0.0) || !(g == g)) {
+    set_global_err("softening and theta must be >= 0");
+    return GX_ERR_INVALID_ARG;
+  }
+  gx_options o{};
+  o.device = -1;
+  if (opt && opt->struct_size) {
+    if (opt->struct_size < sizeof(gx_options)) {
+      set_global_err("gx_options.struct_size too small");
+      return GX_ERR_INVALID_ARG;
+    }
+    o = *opt;
+  }
+  if (o.precision > GX_PREC_F64 || o.multipole > GX_MULTIPOLE_QUAD ||
+      (o.walk_block && (o.walk_block % 32 || o.walk_block > 256))) {
+    set_global_err("invalid gx_options");
+    return GX_ERR_INVALID_ARG;
+  }
+  std::string err;
+  if (!check_device(o.device, err)) {
+    set_global_err(err);
+    return GX_ERR_NO_DEVICE;
+  }
+  gx_handle* h = new gx_handle();
+  h->g = g;
+  h->eps = softening;
+  h->theta = theta;
+  h->opt = o;
+  int dev = o.device;
+  if (dev < 0) cudaGetDevice(&dev);
+  h->device = dev;
+  cudaError_t e = cudaSetDevice(dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  if (e != cudaSuccess) {
+    set_global_err(std::string("stream/event creation failed: ") + cudaGetErrorString(e));
+    delete h;
+    return GX_ERR_CUDA;
+  }
+  *out = h;
+  return GX_OK;
+}
+
+void gx_destroy(gx_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+  h->ar.release();
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* gx_last_error(const gx_handle* h) { return h ? h->err.c_str() : global_err(); }
+
+int gx_device_info(int device, char* name_out, size_t name_len, int* sm_count, int* cc_major, int* cc_minor,
+                   size_t* total_mem) {
+  cudaDeviceProp p;
+  cudaError_t e = cudaGetDeviceProperties(&p, device < 0 ? 0 : device);
+  if (e != cudaSuccess) {
+    set_global_err(cudaGetErrorString(e));
+    return GX_ERR_NO_DEVICE;
+  }
+  if (name_out && name_len) {
+    strncpy(name_out, p.name, name_len - 1);
+    name_out[name_len - 1] = 0;
+  }
+  if (sm_count) *sm_count = p.multiProcessorCount;
+  if (cc_major) *cc_major = p.major;
+  if (cc_minor) *cc_minor = p.minor;
+  if (total_mem) *total_mem = p.totalGlobalMem;
+  return GX_OK;
+}
+
+int gx_accelerations(gx_handle* h, size_t n, const double* pos, const double* mass, double* acc_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n == 0) return GX_OK;
+  if (!pos || !mass || !acc_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  if (n == 1) {
+    acc_out[0] = acc_out[1] = acc_out[2] = 0.0;
+    return GX_OK;
+  }
+  cudaSetDevice(h->device);
+  // A ForceSolver call does not disturb resident state: it uses the same arena, so
+  // the resident system is dropped.
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  enqueue_force(h, b, 0, 0, stats_on(h));
+  GX_CK(h, cudaMemcpyAsync(acc_out, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  h->stats.n = n;
+  return finish(h, stats_on(h));
+}
+
+int gx_accelerations_device(gx_handle* h, size_t n, const double* d_pos, const double* d_mass, double* d_acc) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n == 0) return GX_OK;
+  if (!d_pos || !d_mass || !d_acc) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  cudaSetDevice(h->device);
+  if (n == 1) {
+    GX_CK(h, cudaMemsetAsync(d_acc, 0, 3 * sizeof(double), h->stream));
+    return GX_OK;
+  }
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs b = h->ar.b;
+  b.pos = const_cast<double*>(d_pos);
+  b.mass = d_mass;
+  b.acc = d_acc;
+  enqueue_force(h, b, 0, 0, false);
+  h->stats.n = n;
+  return GX_OK;
+}
+
+int gx_synchronize(gx_handle* h) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  return finish(h, false);
+}
+
+int gx_potential_energy(gx_handle* h, size_t n, const double* pos, const double* mass, double* out) {
+  if (!h || !out) return GX_ERR_INVALID_ARG;
+  *out = 0.0;
+  if (n < 2) return GX_OK;
+  if (!pos || !mass) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  cudaSetDevice(h->device);
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const uint32_t np = potential_partials(static_cast<uint32_t>(n));
+  launch_potential_f64(static_cast<uint32_t>(n), b.pos, b.mass, h->g, h->eps, h->ar.diag_partial, np, h->stream);
+  std::vector<double> part(np);
+  GX_CK(h, cudaMemcpyAsync(part.data(), h->ar.diag_partial, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaStreamSynchronize(h->stream));
+  double u = 0.0;
+  for (double v : part) u += v;
+  *out = u;
+  return GX_OK;
+}
+
+int gx_direct_sum_f64(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_targets,
+                      const uint32_t* targets, double* acc_out) {
+  if (!h || !pos || !mass || !acc_out) return GX_ERR_INVALID_ARG;
+  if (n == 0) return GX_OK;
+  if (!targets) n_targets = n;
+  for (size_t t = 0; targets && t < n_targets; ++t)
+    if (targets[t] >= n) return fail(h, GX_ERR_INVALID_ARG, "target index out of range");
+  cudaSetDevice(h->device);
+  h->resident = false;
+  int rc = layout(h, std::max(n, n_targets), 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  uint32_t* d_t = nullptr;
+  if (targets) {
+    d_t = b.keys_alt;
+    GX_CK(h, cudaMemcpyAsync(d_t, targets, n_targets * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  }
+  launch_direct_sum_f64(static_cast<uint32_t>(n), b.pos, b.mass, h->g, h->eps, static_cast<uint32_t>(n_targets), d_t,
+                        b.acc, h->stream);
+  GX_CK(h, cudaMemcpyAsync(acc_out, b.acc, 3 * n_targets * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaStreamSynchronize(h->stream));
+  return GX_OK;
+}
+
+// ---- resident ----------------------------------------------------------------------
+int gx_upload(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n && (!pos || !vel || !mass)) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  cudaSetDevice(h->device);
+  h->n = n;
+  h->time = 0.0;
+  h->pending_kick = false;
+  h->resident = true;
+  if (n == 0) return GX_OK;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(b.vel, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (n == 1) {
+    GX_CK(h, cudaMemsetAsync(b.acc, 0, 3 * sizeof(double), h->stream));
+    return finish(h, false);
+  }
+  // Prime a(x0) (gpu_resident.rs:1793-1799).
+  enqueue_force(h, b, 0, 0, stats_on(h));
+  h->stats.n = n;
+  return finish(h, stats_on(h));
+}
+
+namespace {
+int step_enqueue(gx_handle* h, double dt, uint64_t steps) {
+  if (!h->resident) return fail(h, GX_ERR_STATE, "step before upload");
+  if (h->n == 0 || steps == 0) {
+    h->time += static_cast<double>(steps) * dt;
+    return GX_OK;
+  }
+  int rc = layout(h, h->n, dt);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  if (h->n == 1) {
+    // No force on a lone particle: kick is zero, drift x += v dt each step.
+    for (uint64_t s = 0; s < steps; ++s) launch_kick_drift_bbox(b, 1, 0, h->stream);
+    h->time += static_cast<double>(steps) * dt;
+    return GX_OK;
+  }
+  uint64_t s = 0;
+  const bool timed = stats_on(h);
+  if (!h->pending_kick || timed) {
+    // First step after upload/snapshot (no deferred closing kick) runs eagerly.
+    enqueue_force(h, b, 1, h->pending_kick ? 1 : 0, timed);
+    h->pending_kick = true;
+    h->time += dt;
+    s = 1;
+  }
+  if (s < steps) {
+    if (timed) {
+      for (; s < steps; ++s) {
+        enqueue_force(h, b, 1, 1, true);
+        h->time += dt;
+      }
+      return GX_OK;
+    }
+    if (!h->step_graph) {
+      cudaGraph_t g = nullptr;
+      GX_CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_force(h, b, 1, 1, false);
+      h->launches -= 1;
+      GX_CK(h, cudaStreamEndCapture(h->stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&h->step_graph, g, 0);
+      cudaGraphDestroy(g);
+      GX_CK(h, e);
+    }
+    for (; s < steps; ++s) {
+      GX_CK(h, cudaGraphLaunch(h->step_graph, h->stream));
+      h->launches += 1;
+      h->time += dt;
+    }
+  }
+  return GX_OK;
+}
+}  // namespace
+
+int gx_step_many_async(gx_handle* h, double dt, uint64_t steps) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  return step_enqueue(h, dt, steps);
+}
+
+int gx_step_many(gx_handle* h, double dt, uint64_t steps) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  int rc = step_enqueue(h, dt, steps);
+  if (rc) return rc;
+  return finish(h, false);
+}
+
+int gx_step(gx_handle* h, double dt) { return gx_step_many(h, dt, 1); }
+
+int gx_step_many_timed(gx_handle* h, double dt, uint64_t steps, float* ms_out) {
+  if (!h || !ms_out) return GX_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  GX_CK(h, cudaEventRecord(h->ev[5], h->stream));
+  int rc = step_enqueue(h, dt, steps);
+  if (rc) return rc;
+  GX_CK(h, cudaEventRecord(h->ev[4], h->stream));
+  rc = finish(h, false);
+  if (rc) return rc;
+  GX_CK(h, cudaEventElapsedTime(ms_out, h->ev[5], h->ev[4]));
+  return GX_OK;
+}
+
+int gx_kdk_step_host(gx_handle* h, size_t n, double* pos, double* vel, const double* mass, double* acc,
+                     int* primed, double dt) {
+  if (!h || !primed) return GX_ERR_INVALID_ARG;
+  if (n == 0) return GX_OK;
+  if (!pos || !vel || !mass || !acc) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  int rc;
+  if (!*primed) {
+    rc = gx_accelerations(h, n, pos, mass, acc);
+    if (rc) return rc;
+    *primed = 1;
+  }
+  const double half = 0.5 * dt;
+  for (size_t i = 0; i < 3 * n; ++i) vel[i] = vel[i] + acc[i] * half;
+  for (size_t i = 0; i < 3 * n; ++i) pos[i] = pos[i] + vel[i] * dt;
+  rc = gx_accelerations(h, n, pos, mass, acc);
+  if (rc) return rc;
+  for (size_t i = 0; i < 3 * n; ++i) vel[i] = vel[i] + acc[i] * half;
+  return GX_OK;
+}
+
+int gx_host_alloc(size_t bytes, void** out) {
+  if (!out) return GX_ERR_INVALID_ARG;
+  cudaError_t e = cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    set_global_err(std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    *out = nullptr;
+    return GX_ERR_CUDA;
+  }
+  return GX_OK;
+}
+
+void gx_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+namespace {
+int apply_pending(gx_handle* h) {
+  if (h->pending_kick && h->n > 1) {
+    launch_kick_half(h->ar.b, h->stream);
+    h->pending_kick = false;
+  }
+  return GX_OK;
+}
+}  // namespace
+
+int gx_snapshot(gx_handle* h, double* pos_out, double* vel_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "snapshot before upload");
+  if (h->n == 0) return GX_OK;
+  cudaSetDevice(h->device);
+  apply_pending(h);
+  const size_t bytes = 3 * h->n * sizeof(double);
+  if (pos_out) GX_CK(h, cudaMemcpyAsync(pos_out, h->ar.b.pos, bytes, cudaMemcpyDeviceToHost, h->stream));
+  if (vel_out) GX_CK(h, cudaMemcpyAsync(vel_out, h->ar.b.vel, bytes, cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_resident_accelerations(gx_handle* h, double* acc_out) {
+  if (!h || !acc_out) return GX_ERR_INVALID_ARG;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "no resident state");
+  if (h->n == 0) return GX_OK;
+  cudaSetDevice(h->device);
+  GX_CK(h, cudaMemcpyAsync(acc_out, h->ar.b.acc, 3 * h->n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_time(const gx_handle* h, double* t_out) {
+  if (!h || !t_out) return GX_ERR_INVALID_ARG;
+  *t_out = h->time;
+  return GX_OK;
+}
+
+int gx_len(const gx_handle* h, size_t* n_out) {
+  if (!h || !n_out) return GX_ERR_INVALID_ARG;
+  *n_out = h->resident ? h->n : 0;
+  return GX_OK;
+}
+
+int gx_launches(const gx_handle* h, uint64_t* out) {
+  if (!h || !out) return GX_ERR_INVALID_ARG;
+  *out = h->launches;
+  return GX_OK;
+}
+
+int gx_diagnostics(gx_handle* h, int with_potential, double* out) {
+  if (!h || !out) return GX_ERR_INVALID_ARG;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "no resident state");
+  for (int i = 0; i < 8; ++i) out[i] = 0.0;
+  if (h->n == 0) return GX_OK;
+  cudaSetDevice(h->device);
+  apply_pending(h);
+  const uint32_t n = static_cast<uint32_t>(h->n);
+  StepBufs& b = h->ar.b;
+  const uint32_t nd = std::min<uint32_t>(potential_partials(n), 1024u);
+  launch_diag_sums(n, b.pos, b.vel, b.mass, h->ar.diag_partial, nd, h->stream);
+  std::vector<double> part(7 * nd);
+  GX_CK(h, cudaMemcpyAsync(part.data(), h->ar.diag_partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+  GX_CK(h, cudaStreamSynchronize(h->stream));
+  for (uint32_t i = 0; i < nd; ++i) {
+    out[0] += part[7 * i];
+    for (int c = 0; c < 3; ++c) {
+      out[2 + c] += part[7 * i + 1 + c];
+      out[5 + c] += part[7 * i + 4 + c];
+    }
+  }
+  if (with_potential && n > 1) {
+    const uint32_t np = potential_partials(n);
+    launch_potential_f64(n, b.pos, b.mass, h->g, h->eps, h->ar.diag_partial, np, h->stream);
+    std::vector<double> pp(np);
+    GX_CK(h, cudaMemcpyAsync(pp.data(), h->ar.diag_partial, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    GX_CK(h, cudaStreamSynchronize(h->stream));
+    for (double v : pp) out[1] += v;
+  }
+  return finish(h, false);
+}
+
+int gx_get_stats(const gx_handle* h, gx_stats* out) {
+  if (!h || !out) return GX_ERR_INVALID_ARG;
+  *out = h->stats;
+  return GX_OK;
+}
+
+// ---- stage entry points -------------------------------------------------------------
+int gx_stage_morton(gx_handle* h, size_t n, const double* pos, uint32_t* lanes_out, uint32_t* codes_out,
+                    double* bounds_out) {
+  if (!h || !pos || !codes_out) return GX_ERR_INVALID_ARG;
+  if (n == 0) return fail(h, GX_ERR_INVALID_ARG, "reference_morton requires a non-empty system");
+  cudaSetDevice(h->device);
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, h->stream));
+  launch_kick_drift_bbox(b, 0, 0, h->stream);
+  // Lanes (3n u32) are staged in leafA (n float4 = 4n u32), unused by this stage.
+  uint32_t* d_lanes = lanes_out ? reinterpret_cast<uint32_t*>(b.leafA) : nullptr;
+  launch_morton_hist(b, d_lanes, h->stream);
+  GX_CK(h, cudaMemcpyAsync(codes_out, b.codes, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  if (lanes_out)
+    GX_CK(h, cudaMemcpyAsync(lanes_out, d_lanes, 3 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  Bounds bd;
+  GX_CK(h, cudaMemcpyAsync(&bd, b.bounds, sizeof(Bounds), cudaMemcpyDeviceToHost, h->stream));
+  rc = finish(h, false);
+  if (rc) return rc;
+  if (bounds_out) {
+    bounds_out[0] = bd.bmin[0];
+    bounds_out[1] = bd.bmin[1];
+    bounds_out[2] = bd.bmin[2];
+    bounds_out[3] = bd.size;
+    bounds_out[4] = bd.scale;
+  }
+  return GX_OK;
+}
+
+int gx_stage_sort(gx_handle* h, size_t n, const uint32_t* codes, uint32_t* order_out, uint32_t* sorted_codes_out) {
+  if (!h || (n && (!codes || !order_out))) return GX_ERR_INVALID_ARG;
+  if (n == 0) return GX_OK;
+  for (size_t i = 0; i < n; ++i)
+    if (codes[i] >= (1u << 30)) return fail(h, GX_ERR_INVALID_ARG, "codes must be 30-bit");
+  cudaSetDevice(h->device);
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.codes, codes, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, h->stream));
+  launch_code_hist(b, h->stream);
+  launch_sort(b, h->stream);
+  GX_CK(h, cudaMemcpyAsync(order_out, b.order, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  if (sorted_codes_out)
+    GX_CK(h, cudaMemcpyAsync(sorted_codes_out, b.codes, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const double* sorted_pos,
+                   const double* sorted_mass, uint32_t* left, uint32_t* right, uint32_t* parent, double* aabb_min,
+                   double* aabb_max, double* com, double* mass, double* quad_out) {
+  if (!h || !sorted_codes || !sorted_pos || !sorted_mass || !parent) return GX_ERR_INVALID_ARG;
+  if (n == 0) return fail(h, GX_ERR_INVALID_ARG, "reference_karras requires a non-empty system");
+  if (n > 1 && (!left || !right)) return GX_ERR_INVALID_ARG;
+  if (quad_out && h->opt.multipole != GX_MULTIPOLE_QUAD)
+    return fail(h, GX_ERR_INVALID_ARG, "quadrupole output needs a GX_MULTIPOLE_QUAD handle");
+  cudaSetDevice(h->device);
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  std::vector<uint32_t> iota(n);
+  for (size_t i = 0; i < n; ++i) iota[i] = static_cast<uint32_t>(i);
+  GX_CK(h, cudaMemcpyAsync(b.codes, sorted_codes, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(b.order, iota.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(b.pos, sorted_pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, sorted_mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const int quad = h->opt.multipole == GX_MULTIPOLE_QUAD && h->opt.precision != GX_PREC_F64;
+  launch_build(b, quad, h->opt.precision == GX_PREC_F64, h->stream);
+  std::vector<uint2> kids(n > 1 ? n - 1 : 1);
+  std::vector<Agg64> agg(n > 1 ? n - 1 : 1);
+  std::vector<double4> leaf(n);
+  std::vector<double> q64(quad ? 6 * n : 0);
+  if (n > 1) {
+    GX_CK(h, cudaMemcpyAsync(kids.data(), b.kids, (n - 1) * sizeof(uint2), cudaMemcpyDeviceToHost, h->stream));
+    GX_CK(h, cudaMemcpyAsync(agg.data(), b.agg64, (n - 1) * sizeof(Agg64), cudaMemcpyDeviceToHost, h->stream));
+    if (quad)
+      GX_CK(h, cudaMemcpyAsync(q64.data(), b.q64, 6 * (n - 1) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  GX_CK(h, cudaMemcpyAsync(parent, b.parent, (2 * n - 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaMemcpyAsync(leaf.data(), b.leaf64, n * sizeof(double4), cudaMemcpyDeviceToHost, h->stream));
+  rc = finish(h, false);
+  if (rc) return rc;
+  for (size_t i = 0; i + 1 < n; ++i) {
+    left[i] = kids[i].x;
+    right[i] = kids[i].y;
+  }
+  for (size_t u = 0; u < 2 * n - 1; ++u) {
+    double mn[3], mx[3], cm[3], m;
+    if (u < n) {
+      const double4 l = leaf[u];
+      mn[0] = mx[0] = cm[0] = l.x;
+      mn[1] = mx[1] = cm[1] = l.y;
+      mn[2] = mx[2] = cm[2] = l.z;
+      m = l.w;
+    } else {
+      const Agg64& a = agg[u - n];
+      for (int c = 0; c < 3; ++c) {
+        mn[c] = a.mn[c];
+        mx[c] = a.mx[c];
+        cm[c] = a.com[c];
+      }
+      m = a.m;
+    }
+    for (int c = 0; c < 3; ++c) {
+      if (aabb_min) aabb_min[3 * u + c] = mn[c];
+      if (aabb_max) aabb_max[3 * u + c] = mx[c];
+      if (com) com[3 * u + c] = cm[c];
+    }
+    if (mass) mass[u] = m;
+    if (quad_out)
+      for (int c = 0; c < 6; ++c) quad_out[6 * u + c] = u < n ? 0.0 : q64[6 * (u - n) + c];
+  }
+  return GX_OK;
+}
+
+}  // extern "C"

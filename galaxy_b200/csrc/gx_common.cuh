@@ -1,0 +1,162 @@
+// gx_common.cuh -- shared device helpers and data layout of the LBVH gravity step.
+//
+// Layout in HBM for one system of N particles (or a batch of systems packed back
+// to back; see gx_batch.cu):
+//   particle state, original order, DVec3 layout (3 x f64 per particle):
+//     pos[3N], vel[3N], acc[3N]; mass[N] (f64)
+//   Morton codes code[N] (u32), the sort's ping-pong (key, index) buffers.
+//   sorted leaves (leaf k = k-th particle in (code, index) order):
+//     leaf64[k] = double4(x, y, z, m)          FP64 payload for folds and rechecks
+//     leafA[k]  = float4(x_hi, y_hi, z_hi, m)  FP32 walk record
+//     leafB[k]  = float4(x_lo, y_lo, z_lo, 0)  low words of the float-float split
+//     order[k]  original index
+//   internal node i (Karras numbering, unified index N + i):
+//     kids[i]   = uint2(left, right) unified children
+//     parent[u] unified parent of every node (root: 0xFFFFFFFF)
+//     agg64[i]  = {aabb_min[3], aabb_max[3], com[3], mass} FP64 (bit-exact fold)
+//     nodeA[i]  = float4(com_hi.xyz, mass)
+//     nodeB[i]  = float4(com_lo.xyz, rcrit2)   rcrit2 = (s/theta + delta)^2
+//     nodeC[i]  = float4(center.xyz, 0), nodeD[i] = float4(half.xyz, 0)  (theta >= 1/sqrt 3)
+//     nodeQ[i]  = 2 x float4 traceless quadrupole (xx, xy, xz, yy), (yz, zz, 0, 0)
+//     node64[i] = {center[3], half[3], com[3], mass, delta, s}  FP64 walk record
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gx {
+
+constexpr uint32_t kNoParent = 0xFFFFFFFFu;
+constexpr uint64_t kEmptySlot = 0xFFFFFFFFFFFFFFFFull;
+
+// Bounded waits: every spin in these kernels gives up after this many polls,
+// raises the device error word and carries on, so no kernel can hang the GPU.
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+// Device error word bits (read back by the host after each call).
+constexpr uint32_t kErrLookbackTimeout = 1u << 0;
+constexpr uint32_t kErrStackOverflow = 1u << 1;
+constexpr uint32_t kErrBadIndex = 1u << 2;
+constexpr uint32_t kErrClimb = 1u << 3;
+
+struct Agg64 {
+  double mn[3];
+  double mx[3];
+  double com[3];
+  double m;
+};
+
+struct Node64 {
+  double c[3];
+  double h[3];
+  double com[3];
+  double m;
+  double delta;
+  double s;
+};
+
+// Morton bounding cube of one system (solvers/src/lbvh.rs:105-120 convention).
+struct Bounds {
+  double bmin[3];
+  double size;
+  double scale;
+  double lo[3];
+  double hi[3];
+  float tiny2;    // absolute guard for FP32 distance comparisons (coincident geometry)
+  uint32_t pad;
+};
+
+// Work is cut into tiles of kTile particles that never straddle two systems; the
+// bbox, Morton, sort and build kernels each run one CTA per tile.
+constexpr int kTile = 4096;
+constexpr int kTileThreads = 256;
+constexpr int kItemsPerThread = kTile / kTileThreads;  // 16
+constexpr int kRadixBits = 8;
+constexpr int kRadixBins = 1 << kRadixBits;
+constexpr int kRadixPasses = 4;  // 30-bit codes: 8 + 8 + 8 + 6 bits
+
+struct TileDesc {
+  uint32_t sys, begin, end, pad;
+};
+
+// One independent particle system (a batch holds many, packed back to back).
+struct SysDesc {
+  uint32_t off, n;              // particle range [off, off + n)
+  uint32_t first_tile, ntiles;  // its tiles
+  double g, eps, theta, dt;
+  uint32_t flags;               // kSysPendingKick: the closing half kick is still owed
+  uint32_t pad;
+};
+constexpr uint32_t kSysPendingKick = 1u;
+
+// 32 consecutive sorted targets of one system, walked by one warp.
+struct WalkItem {
+  uint32_t begin, sys;
+};
+
+// Order-preserving map of an f64 onto u64 so that unsigned atomicMax is a float max;
+// 0 lies below every real number, so a zeroed word is the identity.
+__device__ __forceinline__ unsigned long long enc_max(double x) {
+  unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dec_max(unsigned long long e) {
+  unsigned long long b = (e >> 63) ? (e & 0x7FFFFFFFFFFFFFFFull) : ~e;
+  return __longlong_as_double(static_cast<long long>(b));
+}
+
+// Per-call device scalars.
+struct DevCtl {
+  uint32_t err;
+  uint32_t bbox_done;
+  uint32_t pad[2];
+  unsigned long long stats[8];  // leaf, far, open, recheck, warp visits
+};
+
+// ---- exact f64 arithmetic (no contraction into FMA, as Rust's f64 ops) ---------
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
+// glam dot: (x*x + y*y) + z*z
+__device__ __forceinline__ double dlen2(double x, double y, double z) {
+  return dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
+}
+
+// ---- Morton (solvers/src/lbvh.rs:37-64) ----------------------------------------
+__host__ __device__ __forceinline__ uint32_t expand10(uint32_t v) {
+  uint32_t x = v & 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+__host__ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return expand10(x) | (expand10(y) << 1) | (expand10(z) << 2);
+}
+// Rust `(v.floor().max(0.0) as u32).min(1023)`.
+__device__ __forceinline__ uint32_t quantize_lane(double v) {
+  double f = floor(v);
+  if (!(f >= 0.0)) return 0u;  // negative or NaN
+  if (f >= 1023.0) return 1023u;
+  return static_cast<uint32_t>(f);
+}
+
+// ---- augmented-key common prefix over sorted codes (solvers/src/lbvh.rs:153-165)
+// Positions are local to the system (the reference indexes each system from 0).
+__device__ __forceinline__ int prefix_len(uint32_t ca, uint32_t cb, uint32_t a_local, uint32_t b_local) {
+  if (ca == cb) return 32 + __clz(a_local ^ b_local);
+  return __clz(ca ^ cb);
+}
+
+// ---- float-float split of an f64 coordinate ------------------------------------
+__device__ __forceinline__ void split_ff(double x, float& hi, float& lo) {
+  hi = __double2float_rn(x);
+  lo = __double2float_rn(x - static_cast<double>(hi));
+}
+
+__device__ __forceinline__ void raise_err(DevCtl* ctl, uint32_t bit) { atomicOr(&ctl->err, bit); }
+
+}  // namespace gx

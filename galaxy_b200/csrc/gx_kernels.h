@@ -1,0 +1,85 @@
+// gx_kernels.h -- device buffer bundle and kernel launchers of one step.
+#pragma once
+
+#include "gx_common.cuh"
+
+namespace gx {
+
+// Every device buffer a step touches (owned by gx_solver / gx_batch).
+struct StepBufs {
+  uint32_t n = 0;       // particles over all systems
+  uint32_t nsys = 0;
+  uint32_t ntiles = 0;
+  uint32_t nitems = 0;  // walk items (32 targets each)
+  const TileDesc* tiles = nullptr;
+  const SysDesc* sys = nullptr;
+  const WalkItem* items = nullptr;
+  // particle state, original order
+  double* pos = nullptr;
+  double* vel = nullptr;
+  double* acc = nullptr;
+  const double* mass = nullptr;
+  // per-step scratch (zeroed by one memset per step, see zero_begin/zero_bytes)
+  unsigned long long* bbox_enc = nullptr;  // 6 per system
+  uint32_t* hist = nullptr;                // nsys * 4 * 256
+  uint32_t* sort_status = nullptr;         // 4 * ntiles * 256
+  uint32_t* counters = nullptr;            // [0..3] sort tile counters, [4] walk item counter
+  void* zero_begin = nullptr;
+  size_t zero_bytes = 0;
+  Bounds* bounds = nullptr;  // per system
+  // sort
+  uint32_t* codes = nullptr;     // keys (pass-0 input, final sorted keys)
+  uint32_t* keys_alt = nullptr;
+  uint32_t* order = nullptr;     // values (final permutation)
+  uint32_t* vals_alt = nullptr;
+  // leaves, sorted order
+  double4* leaf64 = nullptr;
+  float4* leafA = nullptr;
+  float4* leafB = nullptr;
+  // internal nodes
+  uint2* kids = nullptr;
+  uint32_t* parent = nullptr;
+  Agg64* agg64 = nullptr;
+  float4* nodeA = nullptr;
+  float4* nodeB = nullptr;
+  float4* nodeC = nullptr;
+  float4* nodeD = nullptr;
+  float4* nodeQ = nullptr;   // 2 per node (quadrupole mode)
+  double* q64 = nullptr;     // 6 per node (quadrupole mode)
+  Node64* node64 = nullptr;  // FP64 walk mode
+  unsigned long long* slots = nullptr;  // climb exchange words, kEmptySlot between builds
+  DevCtl* ctl = nullptr;
+};
+
+struct WalkCfg {
+  int precision = 0;  // 0 = FP32, 1 = FP64
+  int quad = 0;
+  int kahan = 1;
+  int stats = 0;
+  int inside_test = 0;  // some system has theta >= 1/sqrt(3)
+  int block = 256;
+  int persistent_ctas = 0;  // 0 = one warp per item (no stealing)
+};
+
+// gx_step.cu
+void launch_kick_drift_bbox(const StepBufs& b, int kick, int pending, cudaStream_t st);
+void launch_kick_half(const StepBufs& b, cudaStream_t st);
+void launch_morton_hist(const StepBufs& b, uint32_t* lanes_out, cudaStream_t st);
+// gx_sort.cu: the four onesweep passes (codes, iota) -> (codes sorted, order)
+void launch_sort(const StepBufs& b, cudaStream_t st);
+// per-system digit histograms of b.codes (when codes come from the host)
+void launch_code_hist(const StepBufs& b, cudaStream_t st);
+// gx_build.cu: gather leaves + bottom-up Karras build and aggregation
+void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st);
+// gx_walk.cu: tree walk, acc in original order
+void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st);
+// gx_diag.cu
+void launch_direct_sum_f64(uint32_t n, const double* pos, const double* mass, double g, double eps,
+                           uint32_t n_targets, const uint32_t* targets, double* acc, cudaStream_t st);
+void launch_potential_f64(uint32_t n, const double* pos, const double* mass, double g, double eps, double* partial,
+                          uint32_t n_partial, cudaStream_t st);
+void launch_diag_sums(uint32_t n, const double* pos, const double* vel, const double* mass, double* partial,
+                      uint32_t n_partial, cudaStream_t st);
+uint32_t potential_partials(uint32_t n);
+
+}  // namespace gx

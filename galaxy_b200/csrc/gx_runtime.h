@@ -1,0 +1,40 @@
+// gx_runtime.h -- host-side device-memory arena shared by the single-system handle and
+// the batch (one set of step buffers, grown lazily, never shrunk).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "gx_kernels.h"
+
+namespace gx {
+
+struct Arena {
+  StepBufs b;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  size_t cap_n = 0, cap_tiles = 0, cap_items = 0, cap_sys = 0;
+  int cap_quad = 0, cap_f64 = 0;
+  // writable aliases of the const pointers in b
+  double* mass_rw = nullptr;
+  TileDesc* tiles_rw = nullptr;
+  WalkItem* items_rw = nullptr;
+  SysDesc* sys_rw = nullptr;
+  double* diag_partial = nullptr;
+  size_t diag_cap = 0;
+
+  cudaError_t alloc(void** p, size_t nbytes);
+  cudaError_t ensure(size_t n, size_t tiles, size_t items, size_t nsys, int quad, int f64rec, cudaStream_t st);
+  void release();
+  // Device bytes an arena for n particles in nsys systems takes.
+  static size_t bytes_for(size_t n, size_t nsys, int quad, int f64rec);
+  ~Arena() { release(); }
+};
+
+void make_tables(const std::vector<SysDesc>& in, std::vector<SysDesc>& sys, std::vector<TileDesc>& tiles,
+                 std::vector<WalkItem>& items);
+bool check_device(int device, std::string& err);
+void set_global_err(const std::string& s);
+const char* global_err();
+
+}  // namespace gx

@@ -1,0 +1,212 @@
+// gx_sort.cu -- stable LSD radix sort of (Morton code, original index) pairs,
+// one "onesweep" kernel per 8-bit digit pass, segmented by system.
+//
+// Reference: solvers/src/lbvh.rs:143-147 (`reference_sort`: the permutation that
+// sorts by (code, original index)). A stable LSD sort fed with the identity
+// permutation reproduces it bit for bit; every step below keeps stability:
+//   * keys are ranked inside a tile in input order (warp-striped ownership, ranks
+//     from __match_any_sync peer masks and running per-warp digit counters);
+//   * tiles of a system are chained in index order through decoupled look-back;
+//   * the scatter is staged through shared memory so each digit's run of a tile
+//     is written as one contiguous, coalesced segment.
+// The digit histograms of all four passes come from the Morton kernel (one read
+// of the keys), so each pass reads and writes every (key, index) pair once.
+// Tiles never straddle systems and each system has its own histograms and
+// look-back chain, so a batch of systems is sorted per system in one launch.
+#include "gx_kernels.h"
+
+namespace gx {
+
+namespace {
+
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1;
+constexpr int kWarps = kTileThreads / 32;
+
+// Exclusive scan of one value per thread over a 256-thread CTA.
+__device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_t* s_warp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  uint32_t base = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) base += (w < warp) ? s_warp[w] : 0u;
+  __syncthreads();
+  return base + x - v;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
+__device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *reinterpret_cast<volatile uint32_t*>(p) = v; }
+
+}  // namespace
+
+__global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint32_t* __restrict__ keys_in,
+                                                           const uint32_t* __restrict__ vals_in,
+                                                           uint32_t* __restrict__ keys_out,
+                                                           uint32_t* __restrict__ vals_out,
+                                                           const TileDesc* __restrict__ tiles,
+                                                           const SysDesc* __restrict__ sys,
+                                                           const uint32_t* __restrict__ hist,
+                                                           uint32_t* __restrict__ status, uint32_t* counters,
+                                                           uint32_t ntiles, DevCtl* ctl) {
+  __shared__ uint32_t s_keys[kTile];
+  __shared__ uint32_t s_vals[kTile];
+  __shared__ uint32_t s_whist[kWarps][kRadixBins];
+  __shared__ uint32_t s_blk_start[kRadixBins];
+  __shared__ uint32_t s_glob[kRadixBins];
+  __shared__ uint32_t s_scan[kWarps];
+  __shared__ uint32_t s_tile;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int shift = pass * kRadixBits;
+  if (threadIdx.x == 0) s_tile = atomicAdd(&counters[pass], 1u);
+  for (int i = threadIdx.x; i < kWarps * kRadixBins; i += kTileThreads) (&s_whist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  if (tile >= ntiles) {  // counters not re-armed: refuse rather than read past the table
+    if (threadIdx.x == 0) raise_err(ctl, kErrBadIndex);
+    return;
+  }
+  const TileDesc t = tiles[tile];
+  const SysDesc sd = sys[t.sys];
+
+  // Load: warp w owns the contiguous 512-key slice [w*512, w*512+512) of the tile,
+  // item j of lane l at w*512 + 32 j + l (coalesced, and in index order per warp).
+  uint32_t key[kItemsPerThread], val[kItemsPerThread], rank[kItemsPerThread];
+#pragma unroll
+  for (int j = 0; j < kItemsPerThread; ++j) {
+    const uint32_t idx = t.begin + warp * (32 * kItemsPerThread) + 32 * j + lane;
+    if (idx < t.end) {
+      key[j] = keys_in[idx];
+      val[j] = vals_in ? vals_in[idx] : idx;
+    } else {
+      key[j] = 0xFFFFFFFFu;  // pad: largest digit, ranked after every real key
+      val[j] = 0;
+    }
+  }
+
+  // Rank within the warp: peers holding the same digit, in lane order, after the
+  // warp's earlier items of that digit.
+  const uint32_t lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < kItemsPerThread; ++j) {
+    const uint32_t d = (key[j] >> shift) & (kRadixBins - 1);
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t before = s_whist[warp][d];
+    rank[j] = before + __popc(peers & lt_mask);
+    __syncwarp();
+    if (lane == 31 - __clz(peers)) s_whist[warp][d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Thread d owns digit d: per-warp exclusive offsets, tile total, block-local start.
+  const uint32_t d = threadIdx.x;
+  uint32_t total = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const uint32_t c = s_whist[w][d];
+    s_whist[w][d] = total;
+    total += c;
+  }
+  const uint32_t blk_start = block_exclusive_scan_256(total, s_scan);
+  s_blk_start[d] = blk_start;
+
+  // Decoupled look-back along this system's tiles (bounded waits).
+  uint32_t* st = status + (size_t)pass * ntiles * kRadixBins;
+  const uint32_t tl = tile - sd.first_tile;
+  uint32_t excl = 0;
+  if (tl == 0) {
+    st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagPrefix | (total & kValMask));
+  } else {
+    st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagAgg | (total & kValMask));
+    uint32_t p = tile - 1;
+    for (;;) {
+      uint32_t w = ld_volatile(&st[(size_t)p * kRadixBins + d]);
+      uint32_t spins = 0;
+      while ((w & ~kValMask) == 0) {
+        if (++spins > kSpinLimit) {
+          raise_err(ctl, kErrLookbackTimeout);
+          w = kFlagPrefix;
+          break;
+        }
+        __nanosleep(64);
+        w = ld_volatile(&st[(size_t)p * kRadixBins + d]);
+      }
+      excl += w & kValMask;
+      if ((w & ~kValMask) == kFlagPrefix || p == sd.first_tile) break;
+      --p;
+    }
+    st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagPrefix | ((excl + total) & kValMask));
+  }
+  // Global start of digit d for this tile: system offset + digits below d in the
+  // whole system + the same digit in the system's earlier tiles.
+  const uint32_t* hs = hist + ((size_t)t.sys * kRadixPasses + pass) * kRadixBins;
+  const uint32_t pass_base = block_exclusive_scan_256(hs[d], s_scan);
+  s_glob[d] = sd.off + pass_base + excl - blk_start;
+  __syncthreads();
+
+  // Stage in shared memory at the block-local sorted position.
+#pragma unroll
+  for (int j = 0; j < kItemsPerThread; ++j) {
+    const uint32_t dj = (key[j] >> shift) & (kRadixBins - 1);
+    const uint32_t r = s_blk_start[dj] + s_whist[warp][dj] + rank[j];
+    s_keys[r] = key[j];
+    s_vals[r] = val[j];
+  }
+  __syncthreads();
+
+  // Coalesced scatter: consecutive i of one digit land on consecutive addresses.
+  // Pads sort behind every real key, so only the first `count` entries are real.
+  const uint32_t count = t.end - t.begin;
+  for (uint32_t i = threadIdx.x; i < count; i += kTileThreads) {
+    const uint32_t k = s_keys[i];
+    const uint32_t dst = s_glob[(k >> shift) & (kRadixBins - 1)] + i;
+    keys_out[dst] = k;
+    vals_out[dst] = s_vals[i];
+  }
+}
+
+// Digit histograms of all passes from keys already in b.codes (stage entry point).
+__global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __restrict__ tiles,
+                                                            const uint32_t* __restrict__ codes,
+                                                            uint32_t* __restrict__ hist) {
+  __shared__ uint32_t sh[kRadixPasses * kRadixBins];
+  const TileDesc t = tiles[blockIdx.x];
+  for (int i = threadIdx.x; i < kRadixPasses * kRadixBins; i += kTileThreads) sh[i] = 0;
+  __syncthreads();
+  for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += kTileThreads) {
+    const uint32_t c = codes[i];
+#pragma unroll
+    for (int p = 0; p < kRadixPasses; ++p) atomicAdd(&sh[p * kRadixBins + ((c >> (p * kRadixBits)) & (kRadixBins - 1))], 1u);
+  }
+  __syncthreads();
+  uint32_t* hs = hist + (size_t)t.sys * kRadixPasses * kRadixBins;
+  for (int i = threadIdx.x; i < kRadixPasses * kRadixBins; i += kTileThreads)
+    if (sh[i]) atomicAdd(&hs[i], sh[i]);
+}
+
+void launch_code_hist(const StepBufs& b, cudaStream_t st) {
+  k_code_hist<<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.codes, b.hist);
+}
+
+void launch_sort(const StepBufs& b, cudaStream_t st) {
+  // pass 0: codes -> keys_alt (values: identity); 1: keys_alt -> codes;
+  // 2: codes -> keys_alt; 3: keys_alt -> codes. Final: (codes, order).
+  const uint32_t* kin[kRadixPasses] = {b.codes, b.keys_alt, b.codes, b.keys_alt};
+  uint32_t* kout[kRadixPasses] = {b.keys_alt, b.codes, b.keys_alt, b.codes};
+  const uint32_t* vin[kRadixPasses] = {nullptr, b.vals_alt, b.order, b.vals_alt};
+  uint32_t* vout[kRadixPasses] = {b.vals_alt, b.order, b.vals_alt, b.order};
+  for (int p = 0; p < kRadixPasses; ++p)
+    k_onesweep<<<b.ntiles, kTileThreads, 0, st>>>(p, kin[p], vin[p], kout[p], vout[p], b.tiles, b.sys, b.hist,
+                                                   b.sort_status, b.counters, b.ntiles, b.ctl);
+}
+
+}  // namespace gx

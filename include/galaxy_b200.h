@@ -1,0 +1,202 @@
+/*
+ * galaxy_b200.h -- C ABI of libgalaxy_b200.so, a B200 (sm_100a) implementation of
+ * galaxy's LBVH Barnes-Hut gravity step.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or torch
+ * types. Every call returns GX_OK (0) or a negative GX_ERR_* code and never aborts
+ * the process; the text of the last error of a handle is gx_last_error(handle)
+ * (gx_last_error(NULL) for failures that happen before a handle exists).
+ *
+ * Host arrays are owned by the caller and borrowed for the duration of a call.
+ * Positions, velocities and accelerations use the reference's DVec3 layout: 3
+ * consecutive f64 per particle (x, y, z), particle-major. Device memory is owned
+ * by the handle, grows lazily with N and is released by gx_destroy. A handle is
+ * used by one host thread at a time (the reference's `&mut self`).
+ *
+ * Reference interfaces (paths relative to the reference project root) replaced by
+ * these entry points are cited beside each declaration.
+ */
+#ifndef GALAXY_B200_H
+#define GALAXY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------- */
+#define GX_OK 0
+#define GX_ERR_INVALID_ARG -1   /* bad pointer, size or parameter */
+#define GX_ERR_CUDA -2          /* a CUDA runtime call failed (text in gx_last_error) */
+#define GX_ERR_NO_DEVICE -3     /* no CUDA device or not an sm_100 part */
+#define GX_ERR_BUDGET -4        /* device-memory budget would be exceeded */
+#define GX_ERR_STATE -5         /* call out of order (e.g. step before upload) */
+#define GX_ERR_DEVICE_CHECK -6  /* a kernel's bounded wait or bounds check tripped */
+#define GX_ERR_NOT_FOUND -7     /* unknown system / request id */
+#define GX_ERR_CAPACITY -8      /* a fixed-size table is full */
+
+/* ---- options --------------------------------------------------------------- */
+#define GX_PREC_F32 0  /* FP32 interactions with Kahan-compensated accumulation (default) */
+#define GX_PREC_F64 1  /* FP64 walk in the reference's exact operation order */
+
+#define GX_MULTIPOLE_MONO 0  /* monopole nodes, the reference's approximation (default) */
+#define GX_MULTIPOLE_QUAD 1  /* monopole + traceless quadrupole per node */
+
+#define GX_FLAG_NO_KAHAN 1u     /* plain FP32 accumulation in the F32 walk */
+#define GX_FLAG_STATS 2u        /* count interactions/openings per call (slower) */
+#define GX_FLAG_STAGE_TIMES 4u  /* time each stage with CUDA events (eager launches) */
+
+typedef struct gx_options {
+  uint32_t struct_size;    /* sizeof(gx_options); 0 means "all defaults" */
+  uint32_t precision;      /* GX_PREC_* */
+  uint32_t multipole;      /* GX_MULTIPOLE_* */
+  uint32_t flags;          /* GX_FLAG_* */
+  int32_t device;          /* CUDA ordinal, -1 = current device */
+  uint32_t walk_block;     /* threads per block of the tree walk, 0 = tuned default */
+} gx_options;
+
+typedef struct gx_handle gx_handle;
+
+/* Per-call statistics of the most recent force evaluation. */
+typedef struct gx_stats {
+  uint64_t n;              /* particles */
+  uint64_t leaf_interactions;
+  uint64_t far_interactions;
+  uint64_t nodes_opened;
+  uint64_t f64_rechecks;   /* opening decisions re-evaluated in FP64 (guard band) */
+  uint64_t warp_node_visits;
+  float ms_bbox_morton;    /* stage times of the last call, CUDA events */
+  float ms_sort;
+  float ms_build;
+  float ms_walk;
+  float ms_total;
+} gx_stats;
+
+/* ---- lifecycle ------------------------------------------------------------- */
+/* GpuLbvhFused::new / GpuResidentLeapfrog::new / Lbvh::new(g, softening, theta):
+ * gpu/src/gpu_lbvh_fused.rs:50, gpu/src/gpu_resident.rs:1292, solvers/src/lbvh.rs:653 */
+int gx_create(double g, double softening, double theta, const gx_options* opt, gx_handle** out);
+void gx_destroy(gx_handle* h);
+const char* gx_last_error(const gx_handle* h);
+int gx_device_info(int device, char* name_out, size_t name_len, int* sm_count, int* cc_major, int* cc_minor,
+                   size_t* total_mem);
+
+/* ---- ForceSolver (core/src/traits.rs:27, :95) ------------------------------- */
+/* ForceSolver::accelerations -- gpu/src/gpu_lbvh_fused.rs:58-134, solvers/src/lbvh.rs:663-676.
+ * acc_out[3n] receives the acceleration of each particle (x G). n == 0 is a no-op,
+ * n == 1 yields zero, as in the reference. */
+int gx_accelerations(gx_handle* h, size_t n, const double* pos, const double* mass, double* acc_out);
+/* Same on device pointers (pos[3n], mass[n], acc_out[3n] f64 in device memory),
+ * enqueued on the handle's stream; no host synchronisation. */
+int gx_accelerations_device(gx_handle* h, size_t n, const double* d_pos, const double* d_mass, double* d_acc);
+/* ForceSolver::potential_energy -- gpu/src/gpu_lbvh_fused.rs:140-146 delegating to
+ * solvers/src/potential.rs:51-58: the exact O(N^2) softened potential, here an FP64
+ * GPU reduction. */
+int gx_potential_energy(gx_handle* h, size_t n, const double* pos, const double* mass, double* out);
+/* FP64 direct summation (solvers/src/direct_sum.rs:25-45 semantics, unpaired) for the
+ * listed targets: the force oracle for large systems. targets == NULL means all. */
+int gx_direct_sum_f64(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_targets,
+                      const uint32_t* targets, double* acc_out);
+
+/* ---- resident leapfrog (gpu/src/gpu_resident.rs:1685-1960) ------------------- */
+/* GpuResidentLeapfrog::upload: copies state to the device and primes a(x0); resets time. */
+int gx_upload(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass);
+/* GpuResidentLeapfrog::step / step_many: KDK steps of dt, kept on the device. */
+int gx_step(gx_handle* h, double dt);
+int gx_step_many(gx_handle* h, double dt, uint64_t steps);
+/* Enqueue steps without waiting for them (for pipelined callers and CUDA-graph replay). */
+int gx_step_many_async(gx_handle* h, double dt, uint64_t steps);
+int gx_synchronize(gx_handle* h);
+/* GpuResidentLeapfrog::snapshot: pos_out/vel_out[3n] f64 (either may be NULL). */
+int gx_snapshot(gx_handle* h, double* pos_out, double* vel_out);
+/* The resident accelerations a(x_n) of the current state, acc_out[3n]. */
+int gx_resident_accelerations(gx_handle* h, double* acc_out);
+int gx_time(const gx_handle* h, double* t_out);                 /* gpu_resident.rs:1947 */
+int gx_len(const gx_handle* h, size_t* n_out);                  /* gpu_resident.rs:1960 */
+int gx_launches(const gx_handle* h, uint64_t* submits_out);     /* gpu_resident.rs:1955 */
+/* Energy and momentum diagnostics of the resident state (core/src/diagnostics.rs:8-68),
+ * FP64 on the device. out[8] = {kinetic, potential, px, py, pz, lx, ly, lz}; the O(N^2)
+ * potential is skipped (reported as 0) when with_potential == 0. */
+int gx_diagnostics(gx_handle* h, int with_potential, double* out);
+
+int gx_get_stats(const gx_handle* h, gx_stats* out);
+
+/* Enqueue `steps` resident steps and return their device time in milliseconds
+ * (CUDA events on the handle's stream around the steps). */
+int gx_step_many_timed(gx_handle* h, double dt, uint64_t steps, float* ms_out);
+
+/* LeapfrogKdk::step (core/src/integrator.rs:38-78) on HOST arrays with this handle as
+ * the ForceSolver: half kick and drift on the host in f64, accelerations through
+ * gx_accelerations (upload of pos and mass, download of acc). acc[3n] is the
+ * integrator's cached acceleration and *primed its `primed` flag. */
+int gx_kdk_step_host(gx_handle* h, size_t n, double* pos, double* vel, const double* mass, double* acc,
+                     int* primed, double dt);
+
+/* Page-locked host memory (for host buffers whose copies should run at full PCIe/C2C speed). */
+int gx_host_alloc(size_t bytes, void** out);
+void gx_host_free(void* p);
+
+/* ---- stage entry points for parity tests ------------------------------------- */
+/* reference_morton (solvers/src/lbvh.rs:105-129): lanes_out[3n] (may be NULL),
+ * codes_out[n], bounds_out[5] = {bmin.x, bmin.y, bmin.z, size, scale} (may be NULL). */
+int gx_stage_morton(gx_handle* h, size_t n, const double* pos, uint32_t* lanes_out, uint32_t* codes_out,
+                    double* bounds_out);
+/* reference_sort (solvers/src/lbvh.rs:143-147): stable permutation by (code, index). */
+int gx_stage_sort(gx_handle* h, size_t n, const uint32_t* codes, uint32_t* order_out, uint32_t* sorted_codes_out);
+/* reference_karras + reference_aggregate (solvers/src/lbvh.rs:276-348) from sorted
+ * codes and the sorted leaf payload. left/right[n-1], parent[2n-1] (unified index:
+ * leaves [0,n), internal node i at n+i); aabb_min/aabb_max/com[3(2n-1)], mass[2n-1]
+ * f64. quad_out[6(2n-1)] (may be NULL) = traceless quadrupole about each node's com. */
+int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const double* sorted_pos,
+                   const double* sorted_mass, uint32_t* left, uint32_t* right, uint32_t* parent, double* aabb_min,
+                   double* aabb_max, double* com, double* mass, double* quad_out);
+
+/* ---- batched systems (one launch per stage over many independent systems) ----- */
+typedef struct gx_batch gx_batch;
+
+typedef struct gx_batch_stats {
+  uint64_t systems;
+  uint64_t particles;
+  uint64_t steps;           /* batched steps taken */
+  uint64_t bytes_in_use;    /* device bytes held by the batch */
+  uint64_t budget_bytes;
+  float ms_last_step;
+} gx_batch_stats;
+
+/* budget_bytes: device-memory ceiling for system state and scratch (0 = no limit). */
+int gx_batch_create(size_t budget_bytes, const gx_options* opt, gx_batch** out);
+void gx_batch_destroy(gx_batch* b);
+const char* gx_batch_last_error(const gx_batch* b);
+/* Add one system (copies its state, primes a(x0)); GX_ERR_BUDGET when over budget. */
+int gx_system_add(gx_batch* b, size_t n, const double* pos, const double* vel, const double* mass, double g,
+                  double softening, double theta, double dt, uint64_t* id_out);
+int gx_system_remove(gx_batch* b, uint64_t id);
+/* Bytes a system of n particles would add to the batch. */
+int gx_system_bytes(const gx_batch* b, size_t n, size_t* bytes_out);
+/* Advance every live system by `steps` KDK steps of its own dt. */
+int gx_batch_step(gx_batch* b, uint64_t steps);
+int gx_system_snapshot(gx_batch* b, uint64_t id, double* pos_out, double* vel_out, double* time_out);
+int gx_system_len(const gx_batch* b, uint64_t id, size_t* n_out);
+int gx_batch_stats_get(const gx_batch* b, gx_batch_stats* out);
+/* Capture one batched step as a CUDA graph and replay it (1) or launch eagerly (0). */
+int gx_batch_set_graph(gx_batch* b, int enable);
+
+/* ---- seeded initial conditions (the reference's ic/ crate as input generator) -- */
+/* Plummer::sample (ic/src/plummer.rs:94-140): G, total mass M, scale radius a; seed. */
+int gx_ic_plummer(size_t n, uint64_t seed, double g, double total_mass, double scale_radius, double* pos,
+                  double* vel, double* mass);
+/* Composite disk galaxy pair on a parabolic orbit: halo (60% of particles), exponential
+ * disk (35%), Hernquist bulge (5%) per galaxy; mass_ratio m2/m1; pericentre in units
+ * of the disk scale length; inclinations in degrees. n_total particles. */
+int gx_ic_collision(size_t n_total, uint64_t seed, double mass_ratio, double pericentre, double incl1_deg,
+                    double incl2_deg, double* pos, double* vel, double* mass);
+/* A single disk + halo galaxy (no bulge) of n particles, total mass 1. */
+int gx_ic_disk_galaxy(size_t n, uint64_t seed, double* pos, double* vel, double* mass);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GALAXY_B200_H */
