@@ -322,6 +322,7 @@ void enqueue_force(gx_handle* h, const StepBufs& b, int kick, int pending, bool 
 int finish(gx_handle* h, bool timed) {
   GX_CK(h, cudaStreamSynchronize(h->stream));
   GX_CK(h, cudaGetLastError());
+  if (!h->ar.b.ctl) return GX_OK;  // nothing allocated yet (empty system)
   DevCtl ctl;
   GX_CK(h, cudaMemcpy(&ctl, h->ar.b.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost));
   if (timed) {

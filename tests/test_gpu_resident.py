@@ -99,7 +99,10 @@ def test_energy_conservation_plummer_config():
     r.step_many(1e-3, 100)
     e1 = r.diagnostics(True)
     assert abs(e1["total"] - e0["total"]) < 1e-3 * abs(e0["total"])
-    assert np.linalg.norm(e1["momentum"]) < 1e-6
+    # Barnes-Hut forces are not pairwise antisymmetric: momentum drifts at the force-error level.
+    snap = r.snapshot()
+    scale = float((np.linalg.norm(snap.vel, axis=1) * snap.mass).sum())
+    assert np.linalg.norm(e1["momentum"]) < 1e-4 * scale
     assert abs(r.time() - 0.1) < 1e-12
 
 
