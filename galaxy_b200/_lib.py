@@ -103,6 +103,7 @@ SIGNATURES = {
     "gx_kdk_step_host": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, C.POINTER(_i), _d]),
     "gx_host_alloc": (_i, [_sz, C.POINTER(_vp)]),
     "gx_host_free": (None, [_vp]),
+    "gx_sort_noalloc": (_i, [_vp, _vp, _vp, _sz, _vp]),
     "gx_stage_morton": (_i, [_vp, _sz, _vp, _vp, _vp, _vp]),
     "gx_stage_sort": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_stage_build": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

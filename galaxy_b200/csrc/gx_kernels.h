@@ -67,6 +67,11 @@ void launch_kick_half(const StepBufs& b, cudaStream_t st);
 void launch_morton_hist(const StepBufs& b, uint32_t* lanes_out, cudaStream_t st);
 // gx_sort.cu: the four onesweep passes (codes, iota) -> (codes sorted, order)
 void launch_sort(const StepBufs& b, cudaStream_t st);
+// the four passes on explicit buffers: keys_in -> (keys_out, vals_out), values start as
+// the identity; keys_tmp/vals_tmp hold passes 0 and 2
+void launch_sort_passes(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_tmp,
+                        uint32_t* vals_tmp, const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist,
+                        uint32_t* status, uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st);
 // per-system digit histograms of b.codes (when codes come from the host)
 void launch_code_hist(const StepBufs& b, cudaStream_t st);
 // gx_build.cu: gather leaves + bottom-up Karras build and aggregation

@@ -193,6 +193,18 @@ __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __re
     if (sh[i]) atomicAdd(&hs[i], sh[i]);
 }
 
+void launch_sort_passes(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_tmp,
+                        uint32_t* vals_tmp, const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist,
+                        uint32_t* status, uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
+  const uint32_t* kin[kRadixPasses] = {keys_in, keys_tmp, keys_out, keys_tmp};
+  uint32_t* kout[kRadixPasses] = {keys_tmp, keys_out, keys_tmp, keys_out};
+  const uint32_t* vin[kRadixPasses] = {nullptr, vals_tmp, vals_out, vals_tmp};
+  uint32_t* vout[kRadixPasses] = {vals_tmp, vals_out, vals_tmp, vals_out};
+  for (int p = 0; p < kRadixPasses; ++p)
+    k_onesweep<<<ntiles, kTileThreads, 0, st>>>(p, kin[p], vin[p], kout[p], vout[p], tiles, sys, hist, status,
+                                                 counters, ntiles, ctl);
+}
+
 void launch_code_hist(const StepBufs& b, cudaStream_t st) {
   k_code_hist<<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.codes, b.hist);
 }

@@ -153,6 +153,23 @@ int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const d
                    const double* sorted_mass, uint32_t* left, uint32_t* right, uint32_t* parent, double* aabb_min,
                    double* aabb_max, double* com, double* mass, double* quad_out);
 
+/* ---- sort without device allocation ------------------------------------------- */
+/* No counterpart in the reference. For callers that may not allocate device memory
+ * (an application that owns every device buffer through its own pool, a real-time
+ * loop that must not allocate after start-up, a plugin host that hands over buffers
+ * but no allocation rights): the stable (code, index) radix sort of gx_stage_sort on
+ * caller-owned DEVICE buffers -- d_codes[n] in, d_sorted_codes[n] and d_order[n] out,
+ * the order starting from the identity -- with all working memory in one static
+ * device array of the library (about 9 MiB per GPU, held until the process exits).
+ * n may not exceed GX_NOALLOC_MAX_KEYS (GX_ERR_CAPACITY otherwise). Enqueued on
+ * `stream` (a cudaStream_t; NULL = default stream) and waited for before returning.
+ * Calls no cudaMalloc/cudaFree. The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the array: calls overlapping on one GPU race and must be
+ * serialised by the caller. Errors: gx_last_error(NULL). */
+#define GX_NOALLOC_MAX_KEYS (1u << 20)
+int gx_sort_noalloc(const uint32_t* d_codes, uint32_t* d_sorted_codes, uint32_t* d_order, size_t n, void* stream);
+
 /* ---- batched systems (one launch per stage over many independent systems) ----- */
 typedef struct gx_batch gx_batch;
 
