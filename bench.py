@@ -256,7 +256,8 @@ def run_ours(args):
     counts_h = gb.GpuLbvh(1.0, p["eps"], p["theta"], device=local, stats=True)
     counts_h.accelerations(st)
     c = counts_h.stats()
-    counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"]}
+    counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"],
+              "warp_visits": c["warp_node_visits"], "f64_rechecks": c["f64_rechecks"]}
     alg = algorithmic(n, counts)
     walk_s = stage["ms_walk"] / 1e3
     sm_clock = (clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0))
@@ -272,6 +273,7 @@ def run_ours(args):
                                "(MEASURED_PEAKS.json has no FP32 figure); no tensor-core work in this path",
                 "flops_per_launch": alg["walk_flops"], "ms_per_launch": stage["ms_walk"],
                 "interactions_per_particle": (counts["leaf"] + counts["far"]) / n,
+                "lane_utilisation": (counts["leaf"] + counts["far"] + counts["open"]) / (64.0 * counts["warp_visits"]),
                 "hbm_stages": {
                     "sort (4 onesweep passes)": {"achieved_gbs": sort_gbs, "frac": sort_gbs / hbm,
                                                  "ms": stage["ms_sort"], "bytes": 4 * alg["sort_pass"]},

@@ -83,9 +83,9 @@ size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
   size_t s = 0;
   s += 3 * 3 * n * 8 + n * 8;                 // pos, vel, acc, mass
   s += 4 * n * 4;                             // codes, keys_alt, order, vals_alt
-  s += n * (32 + 16 + 16);                    // leaf64, leafA, leafB
+  s += n * 32 + 2 * n * 64;                   // leaf64, walk records (leaves + internal)
   s += n * 8 + 2 * n * 4 + n * sizeof(Agg64); // kids, parent, agg64
-  s += 4 * n * 16;                            // nodeA..D
+  s += n * 16;                                // nodeD
   s += n * 8;                                 // slots
   if (quad) s += 2 * n * 16 + 6 * n * 8;
   if (f64rec) s += n * sizeof(Node64);
@@ -129,14 +129,10 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   GX_A(b.order, nn, uint32_t);
   GX_A(b.vals_alt, nn, uint32_t);
   GX_A(b.leaf64, nn, double4);
-  GX_A(b.leafA, nn, float4);
-  GX_A(b.leafB, nn, float4);
+  GX_A(b.rec, 8 * nn, float4);  // 4 per unified node, 2n nodes
   GX_A(b.kids, nn, uint2);
   GX_A(b.parent, 2 * nn, uint32_t);
   GX_A(b.agg64, nn, Agg64);
-  GX_A(b.nodeA, nn, float4);
-  GX_A(b.nodeB, nn, float4);
-  GX_A(b.nodeC, nn, float4);
   GX_A(b.nodeD, nn, float4);
   if (q) {
     GX_A(b.nodeQ, 2 * nn, float4);
@@ -778,8 +774,8 @@ int gx_stage_morton(gx_handle* h, size_t n, const double* pos, uint32_t* lanes_o
   GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   GX_CK(h, cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, h->stream));
   launch_kick_drift_bbox(b, 0, 0, h->stream);
-  // Lanes (3n u32) are staged in leafA (n float4 = 4n u32), unused by this stage.
-  uint32_t* d_lanes = lanes_out ? reinterpret_cast<uint32_t*>(b.leafA) : nullptr;
+  // Lanes (3n u32) are staged in the walk records, unused by this stage.
+  uint32_t* d_lanes = lanes_out ? reinterpret_cast<uint32_t*>(b.rec) : nullptr;
   launch_morton_hist(b, d_lanes, h->stream);
   GX_CK(h, cudaMemcpyAsync(codes_out, b.codes, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   if (lanes_out)
@@ -838,6 +834,7 @@ int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const d
   GX_CK(h, cudaMemcpyAsync(b.pos, sorted_pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, sorted_mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   const int quad = h->opt.multipole == GX_MULTIPOLE_QUAD && h->opt.precision != GX_PREC_F64;
+  GX_CK(h, cudaMemsetAsync(b.bounds, 0, sizeof(Bounds), h->stream));  // no Morton stage here
   launch_build(b, quad, h->opt.precision == GX_PREC_F64, h->stream);
   std::vector<uint2> kids(n > 1 ? n - 1 : 1);
   std::vector<Agg64> agg(n > 1 ? n - 1 : 1);

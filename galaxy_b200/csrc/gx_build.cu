@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
   const SysDesc sd = sys[t.sys];
   const uint32_t off = sd.off, ns = sd.n;
   const double theta = sd.theta;
+  const double tiny2 = b.bounds[t.sys].tiny2;
   for (uint32_t k = t.begin + threadIdx.x; k < t.end; k += kTileThreads) {
     // ---- leaf: gather the particle into sorted order ----
     const uint32_t o = order[k];
@@ -85,8 +86,10 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
       float h[3], l[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) split_ff(cur.com[c], h[c], l[c]);
-      b.leafA[k] = make_float4(h[0], h[1], h[2], __double2float_rn(cur.m));
-      b.leafB[k] = make_float4(l[0], l[1], l[2], 0.f);
+      b.rec[4 * (size_t)k] = make_float4(h[0], h[1], h[2], __double2float_rn(cur.m));
+      // Take threshold -1: below any squared distance, so the walk always takes a leaf
+      // as a term (the reference's leaf rule) without an opening test.
+      b.rec[4 * (size_t)k + 1] = make_float4(l[0], l[1], l[2], -1.f);
     }
     if (ns == 1) {
       b.parent[k] = kNoParent;
@@ -140,17 +143,25 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
         }
         const double delta = dsqrt(dlen2(dv[0], dv[1], dv[2]));
         const double s = dmul(2.0, fmax(hf[0], fmax(hf[1], hf[2])));
-        float rcrit2 = __int_as_float(0x7fffffff);  // NaN: always re-decided in FP64
+        // Opening thresholds on d^2 for the FP32 walk: take the monopole above
+        // rcrit^2 (1 + band) + tiny2, open below rcrit^2 (1 - band) - tiny2, and
+        // re-decide in FP64 in between, with rcrit = s/theta + delta. NaN (theta = 0
+        // or a zero-size node) sends every visit to the FP64 re-check.
+        float take = __int_as_float(0x7fffffff), open = __int_as_float(0x7fffffff);
         if (theta > 0.0 && s > 0.0) {
           const double rc = s / theta + delta;
-          rcrit2 = __double2float_rn(rc * rc);
+          const double rc2 = rc * rc;
+          take = __double2float_ru(rc2 * (1.0 + kOpenBand) + tiny2);
+          open = __double2float_rd(rc2 * (1.0 - kOpenBand) - tiny2);
         }
         float hh[3], ll[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) split_ff(cur.com[c], hh[c], ll[c]);
-        b.nodeA[gi] = make_float4(hh[0], hh[1], hh[2], __double2float_rn(cur.m));
-        b.nodeB[gi] = make_float4(ll[0], ll[1], ll[2], rcrit2);
-        b.nodeC[gi] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
+        float4* rp = b.rec + 4 * (size_t)u;
+        rp[0] = make_float4(hh[0], hh[1], hh[2], __double2float_rn(cur.m));
+        rp[1] = make_float4(ll[0], ll[1], ll[2], take);
+        rp[2] = make_float4(__uint_as_float(lc), __uint_as_float(rc), open, 0.f);
+        rp[3] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
         b.nodeD[gi] = make_float4(__double2float_rn(hf[0]), __double2float_rn(hf[1]), __double2float_rn(hf[2]), 0.f);
         if (f64rec) {
           Node64 nd;

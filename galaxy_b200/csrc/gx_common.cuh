@@ -7,16 +7,17 @@
 //   Morton codes code[N] (u32), the sort's ping-pong (key, index) buffers.
 //   sorted leaves (leaf k = k-th particle in (code, index) order):
 //     leaf64[k] = double4(x, y, z, m)          FP64 payload for folds and rechecks
-//     leafA[k]  = float4(x_hi, y_hi, z_hi, m)  FP32 walk record
-//     leafB[k]  = float4(x_lo, y_lo, z_lo, 0)  low words of the float-float split
 //     order[k]  original index
+//   walk records, 4 float4 per unified node u (leaves [0, N), internal i at N + i):
+//     rec[4u+0] = (com_hi.xyz, mass)     float-float split of the centre of mass
+//     rec[4u+1] = (com_lo.xyz, take)     take: d^2 threshold to take the monopole
+//     rec[4u+2] = (left, right, open, 0) children and the d^2 threshold to open
+//     rec[4u+3] = (center.xyz, 0)        AABB centre (opening test, theta >= 1/sqrt 3)
 //   internal node i (Karras numbering, unified index N + i):
 //     kids[i]   = uint2(left, right) unified children
 //     parent[u] unified parent of every node (root: 0xFFFFFFFF)
 //     agg64[i]  = {aabb_min[3], aabb_max[3], com[3], mass} FP64 (bit-exact fold)
-//     nodeA[i]  = float4(com_hi.xyz, mass)
-//     nodeB[i]  = float4(com_lo.xyz, rcrit2)   rcrit2 = (s/theta + delta)^2
-//     nodeC[i]  = float4(center.xyz, 0), nodeD[i] = float4(half.xyz, 0)  (theta >= 1/sqrt 3)
+//     nodeD[i]  = float4(half.xyz, 0)  AABB half extents (theta >= 1/sqrt 3)
 //     nodeQ[i]  = 2 x float4 traceless quadrupole (xx, xy, xz, yy), (yz, zz, 0, 0)
 //     node64[i] = {center[3], half[3], com[3], mass, delta, s}  FP64 walk record
 #pragma once
@@ -32,6 +33,10 @@ constexpr uint64_t kEmptySlot = 0xFFFFFFFFFFFFFFFFull;
 // Bounded waits: every spin in these kernels gives up after this many polls,
 // raises the device error word and carries on, so no kernel can hang the GPU.
 constexpr uint32_t kSpinLimit = 1u << 24;
+
+// Relative guard band of the FP32 opening test: within it the decision is re-made in
+// FP64 with the reference's expression (FP32 d^2 carries <= ~1e-6 relative error).
+constexpr double kOpenBand = 4e-6;
 
 // Device error word bits (read back by the host after each call).
 constexpr uint32_t kErrLookbackTimeout = 1u << 0;

@@ -34,16 +34,16 @@ struct StepBufs {
   uint32_t* vals_alt = nullptr;
   // leaves, sorted order
   double4* leaf64 = nullptr;
-  float4* leafA = nullptr;
-  float4* leafB = nullptr;
+  // Walk records, 4 float4 per unified node u (leaves [0, n), internal node i at n + i):
+  //   rec[4u+0] = (com_hi.xyz, mass)       rec[4u+1] = (com_lo.xyz, take threshold)
+  //   rec[4u+2] = (left, right, open threshold, 0)   rec[4u+3] = (center.xyz, 0)
+  // A leaf has only the first two (take threshold -1: always a term).
+  float4* rec = nullptr;
   // internal nodes
   uint2* kids = nullptr;
   uint32_t* parent = nullptr;
   Agg64* agg64 = nullptr;
-  float4* nodeA = nullptr;
-  float4* nodeB = nullptr;
-  float4* nodeC = nullptr;
-  float4* nodeD = nullptr;
+  float4* nodeD = nullptr;   // half extents (opening test for theta >= 1/sqrt 3)
   float4* nodeQ = nullptr;   // 2 per node (quadrupole mode)
   double* q64 = nullptr;     // 6 per node (quadrupole mode)
   Node64* node64 = nullptr;  // FP64 walk mode

@@ -7,13 +7,12 @@
 // opened) and :673-675 (result times G).
 //
 // One warp walks the tree for 32 Morton-consecutive targets of one system. The warp
-// visits the union of the 32 per-target walks in depth-first, left-before-right
-// order (an explicit stack of (node, lane mask) pairs kept in registers, entry j in
-// lane j % 32); every node record is loaded once per warp (a broadcast load) and
-// each lane applies its OWN opening decision, so the sequence of terms a lane adds
-// is exactly the reference's skip-pointer walk for that target. A tree over 30-bit
-// codes with a 32-bit position tie-break is at most 63 levels deep, so 64 stack
-// entries always suffice (overflow raises the device error word).
+// visits the union of the 32 per-target walks (an explicit stack of (node, lane mask)
+// pairs kept in registers, entry j in lane j % 32); every node record is loaded once
+// per warp (a broadcast load) and each lane applies its OWN opening decision, so
+// every lane takes exactly the reference's set of terms for its target. A tree over
+// 30-bit codes with a 32-bit position tie-break is at most 63 levels deep, so 64
+// stack entries always suffice (overflow raises the device error word).
 //
 // FP32 mode: node centres of mass and leaf positions are float-float (hi + lo), so
 // dx = (c_hi - x_hi) + (c_lo - x_lo) keeps ~48 bits of the f64 coordinates; the
@@ -22,15 +21,14 @@
 // relative 4e-6 band of the threshold (or touches the AABB within 2^-20), so every
 // opening decision equals the reference's. Terms are accumulated in FP32 with Kahan
 // compensation.
-// FP64 mode: the reference's arithmetic, operation for operation, so accelerations
-// are bit-identical to the reference's CPU walk on the same tree.
+// FP64 mode: the reference's arithmetic, operation for operation and in its
+// depth-first order, so accelerations are bit-identical to the reference's CPU walk.
 #include "gx_kernels.h"
 
 namespace gx {
 
 namespace {
 
-constexpr float kBand = 4e-6f;
 
 struct Acc32 {
   float s[3], c[3];
@@ -105,6 +103,42 @@ __device__ __forceinline__ void stack_pop(WarpStack& s, uint32_t& u, uint32_t& m
   m = __shfl_sync(0xffffffffu, lo ? s.m0 : s.m1, src);
 }
 
+// Stack of child pairs still to decide: (left child, right child, lane mask), entry
+// j in lane j % 32 of the (x0, y0, m0) or (x1, y1, m1) registers.
+struct PairStack {
+  uint32_t x0, y0, m0, x1, y1, m1;
+  int sp;
+};
+
+__device__ __forceinline__ bool pair_push(PairStack& s, uint2 kd, uint32_t m, int lane) {
+  if (s.sp < 32) {
+    if (lane == s.sp) {
+      s.x0 = kd.x;
+      s.y0 = kd.y;
+      s.m0 = m;
+    }
+  } else if (s.sp < 64) {
+    if (lane == s.sp - 32) {
+      s.x1 = kd.x;
+      s.y1 = kd.y;
+      s.m1 = m;
+    }
+  } else {
+    return false;
+  }
+  ++s.sp;
+  return true;
+}
+
+__device__ __forceinline__ void pair_pop(PairStack& s, uint2& kd, uint32_t& m) {
+  --s.sp;
+  const int src = s.sp & 31;
+  const bool lo = s.sp < 32;
+  kd.x = __shfl_sync(0xffffffffu, lo ? s.x0 : s.x1, src);
+  kd.y = __shfl_sync(0xffffffffu, lo ? s.y0 : s.y1, src);
+  m = __shfl_sync(0xffffffffu, lo ? s.m0 : s.m1, src);
+}
+
 __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -113,8 +147,11 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 
 }  // namespace
 
-template <int F64, bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
-__global__ void __launch_bounds__(256) k_walk(StepBufs b, int persistent) {
+// Exact FP64 walk: one node per warp iteration in strict depth-first, left-before-right
+// order, so each lane adds its terms in the reference's order with the reference's
+// arithmetic.
+template <bool STATS>
+__global__ void __launch_bounds__(256) k_walk_f64(StepBufs b, int persistent) {
   const int lane = threadIdx.x & 31;
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
   uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -125,9 +162,7 @@ __global__ void __launch_bounds__(256) k_walk(StepBufs b, int persistent) {
     const uint32_t end = sd.off + sd.n;
     const uint32_t k = it.begin + lane;
     const bool valid = k < end;
-    const double g = sd.g;
     if (sd.n == 1) {
-      // A lone particle feels no force (its only leaf is itself).
       if (valid) {
         const uint32_t o = b.order[k];
 #pragma unroll
@@ -135,37 +170,21 @@ __global__ void __launch_bounds__(256) k_walk(StepBufs b, int persistent) {
       }
     } else {
       const double eps2 = dmul(sd.eps, sd.eps);
-      const float eps2f = __double2float_rn(eps2);
       const double theta = sd.theta;
-      const float tiny2 = b.bounds[it.sys].tiny2;
       double x64[3] = {0, 0, 0};
-      float xh[3] = {0, 0, 0}, xl[3] = {0, 0, 0};
       if (valid) {
         const double4 p = b.leaf64[k];
         x64[0] = p.x;
         x64[1] = p.y;
         x64[2] = p.z;
-        if (!F64) {
-          const float4 ha = b.leafA[k], hb = b.leafB[k];
-          xh[0] = ha.x;
-          xh[1] = ha.y;
-          xh[2] = ha.z;
-          xl[0] = hb.x;
-          xl[1] = hb.y;
-          xl[2] = hb.z;
-        }
       }
-      Acc32 a32 = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
       double a64[3] = {0.0, 0.0, 0.0};
-      unsigned long long n_leaf = 0, n_far = 0, n_open = 0, n_re = 0, n_vis = 0;
-
+      unsigned long long n_leaf = 0, n_far = 0, n_open = 0, n_vis = 0;
       WarpStack stk{0, 0, 0, 0, 0};
-      uint32_t u = n_total + sd.off;  // root: internal node 0 of this system
+      uint32_t u = n_total + sd.off;
       uint32_t mask = __ballot_sync(0xffffffffu, valid);
-      // Each node is reached at most once per warp (only through its parent), so a
-      // walk longer than the system's node count means a corrupt tree: stop, flag.
       const uint32_t max_iters = 2u * sd.n + 64u;
-      const uint32_t int_lo = n_total + sd.off, int_hi = n_total + sd.off + sd.n - 1;
+      const uint32_t int_lo = n_total + sd.off, int_n = sd.n - 1;
       uint32_t iters = 0;
       for (;;) {
         if (++iters > max_iters) {
@@ -175,131 +194,46 @@ __global__ void __launch_bounds__(256) k_walk(StepBufs b, int persistent) {
         if (STATS) ++n_vis;
         const bool active = (mask >> lane) & 1u;
         if (u < n_total) {
-          // ---- leaf u (sorted index) ----
-          if (F64) {
-            const double4 p = b.leaf64[u];
-            if (active && u != k && p.w > 0.0) {
-              const double dx = dsub(p.x, x64[0]), dy = dsub(p.y, x64[1]), dz = dsub(p.z, x64[2]);
-              const double r2 = dadd(dlen2(dx, dy, dz), eps2);
-              const double f = ddiv(p.w, dmul(r2, dsqrt(r2)));
+          const double4 p = b.leaf64[u];
+          if (active && u != k && p.w > 0.0) {
+            const double dx = dsub(p.x, x64[0]), dy = dsub(p.y, x64[1]), dz = dsub(p.z, x64[2]);
+            const double r2 = dadd(dlen2(dx, dy, dz), eps2);
+            const double f = ddiv(p.w, dmul(r2, dsqrt(r2)));
+            a64[0] = dadd(a64[0], dmul(dx, f));
+            a64[1] = dadd(a64[1], dmul(dy, f));
+            a64[2] = dadd(a64[2], dmul(dz, f));
+            if (STATS) ++n_leaf;
+          }
+        } else {
+          const uint32_t gi = u - n_total;
+          bool open = false;
+          const Node64 nd = b.node64[gi];
+          if (active && nd.m > 0.0) {
+            bool inside = true;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) inside = inside && (fabs(dsub(x64[c], nd.c[c])) <= nd.h[c]);
+            const double dx = dsub(nd.com[0], x64[0]), dy = dsub(nd.com[1], x64[1]), dz = dsub(nd.com[2], x64[2]);
+            const double d2 = dlen2(dx, dy, dz);
+            const double d = dsqrt(d2);
+            if (!inside && dmul(theta, dsub(d, nd.delta)) >= nd.s) {
+              const double r2 = dadd(d2, eps2);
+              const double f = ddiv(nd.m, dmul(r2, dsqrt(r2)));
               a64[0] = dadd(a64[0], dmul(dx, f));
               a64[1] = dadd(a64[1], dmul(dy, f));
               a64[2] = dadd(a64[2], dmul(dz, f));
-              if (STATS) ++n_leaf;
-            }
-          } else {
-            const float4 la = __ldg(&b.leafA[u]);
-            const float4 lb = __ldg(&b.leafB[u]);
-            if (active && u != k && la.w > 0.f) {
-              const float dx = (la.x - xh[0]) + (lb.x - xl[0]);
-              const float dy = (la.y - xh[1]) + (lb.y - xl[1]);
-              const float dz = (la.z - xh[2]) + (lb.z - xl[2]);
-              const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2f)));
-              const float inv = rsqrtf(r2);
-              const float f = la.w * inv * inv * inv;
-              acc_add<KAHAN>(a32, dx * f, dy * f, dz * f);
-              if (STATS) ++n_leaf;
-            }
-          }
-        } else {
-          // ---- internal node gi ----
-          const uint32_t gi = u - n_total;
-          bool open = false;
-          if (F64) {
-            const Node64 nd = b.node64[gi];
-            if (active && nd.m > 0.0) {
-              bool inside = true;
-#pragma unroll
-              for (int c = 0; c < 3; ++c) inside = inside && (fabs(dsub(x64[c], nd.c[c])) <= nd.h[c]);
-              const double dx = dsub(nd.com[0], x64[0]), dy = dsub(nd.com[1], x64[1]), dz = dsub(nd.com[2], x64[2]);
-              const double d2 = dlen2(dx, dy, dz);
-              const double d = dsqrt(d2);
-              if (!inside && dmul(theta, dsub(d, nd.delta)) >= nd.s) {
-                const double r2 = dadd(d2, eps2);
-                const double f = ddiv(nd.m, dmul(r2, dsqrt(r2)));
-                a64[0] = dadd(a64[0], dmul(dx, f));
-                a64[1] = dadd(a64[1], dmul(dy, f));
-                a64[2] = dadd(a64[2], dmul(dz, f));
-                if (STATS) ++n_far;
-              } else {
-                open = true;
-              }
-            }
-          } else {
-            const float4 na = __ldg(&b.nodeA[gi]);
-            const float4 nb = __ldg(&b.nodeB[gi]);
-            if (active && na.w > 0.f) {
-              const float dx = (na.x - xh[0]) + (nb.x - xl[0]);
-              const float dy = (na.y - xh[1]) + (nb.y - xl[1]);
-              const float dz = (na.z - xh[2]) + (nb.z - xl[2]);
-              const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-              const float rc2 = nb.w;
-              int dec;  // 1 accept, 0 open, 2 undecided in FP32
-              if (d2 > fmaf(rc2, kBand, rc2) + tiny2)
-                dec = 1;
-              else if (d2 < fmaf(rc2, -kBand, rc2) - tiny2)
-                dec = 0;
-              else
-                dec = 2;
-              if (INSIDE && dec == 1) {
-                const float4 nc = __ldg(&b.nodeC[gi]);
-                const float4 nd4 = __ldg(&b.nodeD[gi]);
-                const float q0 = fabsf(xh[0] - nc.x) - nd4.x;
-                const float q1 = fabsf(xh[1] - nc.y) - nd4.y;
-                const float q2 = fabsf(xh[2] - nc.z) - nd4.z;
-                const float t0 = 0x1p-20f * (fabsf(nc.x) + nd4.x) + 1e-30f;
-                const float t1 = 0x1p-20f * (fabsf(nc.y) + nd4.y) + 1e-30f;
-                const float t2 = 0x1p-20f * (fabsf(nc.z) + nd4.z) + 1e-30f;
-                if (fabsf(q0) <= t0 || fabsf(q1) <= t1 || fabsf(q2) <= t2)
-                  dec = 2;
-                else if (q0 < 0.f && q1 < 0.f && q2 < 0.f)
-                  dec = 0;  // clearly inside: open
-              }
-              if (dec == 2) {
-                dec = exact_accept(b.agg64, gi, x64, theta) ? 1 : 0;
-                if (STATS) ++n_re;
-              }
-              if (dec == 1) {
-                const float r2 = d2 + eps2f;
-                const float inv = rsqrtf(r2);
-                const float inv2 = inv * inv;
-                const float inv3 = inv * inv2;
-                const float f = na.w * inv3;
-                float tx = dx * f, ty = dy * f, tz = dz * f;
-                if (QUAD) {
-                  const float4 qa = __ldg(&b.nodeQ[2 * (size_t)gi]);
-                  const float4 qb = __ldg(&b.nodeQ[2 * (size_t)gi + 1]);
-                  // r = x - com = -d; a += Q r / r^5 - 2.5 (r.Q r) r / r^7
-                  const float rx = -dx, ry = -dy, rz = -dz;
-                  const float qx = qa.x * rx + qa.y * ry + qa.z * rz;
-                  const float qy = qa.y * rx + qa.w * ry + qb.x * rz;
-                  const float qz = qa.z * rx + qb.x * ry + qb.y * rz;
-                  const float rqr = rx * qx + ry * qy + rz * qz;
-                  const float inv5 = inv3 * inv2;
-                  const float c7 = 2.5f * rqr * inv5 * inv2;
-                  tx += qx * inv5 - rx * c7;
-                  ty += qy * inv5 - ry * c7;
-                  tz += qz * inv5 - rz * c7;
-                }
-                acc_add<KAHAN>(a32, tx, ty, tz);
-                if (STATS) ++n_far;
-              } else {
-                open = true;
-              }
+              if (STATS) ++n_far;
+            } else {
+              open = true;
             }
           }
           const uint32_t open_mask = __ballot_sync(0xffffffffu, open);
           if (open_mask) {
             if (STATS && open) ++n_open;
             const uint2 kd = __ldg(&b.kids[gi]);
-            const bool kx_ok = (kd.x >= sd.off && kd.x < end) || (kd.x >= int_lo && kd.x < int_hi);
-            const bool ky_ok = (kd.y >= sd.off && kd.y < end) || (kd.y >= int_lo && kd.y < int_hi);
-            if (!kx_ok || !ky_ok) {
-              if (lane == 0) raise_err(b.ctl, kErrBadIndex);
-              break;
-            }
-            if (!stack_push(stk, kd.y, open_mask, lane)) {
-              if (lane == 0) raise_err(b.ctl, kErrStackOverflow);
+            const bool kx_ok = (kd.x - sd.off) < sd.n || (kd.x - int_lo) < int_n;
+            const bool ky_ok = (kd.y - sd.off) < sd.n || (kd.y - int_lo) < int_n;
+            if (!kx_ok || !ky_ok || !stack_push(stk, kd.y, open_mask, lane)) {
+              if (lane == 0) raise_err(b.ctl, kx_ok && ky_ok ? kErrStackOverflow : kErrBadIndex);
               break;
             }
             u = kd.x;
@@ -312,32 +246,21 @@ __global__ void __launch_bounds__(256) k_walk(StepBufs b, int persistent) {
       }
       if (valid) {
         const uint32_t o = b.order[k];
-        if (F64) {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) b.acc[3 * (size_t)o + c] = dmul(a64[c], g);
-        } else {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const float v = KAHAN ? __fsub_rn(a32.s[c], a32.c[c]) : a32.s[c];
-            b.acc[3 * (size_t)o + c] = dmul(static_cast<double>(v), g);
-          }
-        }
+        for (int c = 0; c < 3; ++c) b.acc[3 * (size_t)o + c] = dmul(a64[c], sd.g);
       }
       if (STATS) {
         n_leaf = warp_sum64(n_leaf);
         n_far = warp_sum64(n_far);
         n_open = warp_sum64(n_open);
-        n_re = warp_sum64(n_re);
         if (lane == 0) {
           atomicAdd(&b.ctl->stats[0], n_leaf);
           atomicAdd(&b.ctl->stats[1], n_far);
           atomicAdd(&b.ctl->stats[2], n_open);
-          atomicAdd(&b.ctl->stats[3], n_re);
           atomicAdd(&b.ctl->stats[4], n_vis);
         }
       }
     }
-    // next item
     if (persistent) {
       uint32_t nxt = 0;
       if (lane == 0) nxt = atomicAdd(&b.counters[4], 1u) + warps_total;
@@ -350,30 +273,281 @@ __global__ void __launch_bounds__(256) k_walk(StepBufs b, int persistent) {
 
 namespace {
 
-template <int F64, bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
-void launch_walk_t(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
-  const int block = cfg.block > 0 ? cfg.block : 256;
-  const int wpb = block / 32;
-  if (cfg.persistent_ctas > 0) {
-    k_walk<F64, QUAD, KAHAN, STATS, INSIDE><<<cfg.persistent_ctas, block, 0, st>>>(b, 1);
-  } else {
-    const uint32_t grid = (b.nitems + wpb - 1) / wpb;
-    if (grid) k_walk<F64, QUAD, KAHAN, STATS, INSIDE><<<grid, block, 0, st>>>(b, 0);
+// Per-lane state of the FP32 walk.
+struct Lane32 {
+  float xh[3], xl[3];
+  uint32_t k;
+  float eps2f;
+  double theta;
+};
+
+// FP32 opening decision state of one child for one lane.
+struct Child32 {
+  float dx, dy, dz, d2;
+  bool take, open, amb;
+};
+
+// Distance and threshold tests of node u (A = rec[4u], B = rec[4u+1], open_thr =
+// rec[4u+2].z, -2 for leaves) for a lane; no branches. take: a term; open: descend;
+// amb: the FP32 value is inside the guard band and must be re-decided in FP64.
+template <bool INSIDE>
+__device__ __forceinline__ Child32 classify(const StepBufs& b, const Lane32& L, bool act, uint32_t u,
+                                            const float4& A, const float4& B, float open_thr, uint32_t n_total) {
+  Child32 c;
+  c.dx = (A.x - L.xh[0]) + (B.x - L.xl[0]);
+  c.dy = (A.y - L.xh[1]) + (B.y - L.xl[1]);
+  c.dz = (A.z - L.xh[2]) + (B.z - L.xl[2]);
+  c.d2 = fmaf(c.dx, c.dx, fmaf(c.dy, c.dy, c.dz * c.dz));
+  // The target itself and massless subtrees are skipped (lbvh.rs:485-496).
+  const bool ok = act && (u != L.k) && (A.w > 0.f);
+  c.take = ok && (c.d2 > B.w);  // B.w: take threshold (-1 for leaves)
+  c.open = ok && (c.d2 < open_thr);
+  c.amb = ok && !c.take && !c.open;
+  if (INSIDE && u >= n_total) {
+    const float4 nc = __ldg(&b.rec[4 * (size_t)u + 3]);
+    const float4 nd4 = __ldg(&b.nodeD[u - n_total]);
+    const float q0 = fabsf(L.xh[0] - nc.x) - nd4.x;
+    const float q1 = fabsf(L.xh[1] - nc.y) - nd4.y;
+    const float q2 = fabsf(L.xh[2] - nc.z) - nd4.z;
+    const float t0 = 0x1p-20f * (fabsf(nc.x) + nd4.x) + 1e-30f;
+    const float t1 = 0x1p-20f * (fabsf(nc.y) + nd4.y) + 1e-30f;
+    const float t2 = 0x1p-20f * (fabsf(nc.z) + nd4.z) + 1e-30f;
+    const bool near_face = fabsf(q0) <= t0 || fabsf(q1) <= t1 || fabsf(q2) <= t2;
+    const bool inside = q0 < 0.f && q1 < 0.f && q2 < 0.f;
+    const bool t = c.take;
+    c.take = t && !near_face && !inside;
+    c.open = c.open || (t && !near_face && inside);
+    c.amb = c.amb || (t && near_face);
+  }
+  return c;
+}
+
+// The term of a taken node (Plummer-softened monopole, plus the quadrupole of an
+// internal node in QUAD mode), scaled by `take` (0 or 1) and added to t[].
+template <bool QUAD>
+__device__ __forceinline__ void add_term(const StepBufs& b, const Lane32& L, const Child32& c, bool take, float m,
+                                         uint32_t u, uint32_t n_total, float t[3]) {
+  const float r2 = c.d2 + L.eps2f;
+  const float inv = rsqrtf(r2);
+  const float inv2 = inv * inv;
+  const float inv3 = inv * inv2;
+  const float f = take ? m * inv3 : 0.f;
+  t[0] = fmaf(c.dx, f, t[0]);
+  t[1] = fmaf(c.dy, f, t[1]);
+  t[2] = fmaf(c.dz, f, t[2]);
+  if (QUAD && u >= n_total) {
+    const uint32_t gi = u - n_total;
+    const float4 qa = __ldg(&b.nodeQ[2 * (size_t)gi]);
+    const float4 qb = __ldg(&b.nodeQ[2 * (size_t)gi + 1]);
+    // r = x - com = -d;  a += Q r / r^5 - 2.5 (r.Q r) r / r^7
+    const float rx = -c.dx, ry = -c.dy, rz = -c.dz;
+    const float qx = qa.x * rx + qa.y * ry + qa.z * rz;
+    const float qy = qa.y * rx + qa.w * ry + qb.x * rz;
+    const float qz = qa.z * rx + qb.x * ry + qb.y * rz;
+    const float rqr = rx * qx + ry * qy + rz * qz;
+    const float inv5 = take ? inv3 * inv2 : 0.f;
+    const float c7 = 2.5f * rqr * inv5 * inv2;
+    t[0] += qx * inv5 - rx * c7;
+    t[1] += qy * inv5 - ry * c7;
+    t[2] += qz * inv5 - rz * c7;
   }
 }
 
-template <int F64, bool QUAD, bool KAHAN>
-void dispatch_si(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
+__device__ __forceinline__ void resolve_amb(const StepBufs& b, const Lane32& L, Child32& c, uint32_t u,
+                                            uint32_t n_total) {
+  if (c.amb) {
+    const double4 p = b.leaf64[L.k];
+    const double x[3] = {p.x, p.y, p.z};
+    const bool acc = exact_accept(b.agg64, u - n_total, x, L.theta);
+    c.take = acc;
+    c.open = !acc;
+  }
+}
+
+}  // namespace
+
+// FP32 walk: each iteration decides the two children of one opened node for every
+// lane that opened it; their terms are summed and added to the lane's Kahan-
+// compensated accumulator. A node's record carries its children and both FP32
+// thresholds, so the next pair to decide is known from the records just loaded (one
+// dependent load per iteration), and the stack holds ready-to-load child pairs. The
+// decisions are predicated (no per-lane branches); the rare FP64 re-check runs only
+// when some lane of the warp needs it. Indices are clamped into the record array, so
+// even a corrupt tree cannot read out of bounds; a clamp or an exhausted iteration
+// budget raises the device error word. Each lane takes exactly the reference's set of
+// terms; only the order of summation differs from the FP64 walk.
+template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
+__global__ void __launch_bounds__(256, 3) k_walk_f32(StepBufs b, int persistent) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
+  uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t n_total = b.n;
+  const uint32_t umax = 2 * n_total - 2;  // largest unified node index
+  const float4* __restrict__ rec = b.rec;
+  while (item < b.nitems) {
+    const WalkItem it = b.items[item];
+    const SysDesc sd = b.sys[it.sys];
+    const uint32_t end = sd.off + sd.n;
+    Lane32 L;
+    L.k = it.begin + lane;
+    const bool valid = L.k < end;
+    Acc32 acc = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    unsigned long long n_leaf = 0, n_far = 0, n_open = 0, n_re = 0, n_vis = 0;
+    const uint32_t root = n_total + sd.off;
+    bool bad = false;
+    // The root's box is the system's box, so every target is inside it and every lane
+    // opens it -- unless the whole system is massless, when nothing is added.
+    if (sd.n > 1 && __ldg(&rec[4 * (size_t)root]).w > 0.f) {
+      L.eps2f = __double2float_rn(dmul(sd.eps, sd.eps));
+      L.theta = sd.theta;
+      if (valid) {
+        const float4 ha = rec[4 * (size_t)L.k], hb = rec[4 * (size_t)L.k + 1];
+        L.xh[0] = ha.x;
+        L.xh[1] = ha.y;
+        L.xh[2] = ha.z;
+        L.xl[0] = hb.x;
+        L.xl[1] = hb.y;
+        L.xl[2] = hb.z;
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) L.xh[c] = L.xl[c] = 0.f;
+      }
+      uint32_t sx0 = 0, sy0 = 0, sm0 = 0, sx1 = 0, sy1 = 0, sm1 = 0;  // pair stack, entry j in lane j%32
+      int sp = 0;
+      const float4 r2 = __ldg(&rec[4 * (size_t)root + 2]);
+      uint32_t cx = __float_as_uint(r2.x), cy = __float_as_uint(r2.y);
+      uint32_t mask = __ballot_sync(0xffffffffu, valid);
+      const uint32_t max_iters = sd.n + 64u;
+      uint32_t iters = 0;
+      for (;;) {
+        bad |= (cx > umax) | (cy > umax);
+        if (++iters > max_iters) {
+          bad = true;
+          break;
+        }
+        cx = min(cx, umax);
+        cy = min(cy, umax);
+        if (STATS) ++n_vis;
+        const float4* p0 = rec + 4 * (size_t)cx;
+        const float4* p1 = rec + 4 * (size_t)cy;
+        const float4 a0 = __ldg(p0), b0 = __ldg(p0 + 1);
+        const float4 a1 = __ldg(p1), b1 = __ldg(p1 + 1);
+        const float4 k0 = cx >= n_total ? __ldg(p0 + 2) : make_float4(0.f, 0.f, -2.f, 0.f);
+        const float4 k1 = cy >= n_total ? __ldg(p1 + 2) : make_float4(0.f, 0.f, -2.f, 0.f);
+        const bool act = (mask >> lane) & 1u;
+        Child32 c0 = classify<INSIDE>(b, L, act, cx, a0, b0, k0.z, n_total);
+        Child32 c1 = classify<INSIDE>(b, L, act, cy, a1, b1, k1.z, n_total);
+        if (__any_sync(0xffffffffu, c0.amb || c1.amb)) {
+          if (STATS) n_re += (c0.amb ? 1 : 0) + (c1.amb ? 1 : 0);
+          resolve_amb(b, L, c0, cx, n_total);
+          resolve_amb(b, L, c1, cy, n_total);
+        }
+        float t[3] = {0.f, 0.f, 0.f};
+        add_term<QUAD>(b, L, c0, c0.take, a0.w, cx, n_total, t);
+        add_term<QUAD>(b, L, c1, c1.take, a1.w, cy, n_total, t);
+        acc_add<KAHAN>(acc, t[0], t[1], t[2]);
+        if (STATS) {
+          n_leaf += (c0.take && cx < n_total ? 1 : 0) + (c1.take && cy < n_total ? 1 : 0);
+          n_far += (c0.take && cx >= n_total ? 1 : 0) + (c1.take && cy >= n_total ? 1 : 0);
+          n_open += (c0.open ? 1 : 0) + (c1.open ? 1 : 0);
+        }
+        const uint32_t m0 = __ballot_sync(0xffffffffu, c0.open);
+        const uint32_t m1 = __ballot_sync(0xffffffffu, c1.open);
+        const uint32_t n0x = __float_as_uint(k0.x), n0y = __float_as_uint(k0.y);
+        const uint32_t n1x = __float_as_uint(k1.x), n1y = __float_as_uint(k1.y);
+        if (m0 && m1) {
+          // push the right child's pair; continue with the left child's
+          if (sp >= 64) {
+            bad = true;
+            break;
+          }
+          const bool w0 = lane == sp, w1 = lane == sp - 32;
+          sx0 = w0 ? n1x : sx0;
+          sy0 = w0 ? n1y : sy0;
+          sm0 = w0 ? m1 : sm0;
+          sx1 = w1 ? n1x : sx1;
+          sy1 = w1 ? n1y : sy1;
+          sm1 = w1 ? m1 : sm1;
+          ++sp;
+        }
+        if (m0) {
+          cx = n0x;
+          cy = n0y;
+          mask = m0;
+        } else if (m1) {
+          cx = n1x;
+          cy = n1y;
+          mask = m1;
+        } else {
+          if (sp == 0) break;
+          --sp;
+          const int src = sp & 31;
+          const bool lo = sp < 32;
+          cx = __shfl_sync(0xffffffffu, lo ? sx0 : sx1, src);
+          cy = __shfl_sync(0xffffffffu, lo ? sy0 : sy1, src);
+          mask = __shfl_sync(0xffffffffu, lo ? sm0 : sm1, src);
+        }
+      }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) raise_err(b.ctl, kErrBadIndex);
+    if (valid) {
+      const uint32_t o = b.order[L.k];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float v = KAHAN ? __fsub_rn(acc.s[c], acc.c[c]) : acc.s[c];
+        b.acc[3 * (size_t)o + c] = dmul(static_cast<double>(v), sd.g);
+      }
+    }
+    if (STATS) {
+      n_leaf = warp_sum64(n_leaf);
+      n_far = warp_sum64(n_far);
+      n_open = warp_sum64(n_open);
+      n_re = warp_sum64(n_re);
+      const uint32_t n_valid = __popc(__ballot_sync(0xffffffffu, valid));  // the root, opened by all
+      if (lane == 0) {
+        atomicAdd(&b.ctl->stats[0], n_leaf);
+        atomicAdd(&b.ctl->stats[1], n_far);
+        atomicAdd(&b.ctl->stats[2], n_open + (sd.n > 1 ? n_valid : 0u));
+        atomicAdd(&b.ctl->stats[3], n_re);
+        atomicAdd(&b.ctl->stats[4], n_vis);
+      }
+    }
+    if (persistent) {
+      uint32_t nxt = 0;
+      if (lane == 0) nxt = atomicAdd(&b.counters[4], 1u) + warps_total;
+      item = __shfl_sync(0xffffffffu, nxt, 0);
+    } else {
+      item = b.nitems;
+    }
+  }
+}
+
+namespace {
+
+template <class K>
+void launch_k(K kern, const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
+  const int block = cfg.block > 0 ? cfg.block : 256;
+  const int wpb = block / 32;
+  if (cfg.persistent_ctas > 0) {
+    kern<<<cfg.persistent_ctas, block, 0, st>>>(b, 1);
+  } else {
+    const uint32_t grid = (b.nitems + wpb - 1) / wpb;
+    if (grid) kern<<<grid, block, 0, st>>>(b, 0);
+  }
+}
+
+template <bool QUAD, bool KAHAN>
+void dispatch_f32(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
   if (cfg.stats) {
     if (cfg.inside_test)
-      launch_walk_t<F64, QUAD, KAHAN, true, true>(b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, true, true>, b, cfg, st);
     else
-      launch_walk_t<F64, QUAD, KAHAN, true, false>(b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, true, false>, b, cfg, st);
   } else {
     if (cfg.inside_test)
-      launch_walk_t<F64, QUAD, KAHAN, false, true>(b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, false, true>, b, cfg, st);
     else
-      launch_walk_t<F64, QUAD, KAHAN, false, false>(b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, false, false>, b, cfg, st);
   }
 }
 
@@ -383,17 +557,20 @@ void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
   if (cfg.precision == 1) {
     // The FP64 walk has no quadrupole or compensation variants: it is the
     // reference's arithmetic.
-    dispatch_si<1, false, false>(b, cfg, st);
+    if (cfg.stats)
+      launch_k(k_walk_f64<true>, b, cfg, st);
+    else
+      launch_k(k_walk_f64<false>, b, cfg, st);
   } else if (cfg.quad) {
     if (cfg.kahan)
-      dispatch_si<0, true, true>(b, cfg, st);
+      dispatch_f32<true, true>(b, cfg, st);
     else
-      dispatch_si<0, true, false>(b, cfg, st);
+      dispatch_f32<true, false>(b, cfg, st);
   } else {
     if (cfg.kahan)
-      dispatch_si<0, false, true>(b, cfg, st);
+      dispatch_f32<false, true>(b, cfg, st);
     else
-      dispatch_si<0, false, false>(b, cfg, st);
+      dispatch_f32<false, false>(b, cfg, st);
   }
 }
 
