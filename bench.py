@@ -9,7 +9,7 @@ aggregation, tree walk). The state plus tree (~330 MB) is larger than the 126 MB
 L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config collision|plummer|batched]
+                    [--config collision|plummer|batched|serving]
 
 Under torchrun each rank steps its own replica (a single system does not shard:
 replicas only) and value = all ranks' particle-steps / max-over-ranks device time.
@@ -308,17 +308,133 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """256 independent systems (N log-uniform in [4096, 262144], half Plummer, half disk +
+    halo, eps 0.01, theta 0.5, dt 1e-3 / 5e-4) in one batch vs the plain single-system
+    path stepping the same systems one at a time."""
+    import galaxy_b200 as gb
+    from galaxy_b200 import workloads
+
+    dist, rank, ws, local = _dist()
+    mix = workloads.batched_mix(args.systems, seed=rank)
+    n_tot = sum(len(m.state) for m in mix)
+    b = gb.Batch(device=local)
+    for m in mix:
+        b.add(m.state, m.g, m.eps, m.theta, m.dt)
+    b.step(args.warmup)
+    clocks = ClockSampler(local)
+    clocks.start()
+    _barrier(dist, local)
+    ms = []
+    for _ in range(args.steps):
+        b.step(1)
+        ms.append(b.stats()["ms_last_step"])
+    _barrier(dist, local)
+    clk = clocks.stop()
+    t = _max_over_ranks(dist, sum(ms) / 1e3, local)
+    value = n_tot * ws * args.steps / t
+    del b
+    # plain path: the same systems, each stepped alone by the single-system handle
+    hs = []
+    for m in mix:
+        r = gb.GpuResidentLeapfrog(m.g, m.eps, m.theta, device=local)
+        r.upload(m.state)
+        r.step_many(m.dt, 1)
+        hs.append((r, m))
+    k_plain = max(1, min(args.steps, 3))
+    t_plain = 0.0
+    for _ in range(k_plain):
+        for r, m in hs:
+            t_plain += r.step_many_timed(m.dt, 1) / 1e3
+    t_plain = _max_over_ranks(dist, t_plain, local)
+    plain = n_tot * ws * k_plain / t_plain
+    del hs
+    if rank == 0:
+        line = {"metric": "particle-steps/s at theta=0.5, batched uneven systems", "value": value,
+                "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"batched-{args.systems}-systems", "particles_per_gpu": n_tot,
+                           "systems": args.systems, "n_range": [4096, 262144], "theta": 0.5, "eps": 0.01,
+                           "dt": [1e-3, 5e-4], "cuda_graph": True, "parallelism": "replicas" if ws > 1 else "1 GPU"},
+                "step_ms_p50": float(np.percentile(ms, 50)), "step_ms_p99": float(np.percentile(ms, 99)),
+                "plain_path": {"value": plain, "unit": "particle-steps/s", "steps": k_plain,
+                               "how": "same systems, one single-system handle each, stepped one after another "
+                                      "(device time of each step summed)"},
+                "batched_over_plain": value / plain, "gpu_launches": 8 * args.steps, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_serving(args):
+    """A Poisson stream (50 req/s) of collision scenarios, N log-uniform in [16384,
+    2097152], mass ratio U[1,10], pericentre U[2,8] Rd, 100-1000 steps each, served
+    with continuous batching against a 150 GB budget for a fixed horizon."""
+    import galaxy_b200 as gb
+    from galaxy_b200 import workloads
+
+    dist, rank, ws, local = _dist()
+    reqs = workloads.request_stream(args.requests, rate=50.0, seed=rank)
+    specs = [r.spec() for r in reqs]  # generated before the clock starts
+    srv = gb.Server(budget_bytes=150 << 30, device=local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    rids = []
+    for r, sp in zip(reqs, specs):
+        delay = r.arrival - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        rids.append(srv.submit(sp.state, sp.g, sp.eps, sp.theta, sp.dt, r.steps))
+    deadline = t0 + args.horizon
+    for rid in rids:
+        left = deadline - time.perf_counter()
+        if left <= 0:
+            break
+        try:
+            srv.wait(rid, left)
+        except gb.GxError:
+            break
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    clk = clocks.stop()
+    srv.close()
+    if rank == 0:
+        line = {"metric": "particle-steps/s at theta=0.5, served (continuous batching)",
+                "value": st["particle_steps_per_s_device"], "unit": "particle-steps/s", "n_gpus": ws,
+                "steps": st["steps"], "warmup": 0, "ms_per_step": st["step_ms_mean"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"serving-{args.requests}-requests", "rate_per_s": 50.0,
+                           "n_range": [16384, 2097152], "steps_range": [100, 1000], "budget_gb": 150,
+                           "horizon_s": args.horizon},
+                "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],
+                "wall_particle_steps_per_s": st["particle_steps"] / wall, "completed": st["completed"],
+                "submitted": len(rids), "max_live": st["max_live"], "queue_s_p50": st["queue_s_p50"],
+                "queue_s_p99": st["queue_s_p99"], "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="collision", choices=["collision", "plummer"])
+    ap.add_argument("--config", default="collision", choices=["collision", "plummer", "batched", "serving"])
+    ap.add_argument("--systems", type=int, default=256, help="batched: number of systems")
+    ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
+    ap.add_argument("--horizon", type=float, default=60.0, help="serving: seconds to serve")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "batched":
+        run_batched(args)
+    elif args.config == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

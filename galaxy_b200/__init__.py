@@ -31,7 +31,8 @@ from ._lib import (GX_FLAG_NO_KAHAN, GX_FLAG_STAGE_TIMES, GX_FLAG_STATS, GX_MULT
                    GX_PREC_F32, GX_PREC_F64, GxError, check, lib)
 
 __all__ = [
-    "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "GxError", "PinnedState",
+    "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "Server", "GxError",
+    "PinnedState",
     "stage_morton",
     "stage_sort", "stage_build", "device_info", "ic",
 ]
@@ -83,7 +84,7 @@ class ForceSolver:
 
 
 def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: int, walk_block: int,
-             stage_times: bool = False):
+             stage_times: bool = False, walk_ctas_per_sm: int = 0):
     o = _lib.Options()
     o.struct_size = C.sizeof(_lib.Options)
     o.precision = {"f32": GX_PREC_F32, "f64": GX_PREC_F64}[precision]
@@ -92,15 +93,16 @@ def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: i
                (GX_FLAG_STAGE_TIMES if stage_times else 0))
     o.device = device
     o.walk_block = walk_block
+    o.walk_ctas_per_sm = walk_ctas_per_sm
     return o
 
 
 class _Handle:
     def __init__(self, g, softening, theta, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
-                 walk_block=0, stage_times=False):
+                 walk_block=0, stage_times=False, walk_ctas_per_sm=0):
         self.g, self.softening, self.theta = float(g), float(softening), float(theta)
         self._h = C.c_void_p()
-        o = _options(precision, multipole, kahan, stats, device, walk_block, stage_times)
+        o = _options(precision, multipole, kahan, stats, device, walk_block, stage_times, walk_ctas_per_sm)
         rc = lib().gx_create(self.g, self.softening, self.theta, C.byref(o), C.byref(self._h))
         if rc != 0:
             check(rc, None)
@@ -317,9 +319,9 @@ class Batch:
     """Many independent systems, one launch per stage (see include/galaxy_b200.h)."""
 
     def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
-                 walk_block=0):
+                 walk_block=0, walk_ctas_per_sm=0):
         self._b = C.c_void_p()
-        o = _options(precision, multipole, kahan, stats, device, walk_block)
+        o = _options(precision, multipole, kahan, stats, device, walk_block, False, walk_ctas_per_sm)
         rc = lib().gx_batch_create(int(budget_bytes), C.byref(o), C.byref(self._b))
         if rc != 0:
             check(rc, None)
@@ -371,6 +373,66 @@ class Batch:
     def stats(self) -> dict:
         s = _lib.BatchStats()
         self._ck(lib().gx_batch_stats_get(self._b, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in s._fields_}
+
+
+class Server:
+    """Continuous-batching server (include/galaxy_b200.h, gx_server_*): submit systems
+    from any thread; a native stepping thread admits them against the device budget,
+    steps all live systems together and retires each after its steps."""
+
+    QUEUED, RUNNING, DONE, REJECTED = 0, 1, 2, 3
+
+    def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, device=-1):
+        self._s = C.c_void_p()
+        o = _options(precision, multipole, kahan, False, device, 0)
+        rc = lib().gx_server_create(int(budget_bytes), C.byref(o), C.byref(self._s))
+        if rc != 0:
+            check(rc, None)
+        self._n = {}
+
+    def _ck(self, rc):
+        check(rc, self._s, "gx_server_last_error")
+
+    def close(self):
+        if getattr(self, "_s", None) and self._s.value:
+            lib().gx_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, state: State, g: float, softening: float, theta: float, dt: float, steps: int) -> int:
+        rid = C.c_uint64()
+        self._ck(lib().gx_server_submit(self._s, len(state), _ptr(state.pos), _ptr(state.vel), _ptr(state.mass), g,
+                                        softening, theta, dt, int(steps), C.byref(rid)))
+        self._n[rid.value] = (len(state), state.mass.copy())
+        return rid.value
+
+    def status(self, rid: int):
+        st, done = C.c_int(), C.c_uint64()
+        self._ck(lib().gx_server_status(self._s, rid, C.byref(st), C.byref(done)))
+        return st.value, done.value
+
+    def wait(self, rid: int, timeout: float = 600.0) -> None:
+        self._ck(lib().gx_server_wait(self._s, rid, float(timeout)))
+
+    def result(self, rid: int) -> State:
+        n, mass = self._n[rid]
+        pos, vel, t = np.empty((n, 3)), np.empty((n, 3)), C.c_double()
+        self._ck(lib().gx_server_result(self._s, rid, _ptr(pos), _ptr(vel), C.byref(t)))
+        return State(pos, vel, mass.copy(), t.value)
+
+    def release(self, rid: int) -> None:
+        self._ck(lib().gx_server_release(self._s, rid))
+        self._n.pop(rid, None)
+
+    def stats(self) -> dict:
+        s = _lib.ServerStats()
+        self._ck(lib().gx_server_stats_get(self._s, C.byref(s)))
         return {f: getattr(s, f) for f, _ in s._fields_}
 
 

@@ -44,6 +44,7 @@ class Options(C.Structure):
         ("flags", C.c_uint32),
         ("device", C.c_int32),
         ("walk_block", C.c_uint32),
+        ("walk_ctas_per_sm", C.c_uint32),
     ]
 
 
@@ -71,6 +72,26 @@ class BatchStats(C.Structure):
         ("bytes_in_use", C.c_uint64),
         ("budget_bytes", C.c_uint64),
         ("ms_last_step", C.c_float),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_uint64),
+        ("particle_steps", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("queued", C.c_uint64),
+        ("live", C.c_uint64),
+        ("max_live", C.c_uint64),
+        ("bytes_in_use", C.c_uint64),
+        ("busy_s", C.c_double),
+        ("wall_s", C.c_double),
+        ("step_ms_p50", C.c_double),
+        ("step_ms_p99", C.c_double),
+        ("step_ms_mean", C.c_double),
+        ("particle_steps_per_s_device", C.c_double),
+        ("queue_s_p50", C.c_double),
+        ("queue_s_p99", C.c_double),
     ]
 
 
@@ -118,6 +139,15 @@ SIGNATURES = {
     "gx_system_len": (_i, [_vp, _u64, C.POINTER(_sz)]),
     "gx_batch_stats_get": (_i, [_vp, C.POINTER(BatchStats)]),
     "gx_batch_set_graph": (_i, [_vp, _i]),
+    "gx_server_create": (_i, [_sz, C.POINTER(Options), C.POINTER(_vp)]),
+    "gx_server_destroy": (None, [_vp]),
+    "gx_server_last_error": (C.c_char_p, [_vp]),
+    "gx_server_submit": (_i, [_vp, _sz, _vp, _vp, _vp, _d, _d, _d, _d, _u64, C.POINTER(_u64)]),
+    "gx_server_status": (_i, [_vp, _u64, C.POINTER(_i), C.POINTER(_u64)]),
+    "gx_server_wait": (_i, [_vp, _u64, _d]),
+    "gx_server_result": (_i, [_vp, _u64, _vp, _vp, C.POINTER(_d)]),
+    "gx_server_release": (_i, [_vp, _u64]),
+    "gx_server_stats_get": (_i, [_vp, C.POINTER(ServerStats)]),
     "gx_ic_plummer": (_i, [_sz, _u64, _d, _d, _d, _vp, _vp, _vp]),
     "gx_ic_collision": (_i, [_sz, _u64, _d, _d, _d, _d, _vp, _vp, _vp]),
     "gx_ic_disk_galaxy": (_i, [_sz, _u64, _vp, _vp, _vp]),

@@ -7,6 +7,7 @@
 // The closing half kick of a step is deferred into the next step's kick + drift
 // kernel (two separately rounded half kicks, as integrator.rs:61-73 applies them)
 // or into a snapshot, so it costs no extra pass over the state.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -100,12 +101,15 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   if (n <= cap_n && tiles <= cap_tiles && items <= cap_items && nsys <= cap_sys && quad <= cap_quad &&
       f64rec <= cap_f64)
     return cudaSuccess;
-  // Grow (never shrink), with headroom so a slowly growing N does not reallocate
-  // every call.
-  size_t nn = std::max(n, cap_n + cap_n / 4);
-  size_t nt = std::max(tiles, cap_tiles + cap_tiles / 4);
-  size_t ni = std::max(items, cap_items + cap_items / 4);
-  size_t ns = std::max(nsys, cap_sys);
+  // Grow (never shrink) only the dimensions that are short, each with headroom so a
+  // slowly growing batch does not reallocate on every call.
+  auto grown = [](size_t need, size_t cap, size_t floor_) {
+    return need <= cap ? cap : std::max({need, cap + cap / 4, floor_});
+  };
+  size_t nn = grown(n, cap_n, 0);
+  size_t nt = grown(tiles, cap_tiles, 0);
+  size_t ni = grown(items, cap_items, 0);
+  size_t ns = grown(nsys, cap_sys, 16);
   int q = std::max(quad, cap_quad), f = std::max(f64rec, cap_f64);
   cudaStreamSynchronize(st);
   release();
@@ -212,6 +216,7 @@ struct gx_handle {
   double g = 1.0, eps = 0.0, theta = 0.5;
   gx_options opt{};
   int device = 0;
+  int sm_count = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[6] = {};
   std::string err;
@@ -254,6 +259,7 @@ WalkCfg walk_cfg(const gx_handle* h) {
   c.stats = (h->opt.flags & GX_FLAG_STATS) ? 1 : 0;
   c.inside_test = h->theta >= 0.57 ? 1 : 0;
   c.block = h->opt.walk_block ? static_cast<int>(h->opt.walk_block) : 256;
+  c.persistent_ctas = h->opt.walk_ctas_per_sm ? static_cast<int>(h->opt.walk_ctas_per_sm) * h->sm_count : 0;
   return c;
 }
 
@@ -386,6 +392,7 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
   int dev = o.device;
   if (dev < 0) cudaGetDevice(&dev);
   h->device = dev;
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);

@@ -71,7 +71,8 @@ WalkCfg bcfg(const gx_batch* bt, bool inside) {
   c.stats = (bt->opt.flags & GX_FLAG_STATS) ? 1 : 0;
   c.inside_test = inside ? 1 : 0;
   c.block = bt->opt.walk_block ? static_cast<int>(bt->opt.walk_block) : 256;
-  c.persistent_ctas = bt->sm_count * (2048 / c.block / 2);
+  c.persistent_ctas = bt->sm_count * (bt->opt.walk_ctas_per_sm ? static_cast<int>(bt->opt.walk_ctas_per_sm)
+                                                               : 2048 / c.block / 2);
   return c;
 }
 
@@ -164,9 +165,7 @@ int grow(gx_batch* bt, size_t n_total, size_t nsys) {
     GB_CK(bt, cudaMemcpyAsync(tmp + 6 * keep, ar.b.acc, 3 * keep * 8, cudaMemcpyDeviceToDevice, bt->stream));
     GB_CK(bt, cudaMemcpyAsync(tmp + 9 * keep, ar.mass_rw, keep * 8, cudaMemcpyDeviceToDevice, bt->stream));
   }
-  cudaError_t e = ar.ensure(std::max(n_total, ar.cap_n), std::max(tiles, ar.cap_tiles),
-                            std::max(items, ar.cap_items), std::max(nsys, std::max<size_t>(ar.cap_sys, 64)), quad,
-                            f64, bt->stream);
+  cudaError_t e = ar.ensure(n_total, tiles, items, nsys, quad, f64, bt->stream);
   if (e != cudaSuccess) {
     if (tmp) cudaFree(tmp);
     return bfail(bt, GX_ERR_CUDA, std::string("arena: ") + cudaGetErrorString(e));

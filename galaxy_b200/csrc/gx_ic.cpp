@@ -135,16 +135,27 @@ struct JeansTable {
   }
 };
 
-double invert_monotone(double target, double lo, double hi, double (*f)(double, const void*), const void* ctx) {
-  for (int it = 0; it < 80; ++it) {
-    double mid = 0.5 * (lo + hi);
-    if (f(mid, ctx) < target)
-      lo = mid;
-    else
-      hi = mid;
+// Inverse of a monotone CDF on [lo, hi], tabulated once and interpolated linearly.
+struct InverseCdf {
+  std::vector<double> u, x;
+  template <class F>
+  InverseCdf(F cdf, double lo, double hi, int n = 8192) {
+    x.resize(n);
+    u.resize(n);
+    for (int i = 0; i < n; ++i) {
+      const double t = static_cast<double>(i) / (n - 1);
+      x[i] = lo + (hi - lo) * t * t;  // denser near the centre, where the mass is
+      u[i] = cdf(x[i]);
+    }
   }
-  return 0.5 * (lo + hi);
-}
+  double operator()(double v) const {
+    if (v <= u.front()) return x.front();
+    if (v >= u.back()) return x.back();
+    const size_t k = std::upper_bound(u.begin(), u.end(), v) - u.begin();
+    const double t = (v - u[k - 1]) / std::max(u[k] - u[k - 1], 1e-300);
+    return x[k - 1] + t * (x[k] - x[k - 1]);
+  }
+};
 
 void sample_galaxy(const Galaxy& g, SplitMix64& rng, double* pos, double* vel, double* mass, size_t a, size_t b,
                    bool with_bulge) {
@@ -160,11 +171,9 @@ void sample_galaxy(const Galaxy& g, SplitMix64& rng, double* pos, double* vel, d
   if (nb) jb.build(g, [&](double r) { return g.bulge_menc(r); }, 1e-4, g.rbmax);
   size_t i = a;
   // halo
+  const InverseCdf halo_r([&](double x) { return Galaxy::nfw_mu(x) / g.nfw_norm; }, 0.0, g.rt / g.rs);
   for (size_t k = 0; k < nh; ++k, ++i) {
-    double u = rng.next_f64();
-    double x = invert_monotone(u * g.nfw_norm, 0.0, g.rt / g.rs,
-                               [](double xx, const void*) { return Galaxy::nfw_mu(xx); }, nullptr);
-    double r = x * g.rs, d[3];
+    double r = halo_r(rng.next_f64()) * g.rs, d[3];
     random_direction(rng, d);
     double sig = jh.at(r);
     for (int c = 0; c < 3; ++c) {
@@ -176,11 +185,9 @@ void sample_galaxy(const Galaxy& g, SplitMix64& rng, double* pos, double* vel, d
   // disk
   const double xm = g.rdmax / g.rd;
   const double cdf_max = 1.0 - (1.0 + xm) * std::exp(-xm);
+  const InverseCdf disk_r([&](double x) { return (1.0 - (1.0 + x) * std::exp(-x)) / cdf_max; }, 0.0, xm);
   for (size_t k = 0; k < nd; ++k, ++i) {
-    double u = rng.next_f64() * cdf_max;
-    double x = invert_monotone(u, 0.0, xm, [](double xx, const void*) { return 1.0 - (1.0 + xx) * std::exp(-xx); },
-                               nullptr);
-    double R = x * g.rd;
+    double R = disk_r(rng.next_f64()) * g.rd;
     double phi = kTau * rng.next_f64();
     double w = 2.0 * rng.next_f64() - 1.0;
     w = std::max(-0.999999, std::min(0.999999, w));

@@ -103,42 +103,6 @@ __device__ __forceinline__ void stack_pop(WarpStack& s, uint32_t& u, uint32_t& m
   m = __shfl_sync(0xffffffffu, lo ? s.m0 : s.m1, src);
 }
 
-// Stack of child pairs still to decide: (left child, right child, lane mask), entry
-// j in lane j % 32 of the (x0, y0, m0) or (x1, y1, m1) registers.
-struct PairStack {
-  uint32_t x0, y0, m0, x1, y1, m1;
-  int sp;
-};
-
-__device__ __forceinline__ bool pair_push(PairStack& s, uint2 kd, uint32_t m, int lane) {
-  if (s.sp < 32) {
-    if (lane == s.sp) {
-      s.x0 = kd.x;
-      s.y0 = kd.y;
-      s.m0 = m;
-    }
-  } else if (s.sp < 64) {
-    if (lane == s.sp - 32) {
-      s.x1 = kd.x;
-      s.y1 = kd.y;
-      s.m1 = m;
-    }
-  } else {
-    return false;
-  }
-  ++s.sp;
-  return true;
-}
-
-__device__ __forceinline__ void pair_pop(PairStack& s, uint2& kd, uint32_t& m) {
-  --s.sp;
-  const int src = s.sp & 31;
-  const bool lo = s.sp < 32;
-  kd.x = __shfl_sync(0xffffffffu, lo ? s.x0 : s.x1, src);
-  kd.y = __shfl_sync(0xffffffffu, lo ? s.y0 : s.y1, src);
-  m = __shfl_sync(0xffffffffu, lo ? s.m0 : s.m1, src);
-}
-
 __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -376,8 +340,12 @@ __device__ __forceinline__ void resolve_amb(const StepBufs& b, const Lane32& L, 
 // even a corrupt tree cannot read out of bounds; a clamp or an exhausted iteration
 // budget raises the device error word. Each lane takes exactly the reference's set of
 // terms; only the order of summation differs from the FP64 walk.
+#ifndef GX_WALK_MINB
+#define GX_WALK_MINB 3  // resident 256-thread blocks per SM the register budget is sized for
+#endif
+
 template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
-__global__ void __launch_bounds__(256, 3) k_walk_f32(StepBufs b, int persistent) {
+__global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int persistent) {
   const int lane = threadIdx.x & 31;
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
   uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;

@@ -55,6 +55,8 @@ typedef struct gx_options {
   uint32_t flags;          /* GX_FLAG_* */
   int32_t device;          /* CUDA ordinal, -1 = current device */
   uint32_t walk_block;     /* threads per block of the tree walk, 0 = tuned default */
+  uint32_t walk_ctas_per_sm; /* >0: persistent work-stealing walk with this many CTAs per SM;
+                                0: tuned default (one warp per 32 targets for a single system) */
 } gx_options;
 
 typedef struct gx_handle gx_handle;
@@ -199,6 +201,52 @@ int gx_system_len(const gx_batch* b, uint64_t id, size_t* n_out);
 int gx_batch_stats_get(const gx_batch* b, gx_batch_stats* out);
 /* Capture one batched step as a CUDA graph and replay it (1) or launch eagerly (0). */
 int gx_batch_set_graph(gx_batch* b, int enable);
+
+/* ---- continuous-batching server ----------------------------------------------- */
+/* A stepping thread admits submitted systems in arrival order as the device budget
+ * allows (between batched steps, so new requests join systems in flight), keeps every
+ * admitted system resident, advances all live systems together one KDK step per
+ * iteration and retires each after its steps. A result is bit-identical to running
+ * the same system alone. (No counterpart in the reference, which runs one scenario
+ * per process: xtask/src/simulate.rs.) */
+typedef struct gx_server gx_server;
+
+#define GX_REQ_QUEUED 0
+#define GX_REQ_RUNNING 1
+#define GX_REQ_DONE 2
+#define GX_REQ_REJECTED 3
+
+typedef struct gx_server_stats {
+  uint64_t steps;            /* batched steps taken */
+  uint64_t particle_steps;   /* sum over steps of live particles */
+  uint64_t completed;
+  uint64_t queued;
+  uint64_t live;
+  uint64_t max_live;
+  uint64_t bytes_in_use;
+  double busy_s;             /* host time spent in batched steps */
+  double wall_s;             /* since creation */
+  double step_ms_p50;        /* device time per batched step (CUDA events) */
+  double step_ms_p99;
+  double step_ms_mean;
+  double particle_steps_per_s_device;
+  double queue_s_p50;        /* submit -> admission delay */
+  double queue_s_p99;
+} gx_server_stats;
+
+int gx_server_create(size_t budget_bytes, const gx_options* opt, gx_server** out);
+void gx_server_destroy(gx_server* s);
+const char* gx_server_last_error(const gx_server* s);
+/* Copy a scenario in and queue it; thread-safe. */
+int gx_server_submit(gx_server* s, size_t n, const double* pos, const double* vel, const double* mass, double g,
+                     double softening, double theta, double dt, uint64_t steps, uint64_t* rid_out);
+int gx_server_status(gx_server* s, uint64_t rid, int* status_out, uint64_t* steps_done);
+/* Block until the request is done (GX_OK) or rejected; GX_ERR_STATE on timeout. */
+int gx_server_wait(gx_server* s, uint64_t rid, double timeout_s);
+/* Final state of a finished request (pos/vel [3n], time). */
+int gx_server_result(gx_server* s, uint64_t rid, double* pos_out, double* vel_out, double* time_out);
+int gx_server_release(gx_server* s, uint64_t rid);
+int gx_server_stats_get(gx_server* s, gx_server_stats* out);
 
 /* ---- seeded initial conditions (the reference's ic/ crate as input generator) -- */
 /* Plummer::sample (ic/src/plummer.rs:94-140): G, total mass M, scale radius a; seed. */

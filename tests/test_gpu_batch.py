@@ -68,3 +68,20 @@ def test_budget_rejects():
         b.add(gb.ic.plummer(400_000, 2), 1.0, 0.01, 0.5, 1e-3)
     assert e.value.code == -4
     assert b.stats()["systems"] == 1
+
+
+def test_many_systems_memory_stays_linear():
+    b = gb.Batch()
+    sts = [gb.ic.plummer(500 + (i % 7) * 50, 300 + i) for i in range(150)]
+    for st in sts:
+        b.add(st, 1.0, 0.01, 0.5, 1e-3)
+    s = b.stats()
+    assert s["systems"] == 150
+    per_particle = s["bytes_in_use"] / s["particles"]
+    assert per_particle < 3000, per_particle  # ~400 B/particle plus headroom and per-system tables
+    b.step(2)
+    ref = gb.GpuResidentLeapfrog(1.0, 0.01, 0.5)
+    ref.upload(sts[77])
+    ref.step_many(1e-3, 2)
+    got = b.snapshot(78)  # ids start at 1
+    assert np.array_equal(got.pos, ref.snapshot().pos)
