@@ -157,6 +157,18 @@ def algorithmic(n: int, counts: dict) -> dict:
             "walk_flops": flops}
 
 
+def profiled_walk_traffic(workload_name: str):
+    """DRAM bytes per walk launch from the committed ncu summary of this workload (or None)."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", f"k_walk_f32_{workload_name.replace('collision-', 'collision_')}.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*(\d+)", open(path).read())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
 def cpu_sample_step(st, params, threads: int, n_targets: int, rng) -> float:
     """Seconds for one CPU step estimated from a bounded sample: the oracle's full tree
     build plus the walk of n_targets random targets, scaled to all N targets."""
@@ -267,8 +279,12 @@ def run_ours(args):
     sort_gbs = 4 * alg["sort_pass"] / (stage["ms_sort"] / 1e3) / 1e9
     build_gbs = alg["build"] / (stage["ms_build"] / 1e3) / 1e9
     mort_gbs = (alg["kick_bbox"] + alg["morton"]) / (stage["ms_bbox_morton"] / 1e3) / 1e9
-    roofline = {"kernel": "k_walk (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+    traffic = profiled_walk_traffic(p["name"])
+    roofline = {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                  "profiles/k_walk_f32_collision_2x524288.md" if traffic else None,
+                "algorithmic_bytes_per_launch": alg["walk_bytes"],
                 "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm "
                                "(MEASURED_PEAKS.json has no FP32 figure); no tensor-core work in this path",
                 "flops_per_launch": alg["walk_flops"], "ms_per_launch": stage["ms_walk"],

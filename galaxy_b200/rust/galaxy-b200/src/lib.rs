@@ -1,0 +1,151 @@
+//! `GpuLbvhB200` and `GpuResidentB200`: galaxy's gravity-solver interface over
+//! libgalaxy_b200 (a B200 LBVH Barnes-Hut). `GpuLbvhB200` implements `ForceSolver`
+//! (core/src/traits.rs) and drops in beside `Lbvh`, `BarnesHut` and `GpuLbvhFused`;
+//! `GpuResidentB200` mirrors `GpuResidentLeapfrog`'s upload / step_many / snapshot.
+//!
+//! Written against include/galaxy_b200.h; DVec3 is three f64 (`#[repr(C)]`-compatible
+//! in glam), so `&[DVec3]` is passed as `*const f64` with no copy.
+
+use galaxy_core::{DVec3, ForceSolver, State};
+use std::ffi::CStr;
+use std::os::raw::{c_char, c_int};
+
+#[repr(C)]
+#[derive(Clone, Copy, Default)]
+pub struct GxOptions {
+    pub struct_size: u32,
+    pub precision: u32,
+    pub multipole: u32,
+    pub flags: u32,
+    pub device: i32,
+    pub walk_block: u32,
+    pub walk_ctas_per_sm: u32,
+}
+
+#[repr(C)]
+pub struct GxHandle {
+    _private: [u8; 0],
+}
+
+extern "C" {
+    fn gx_create(g: f64, softening: f64, theta: f64, opt: *const GxOptions, out: *mut *mut GxHandle) -> c_int;
+    fn gx_destroy(h: *mut GxHandle);
+    fn gx_last_error(h: *const GxHandle) -> *const c_char;
+    fn gx_accelerations(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, acc: *mut f64) -> c_int;
+    fn gx_potential_energy(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, out: *mut f64) -> c_int;
+    fn gx_upload(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64) -> c_int;
+    fn gx_step_many(h: *mut GxHandle, dt: f64, steps: u64) -> c_int;
+    fn gx_snapshot(h: *mut GxHandle, pos: *mut f64, vel: *mut f64) -> c_int;
+    fn gx_time(h: *const GxHandle, t: *mut f64) -> c_int;
+}
+
+/// Error of a libgalaxy_b200 call: the status code and the library's message.
+#[derive(Debug)]
+pub struct GxError {
+    pub code: i32,
+    pub message: String,
+}
+
+fn err(h: *const GxHandle, code: c_int) -> GxError {
+    let msg = unsafe { CStr::from_ptr(gx_last_error(h)) }.to_string_lossy().into_owned();
+    GxError { code, message: msg }
+}
+
+fn as_f64(v: &[DVec3]) -> *const f64 {
+    debug_assert_eq!(std::mem::size_of::<DVec3>(), 24);
+    v.as_ptr() as *const f64
+}
+
+/// Drop-in `ForceSolver` (the role of `GpuLbvhFused`): host state in, accelerations out.
+pub struct GpuLbvhB200 {
+    h: *mut GxHandle,
+    pub g: f64,
+    pub softening: f64,
+}
+
+impl GpuLbvhB200 {
+    /// `precision`: 0 = FP32 walk (default), 1 = FP64 (bit-identical to `Lbvh`).
+    pub fn new(g: f64, softening: f64, theta: f64, precision: u32) -> Result<Self, GxError> {
+        let opt = GxOptions { struct_size: std::mem::size_of::<GxOptions>() as u32, precision, device: -1, ..Default::default() };
+        let mut h = std::ptr::null_mut();
+        let rc = unsafe { gx_create(g, softening, theta, &opt, &mut h) };
+        if rc != 0 {
+            return Err(err(std::ptr::null(), rc));
+        }
+        Ok(Self { h, g, softening })
+    }
+}
+
+impl Drop for GpuLbvhB200 {
+    fn drop(&mut self) {
+        unsafe { gx_destroy(self.h) }
+    }
+}
+
+impl ForceSolver for GpuLbvhB200 {
+    fn accelerations(&mut self, state: &State, acc: &mut [DVec3]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        let rc = unsafe {
+            gx_accelerations(self.h, n, as_f64(&state.pos), state.mass.as_ptr(), acc.as_mut_ptr() as *mut f64)
+        };
+        // A device failure here is a lost GPU, as in GpuLbvhFused: panic rather than corrupt state.
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    fn potential_energy(&self, state: &State) -> f64 {
+        let mut u = 0.0;
+        let rc = unsafe { gx_potential_energy(self.h, state.len(), as_f64(&state.pos), state.mass.as_ptr(), &mut u) };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+        u
+    }
+}
+
+/// Device-resident KDK stepping (the role of `GpuResidentLeapfrog`).
+pub struct GpuResidentB200 {
+    h: *mut GxHandle,
+    mass: Vec<f64>,
+}
+
+impl GpuResidentB200 {
+    pub fn new(g: f64, softening: f64, theta: f64) -> Result<Self, GxError> {
+        let mut h = std::ptr::null_mut();
+        let rc = unsafe { gx_create(g, softening, theta, std::ptr::null(), &mut h) };
+        if rc != 0 {
+            return Err(err(std::ptr::null(), rc));
+        }
+        Ok(Self { h, mass: Vec::new() })
+    }
+
+    pub fn upload(&mut self, state: &State) -> Result<(), GxError> {
+        self.mass = state.mass.clone();
+        let rc = unsafe {
+            gx_upload(self.h, state.len(), as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr())
+        };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok(()) }
+    }
+
+    pub fn step_many(&mut self, dt: f64, steps: u64) -> Result<(), GxError> {
+        let rc = unsafe { gx_step_many(self.h, dt, steps) };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok(()) }
+    }
+
+    pub fn snapshot(&mut self) -> Result<State, GxError> {
+        let n = self.mass.len();
+        let mut pos = vec![DVec3::ZERO; n];
+        let mut vel = vec![DVec3::ZERO; n];
+        let rc = unsafe { gx_snapshot(self.h, pos.as_mut_ptr() as *mut f64, vel.as_mut_ptr() as *mut f64) };
+        if rc != 0 {
+            return Err(err(self.h, rc));
+        }
+        let mut s = State::from_phase_space(pos, vel, self.mass.clone());
+        unsafe { gx_time(self.h, &mut s.time) };
+        Ok(s)
+    }
+}
+
+impl Drop for GpuResidentB200 {
+    fn drop(&mut self) {
+        unsafe { gx_destroy(self.h) }
+    }
+}
