@@ -334,7 +334,8 @@ def run_batched(args):
     dist, rank, ws, local = _dist()
     mix = workloads.batched_mix(args.systems, seed=rank)
     n_tot = sum(len(m.state) for m in mix)
-    b = gb.Batch(device=local)
+    k63 = args.morton63
+    b = gb.Batch(device=local, morton63=k63)
     for m in mix:
         b.add(m.state, m.g, m.eps, m.theta, m.dt)
     b.step(args.warmup)
@@ -353,7 +354,7 @@ def run_batched(args):
     # plain path: the same systems, each stepped alone by the single-system handle
     hs = []
     for m in mix:
-        r = gb.GpuResidentLeapfrog(m.g, m.eps, m.theta, device=local)
+        r = gb.GpuResidentLeapfrog(m.g, m.eps, m.theta, device=local, morton63=k63)
         r.upload(m.state)
         r.step_many(m.dt, 1)
         hs.append((r, m))
@@ -371,6 +372,7 @@ def run_batched(args):
                 "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"batched-{args.systems}-systems", "particles_per_gpu": n_tot,
+                           "morton_bits": 63 if k63 else 30,
                            "systems": args.systems, "n_range": [4096, 262144], "theta": 0.5, "eps": 0.01,
                            "dt": [1e-3, 5e-4], "cuda_graph": True, "parallelism": "replicas" if ws > 1 else "1 GPU"},
                 "step_ms_p50": float(np.percentile(ms, 50)), "step_ms_p99": float(np.percentile(ms, 99)),
@@ -393,7 +395,7 @@ def run_serving(args):
     dist, rank, ws, local = _dist()
     reqs = workloads.request_stream(args.requests, rate=50.0, seed=rank)
     specs = [r.spec() for r in reqs]  # generated before the clock starts
-    srv = gb.Server(budget_bytes=150 << 30, device=local)
+    srv = gb.Server(budget_bytes=150 << 30, device=local, morton63=args.morton63)
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
@@ -443,6 +445,7 @@ def main():
     ap.add_argument("--systems", type=int, default=256, help="batched: number of systems")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
     ap.add_argument("--horizon", type=float, default=60.0, help="serving: seconds to serve")
+    ap.add_argument("--morton63", action="store_true", help="batched/serving: 63-bit Morton keys")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -27,8 +27,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (GX_FLAG_NO_KAHAN, GX_FLAG_STAGE_TIMES, GX_FLAG_STATS, GX_MULTIPOLE_MONO, GX_MULTIPOLE_QUAD,
-                   GX_PREC_F32, GX_PREC_F64, GxError, check, lib)
+from ._lib import (GX_FLAG_MORTON63, GX_FLAG_NO_KAHAN, GX_FLAG_STAGE_TIMES, GX_FLAG_STATS, GX_MULTIPOLE_MONO,
+                   GX_MULTIPOLE_QUAD, GX_PREC_F32, GX_PREC_F64, GxError, check, lib)
 
 __all__ = [
     "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "Server", "GxError",
@@ -84,13 +84,13 @@ class ForceSolver:
 
 
 def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: int, walk_block: int,
-             stage_times: bool = False, walk_ctas_per_sm: int = 0):
+             stage_times: bool = False, walk_ctas_per_sm: int = 0, morton63: bool = False):
     o = _lib.Options()
     o.struct_size = C.sizeof(_lib.Options)
     o.precision = {"f32": GX_PREC_F32, "f64": GX_PREC_F64}[precision]
     o.multipole = {"mono": GX_MULTIPOLE_MONO, "quad": GX_MULTIPOLE_QUAD}[multipole]
     o.flags = ((0 if kahan else GX_FLAG_NO_KAHAN) | (GX_FLAG_STATS if stats else 0) |
-               (GX_FLAG_STAGE_TIMES if stage_times else 0))
+               (GX_FLAG_STAGE_TIMES if stage_times else 0) | (GX_FLAG_MORTON63 if morton63 else 0))
     o.device = device
     o.walk_block = walk_block
     o.walk_ctas_per_sm = walk_ctas_per_sm
@@ -99,10 +99,10 @@ def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: i
 
 class _Handle:
     def __init__(self, g, softening, theta, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
-                 walk_block=0, stage_times=False, walk_ctas_per_sm=0):
+                 walk_block=0, stage_times=False, walk_ctas_per_sm=0, morton63=False):
         self.g, self.softening, self.theta = float(g), float(softening), float(theta)
         self._h = C.c_void_p()
-        o = _options(precision, multipole, kahan, stats, device, walk_block, stage_times, walk_ctas_per_sm)
+        o = _options(precision, multipole, kahan, stats, device, walk_block, stage_times, walk_ctas_per_sm, morton63)
         rc = lib().gx_create(self.g, self.softening, self.theta, C.byref(o), C.byref(self._h))
         if rc != 0:
             check(rc, None)
@@ -319,9 +319,9 @@ class Batch:
     """Many independent systems, one launch per stage (see include/galaxy_b200.h)."""
 
     def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
-                 walk_block=0, walk_ctas_per_sm=0):
+                 walk_block=0, walk_ctas_per_sm=0, morton63=False):
         self._b = C.c_void_p()
-        o = _options(precision, multipole, kahan, stats, device, walk_block, False, walk_ctas_per_sm)
+        o = _options(precision, multipole, kahan, stats, device, walk_block, False, walk_ctas_per_sm, morton63)
         rc = lib().gx_batch_create(int(budget_bytes), C.byref(o), C.byref(self._b))
         if rc != 0:
             check(rc, None)
@@ -383,9 +383,10 @@ class Server:
 
     QUEUED, RUNNING, DONE, REJECTED = 0, 1, 2, 3
 
-    def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, device=-1):
+    def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, device=-1,
+                 morton63=False):
         self._s = C.c_void_p()
-        o = _options(precision, multipole, kahan, False, device, 0)
+        o = _options(precision, multipole, kahan, False, device, 0, morton63=morton63)
         rc = lib().gx_server_create(int(budget_bytes), C.byref(o), C.byref(self._s))
         if rc != 0:
             check(rc, None)

@@ -27,7 +27,7 @@ ERRORS = {
 
 GX_PREC_F32, GX_PREC_F64 = 0, 1
 GX_MULTIPOLE_MONO, GX_MULTIPOLE_QUAD = 0, 1
-GX_FLAG_NO_KAHAN, GX_FLAG_STATS, GX_FLAG_STAGE_TIMES = 1, 2, 4
+GX_FLAG_NO_KAHAN, GX_FLAG_STATS, GX_FLAG_STAGE_TIMES, GX_FLAG_MORTON63 = 1, 2, 4, 8
 
 
 class GxError(RuntimeError):

@@ -83,7 +83,7 @@ size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
   const size_t tiles = n / kTile + nsys + 1;
   size_t s = 0;
   s += 3 * 3 * n * 8 + n * 8;                 // pos, vel, acc, mass
-  s += 4 * n * 4;                             // codes, keys_alt, order, vals_alt
+  s += 6 * n * 4;                             // codes, keys_alt (u64-capable), order, vals_alt
   s += n * 32 + 2 * n * 64;                   // leaf64, walk records (leaves + internal)
   s += n * 8 + 2 * n * 4 + n * sizeof(Agg64); // kids, parent, agg64
   s += n * 16;                                // nodeD
@@ -91,8 +91,8 @@ size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
   if (quad) s += 2 * n * 16 + 6 * n * 8;
   if (f64rec) s += n * sizeof(Node64);
   s += tiles * sizeof(TileDesc) + (n / 32 + nsys + 1) * sizeof(WalkItem);
-  s += nsys * (sizeof(SysDesc) + sizeof(Bounds) + 48 + kRadixPasses * kRadixBins * 4);
-  s += kRadixPasses * tiles * kRadixBins * 4 + 64;
+  s += nsys * (sizeof(SysDesc) + sizeof(Bounds) + 48 + kMaxRadixPasses * kRadixBins * 4);
+  s += kMaxRadixPasses * tiles * kRadixBins * 4 + 64;
   s += (n / 256 + 1) * 8 * 8;  // diagnostic partials
   return s + 64 * 256;         // alignment slack
 }
@@ -128,8 +128,8 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   GX_A(mass, nn, double);
   b.mass = mass;
   mass_rw = mass;
-  GX_A(b.codes, nn, uint32_t);
-  GX_A(b.keys_alt, nn, uint32_t);
+  GX_A(b.codes, 2 * nn, uint32_t);     // room for 63-bit keys
+  GX_A(b.keys_alt, 2 * nn, uint32_t);
   GX_A(b.order, nn, uint32_t);
   GX_A(b.vals_alt, nn, uint32_t);
   GX_A(b.leaf64, nn, double4);
@@ -159,8 +159,8 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   GX_A(b.bounds, ns, Bounds);
   // One zeroed region per step: bbox words, histograms, look-back status, counters.
   const size_t z_bbox = 6 * ns * sizeof(unsigned long long);
-  const size_t z_hist = ns * kRadixPasses * kRadixBins * sizeof(uint32_t);
-  const size_t z_stat = (size_t)kRadixPasses * nt * kRadixBins * sizeof(uint32_t);
+  const size_t z_hist = ns * kMaxRadixPasses * kRadixBins * sizeof(uint32_t);
+  const size_t z_stat = (size_t)kMaxRadixPasses * nt * kRadixBins * sizeof(uint32_t);
   const size_t z_ctr = 16 * sizeof(uint32_t);
   char* z = nullptr;
   GX_A(z, z_bbox + z_hist + z_stat + z_ctr, char);
@@ -282,6 +282,7 @@ int layout(gx_handle* h, size_t n, double dt) {
   GX_CK(h, h->ar.ensure(n, tiles.size(), items.size(), 1, quad, f64, h->stream));
   StepBufs& b = h->ar.b;
   b.n = static_cast<uint32_t>(n);
+  b.key64 = (h->opt.flags & GX_FLAG_MORTON63) ? 1 : 0;
   b.nsys = 1;
   b.ntiles = static_cast<uint32_t>(tiles.size());
   b.nitems = static_cast<uint32_t>(items.size());
@@ -772,6 +773,7 @@ int gx_get_stats(const gx_handle* h, gx_stats* out) {
 int gx_stage_morton(gx_handle* h, size_t n, const double* pos, uint32_t* lanes_out, uint32_t* codes_out,
                     double* bounds_out) {
   if (!h || !pos || !codes_out) return GX_ERR_INVALID_ARG;
+  if (h->opt.flags & GX_FLAG_MORTON63) return fail(h, GX_ERR_INVALID_ARG, "stage entry points take 30-bit keys");
   if (n == 0) return fail(h, GX_ERR_INVALID_ARG, "reference_morton requires a non-empty system");
   cudaSetDevice(h->device);
   h->resident = false;
@@ -803,6 +805,7 @@ int gx_stage_morton(gx_handle* h, size_t n, const double* pos, uint32_t* lanes_o
 
 int gx_stage_sort(gx_handle* h, size_t n, const uint32_t* codes, uint32_t* order_out, uint32_t* sorted_codes_out) {
   if (!h || (n && (!codes || !order_out))) return GX_ERR_INVALID_ARG;
+  if (h->opt.flags & GX_FLAG_MORTON63) return fail(h, GX_ERR_INVALID_ARG, "stage entry points take 30-bit keys");
   if (n == 0) return GX_OK;
   for (size_t i = 0; i < n; ++i)
     if (codes[i] >= (1u << 30)) return fail(h, GX_ERR_INVALID_ARG, "codes must be 30-bit");
@@ -827,6 +830,7 @@ int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const d
   if (!h || !sorted_codes || !sorted_pos || !sorted_mass || !parent) return GX_ERR_INVALID_ARG;
   if (n == 0) return fail(h, GX_ERR_INVALID_ARG, "reference_karras requires a non-empty system");
   if (n > 1 && (!left || !right)) return GX_ERR_INVALID_ARG;
+  if (h->opt.flags & GX_FLAG_MORTON63) return fail(h, GX_ERR_INVALID_ARG, "stage entry points take 30-bit keys");
   if (quad_out && h->opt.multipole != GX_MULTIPOLE_QUAD)
     return fail(h, GX_ERR_INVALID_ARG, "quadrupole output needs a GX_MULTIPOLE_QUAD handle");
   cudaSetDevice(h->device);

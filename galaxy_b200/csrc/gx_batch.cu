@@ -108,6 +108,7 @@ int upload_tables(gx_batch* bt, const std::vector<size_t>& which, bool* inside) 
                    [&](const WalkItem& a, const WalkItem& b) { return sys[a.sys].n > sys[b.sys].n; });
   StepBufs& b = bt->ar.b;
   b.n = bt->total;
+  b.key64 = (bt->opt.flags & GX_FLAG_MORTON63) ? 1 : 0;
   b.nsys = static_cast<uint32_t>(sys.size());
   b.ntiles = static_cast<uint32_t>(tiles.size());
   b.nitems = static_cast<uint32_t>(items.size());

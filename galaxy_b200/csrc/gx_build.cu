@@ -58,10 +58,10 @@ __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
 }  // namespace
 
-template <bool QUAD>
+template <bool QUAD, typename K>
 __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restrict__ tiles,
                                                         const SysDesc* __restrict__ sys, uint32_t n_total,
-                                                        const uint32_t* __restrict__ codes,
+                                                        const K* __restrict__ codes,
                                                         const uint32_t* __restrict__ order,
                                                         const double* __restrict__ pos,
                                                         const double* __restrict__ mass, StepBufs b, int f64rec) {
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
     uint32_t cur_u = k;                 // unified index of the current node
     uint32_t lc = 0, rc = 0;            // children of the current node (if internal)
     bool internal = false;
-    for (int level = 0; level < 80; ++level) {
+    for (int level = 0; level < kMaxDepth; ++level) {
       const bool root = (l == 0 && r == ns - 1);
       bool is_left = true;
       if (!root) {
@@ -259,18 +259,28 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
       }
       cur = par;
       internal = true;
-      if (level == 79) raise_err(b.ctl, kErrClimb);
+      if (level == kMaxDepth - 1) raise_err(b.ctl, kErrClimb);
     }
   }
 }
 
 void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st) {
-  if (quad)
-    k_build<true><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos, b.mass, b,
-                                                      f64_records);
-  else
-    k_build<false><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos, b.mass, b,
-                                                       f64_records);
+  const uint64_t* c64 = reinterpret_cast<const uint64_t*>(b.codes);
+  if (b.key64) {
+    if (quad)
+      k_build<true, uint64_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, c64, b.order, b.pos, b.mass, b,
+                                                                  f64_records);
+    else
+      k_build<false, uint64_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, c64, b.order, b.pos, b.mass,
+                                                                   b, f64_records);
+  } else {
+    if (quad)
+      k_build<true, uint32_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos, b.mass,
+                                                                  b, f64_records);
+    else
+      k_build<false, uint32_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos,
+                                                                   b.mass, b, f64_records);
+  }
 }
 
 }  // namespace gx

@@ -65,6 +65,7 @@ struct Bounds {
   double bmin[3];
   double size;
   double scale;
+  double scale63;  // 2^21 / size, for 63-bit keys
   double lo[3];
   double hi[3];
   float tiny2;    // absolute guard for FP32 distance comparisons (coincident geometry)
@@ -78,7 +79,12 @@ constexpr int kTileThreads = 256;
 constexpr int kItemsPerThread = kTile / kTileThreads;  // 16
 constexpr int kRadixBits = 8;
 constexpr int kRadixBins = 1 << kRadixBits;
-constexpr int kRadixPasses = 4;  // 30-bit codes: 8 + 8 + 8 + 6 bits
+constexpr int kRadixPasses = 4;     // 30-bit codes: 8 + 8 + 8 + 6 bits
+constexpr int kRadixPasses63 = 8;   // 63-bit codes: 7 x 8 + 7 bits
+constexpr int kMaxRadixPasses = 8;  // histogram / look-back arrays are sized for this
+// Tree depth bound: the augmented key is (code, 32-bit position), so a root-to-leaf path
+// has at most 30 + 32 (30-bit codes) or 63 + 32 (63-bit codes) internal levels.
+constexpr int kMaxDepth = 100;
 
 struct TileDesc {
   uint32_t sys, begin, end, pad;
@@ -141,6 +147,27 @@ __host__ __device__ __forceinline__ uint32_t expand10(uint32_t v) {
 __host__ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
   return expand10(x) | (expand10(y) << 1) | (expand10(z) << 2);
 }
+// 63-bit keys (21 bits per axis): the finer grid the reference defers for dense cores
+// and large coordinates (solvers/src/lbvh.rs:29-32). Spreads bit i of v to bit 3i.
+__host__ __device__ __forceinline__ uint64_t expand21(uint32_t v) {
+  uint64_t x = v & 0x1fffffu;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+__host__ __device__ __forceinline__ uint64_t morton3_63(uint32_t x, uint32_t y, uint32_t z) {
+  return expand21(x) | (expand21(y) << 1) | (expand21(z) << 2);
+}
+__device__ __forceinline__ uint32_t quantize_lane21(double v) {
+  double f = floor(v);
+  if (!(f >= 0.0)) return 0u;
+  if (f >= 2097151.0) return 2097151u;
+  return static_cast<uint32_t>(f);
+}
+
 // Rust `(v.floor().max(0.0) as u32).min(1023)`.
 __device__ __forceinline__ uint32_t quantize_lane(double v) {
   double f = floor(v);
@@ -154,6 +181,11 @@ __device__ __forceinline__ uint32_t quantize_lane(double v) {
 __device__ __forceinline__ int prefix_len(uint32_t ca, uint32_t cb, uint32_t a_local, uint32_t b_local) {
   if (ca == cb) return 32 + __clz(a_local ^ b_local);
   return __clz(ca ^ cb);
+}
+// The same over 64-bit codes: (code, position) is a 96-bit augmented key.
+__device__ __forceinline__ int prefix_len(uint64_t ca, uint64_t cb, uint32_t a_local, uint32_t b_local) {
+  if (ca == cb) return 64 + __clz(a_local ^ b_local);
+  return __clzll(static_cast<long long>(ca ^ cb));
 }
 
 // ---- float-float split of an f64 coordinate ------------------------------------

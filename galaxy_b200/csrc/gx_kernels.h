@@ -8,6 +8,7 @@ namespace gx {
 // Every device buffer a step touches (owned by gx_solver / gx_batch).
 struct StepBufs {
   uint32_t n = 0;       // particles over all systems
+  int key64 = 0;        // 63-bit Morton keys (codes/keys_alt hold u64) instead of 30-bit
   uint32_t nsys = 0;
   uint32_t ntiles = 0;
   uint32_t nitems = 0;  // walk items (32 targets each)
@@ -21,15 +22,15 @@ struct StepBufs {
   const double* mass = nullptr;
   // per-step scratch (zeroed by one memset per step, see zero_begin/zero_bytes)
   unsigned long long* bbox_enc = nullptr;  // 6 per system
-  uint32_t* hist = nullptr;                // nsys * 4 * 256
-  uint32_t* sort_status = nullptr;         // 4 * ntiles * 256
+  uint32_t* hist = nullptr;                // nsys * kMaxRadixPasses * 256
+  uint32_t* sort_status = nullptr;         // kMaxRadixPasses * ntiles * 256
   uint32_t* counters = nullptr;            // [0..3] sort tile counters, [4] walk item counter
   void* zero_begin = nullptr;
   size_t zero_bytes = 0;
   Bounds* bounds = nullptr;  // per system
   // sort
-  uint32_t* codes = nullptr;     // keys (pass-0 input, final sorted keys)
-  uint32_t* keys_alt = nullptr;
+  uint32_t* codes = nullptr;     // keys (pass-0 input, final sorted keys); u64 when key64
+  uint32_t* keys_alt = nullptr;  // sized for u64 keys
   uint32_t* order = nullptr;     // values (final permutation)
   uint32_t* vals_alt = nullptr;
   // leaves, sorted order

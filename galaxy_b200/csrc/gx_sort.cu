@@ -47,17 +47,20 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *reinterp
 
 }  // namespace
 
-__global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint32_t* __restrict__ keys_in,
+// One onesweep pass over the tiles of every system, for 30-bit (u32) or 63-bit (u64)
+// keys. Shared memory (dynamic): the tile's keys and indices staged in sorted order.
+template <typename K>
+__global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __restrict__ keys_in,
                                                            const uint32_t* __restrict__ vals_in,
-                                                           uint32_t* __restrict__ keys_out,
-                                                           uint32_t* __restrict__ vals_out,
+                                                           K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                                                            const TileDesc* __restrict__ tiles,
                                                            const SysDesc* __restrict__ sys,
                                                            const uint32_t* __restrict__ hist,
                                                            uint32_t* __restrict__ status, uint32_t* counters,
                                                            uint32_t ntiles, DevCtl* ctl) {
-  __shared__ uint32_t s_keys[kTile];
-  __shared__ uint32_t s_vals[kTile];
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  K* s_keys = reinterpret_cast<K*>(s_dyn);
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + kTile * sizeof(K));
   __shared__ uint32_t s_whist[kWarps][kRadixBins];
   __shared__ uint32_t s_blk_start[kRadixBins];
   __shared__ uint32_t s_glob[kRadixBins];
@@ -79,7 +82,8 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint3
 
   // Load: warp w owns the contiguous 512-key slice [w*512, w*512+512) of the tile,
   // item j of lane l at w*512 + 32 j + l (coalesced, and in index order per warp).
-  uint32_t key[kItemsPerThread], val[kItemsPerThread], rank[kItemsPerThread];
+  K key[kItemsPerThread];
+  uint32_t val[kItemsPerThread], rank[kItemsPerThread];
 #pragma unroll
   for (int j = 0; j < kItemsPerThread; ++j) {
     const uint32_t idx = t.begin + warp * (32 * kItemsPerThread) + 32 * j + lane;
@@ -87,7 +91,7 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint3
       key[j] = keys_in[idx];
       val[j] = vals_in ? vals_in[idx] : idx;
     } else {
-      key[j] = 0xFFFFFFFFu;  // pad: largest digit, ranked after every real key
+      key[j] = ~K(0);  // pad: largest digit, ranked after every real key
       val[j] = 0;
     }
   }
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint3
   const uint32_t lt_mask = (1u << lane) - 1u;
 #pragma unroll
   for (int j = 0; j < kItemsPerThread; ++j) {
-    const uint32_t d = (key[j] >> shift) & (kRadixBins - 1);
+    const uint32_t d = static_cast<uint32_t>(key[j] >> shift) & (kRadixBins - 1);
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t before = s_whist[warp][d];
     rank[j] = before + __popc(peers & lt_mask);
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint3
   }
   // Global start of digit d for this tile: system offset + digits below d in the
   // whole system + the same digit in the system's earlier tiles.
-  const uint32_t* hs = hist + ((size_t)t.sys * kRadixPasses + pass) * kRadixBins;
+  const uint32_t* hs = hist + ((size_t)t.sys * kMaxRadixPasses + pass) * kRadixBins;
   const uint32_t pass_base = block_exclusive_scan_256(hs[d], s_scan);
   s_glob[d] = sd.off + pass_base + excl - blk_start;
   __syncthreads();
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint3
   // Stage in shared memory at the block-local sorted position.
 #pragma unroll
   for (int j = 0; j < kItemsPerThread; ++j) {
-    const uint32_t dj = (key[j] >> shift) & (kRadixBins - 1);
+    const uint32_t dj = static_cast<uint32_t>(key[j] >> shift) & (kRadixBins - 1);
     const uint32_t r = s_blk_start[dj] + s_whist[warp][dj] + rank[j];
     s_keys[r] = key[j];
     s_vals[r] = val[j];
@@ -167,12 +171,49 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const uint3
   // Pads sort behind every real key, so only the first `count` entries are real.
   const uint32_t count = t.end - t.begin;
   for (uint32_t i = threadIdx.x; i < count; i += kTileThreads) {
-    const uint32_t k = s_keys[i];
-    const uint32_t dst = s_glob[(k >> shift) & (kRadixBins - 1)] + i;
+    const K k = s_keys[i];
+    const uint32_t dst = s_glob[static_cast<uint32_t>(k >> shift) & (kRadixBins - 1)] + i;
     keys_out[dst] = k;
     vals_out[dst] = s_vals[i];
   }
 }
+
+namespace {
+
+template <typename K>
+constexpr size_t onesweep_smem() {
+  return kTile * (sizeof(K) + sizeof(uint32_t));
+}
+
+// keys_in -> (keys_out, vals_out) over `passes` passes; keys_tmp/vals_tmp take the odd
+// passes' outputs (an even pass count lands in keys_out).
+template <typename K>
+void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K* keys_tmp, uint32_t* vals_tmp,
+                const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist, uint32_t* status,
+                uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
+  // The dynamic shared-memory opt-in is a per-device function attribute.
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(onesweep_smem<K>()));
+    attr_set[dev] = true;
+  }
+  const K* kin = keys_in;
+  const uint32_t* vin = nullptr;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_tmp = (p % 2) == 0;
+    K* kout = to_tmp ? keys_tmp : keys_out;
+    uint32_t* vout = to_tmp ? vals_tmp : vals_out;
+    k_onesweep<K><<<ntiles, kTileThreads, onesweep_smem<K>(), st>>>(p, kin, vin, kout, vout, tiles, sys, hist,
+                                                                     status, counters, ntiles, ctl);
+    kin = kout;
+    vin = vout;
+  }
+}
+
+}  // namespace
 
 // Digit histograms of all passes from keys already in b.codes (stage entry point).
 __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __restrict__ tiles,
@@ -188,7 +229,7 @@ __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __re
     for (int p = 0; p < kRadixPasses; ++p) atomicAdd(&sh[p * kRadixBins + ((c >> (p * kRadixBits)) & (kRadixBins - 1))], 1u);
   }
   __syncthreads();
-  uint32_t* hs = hist + (size_t)t.sys * kRadixPasses * kRadixBins;
+  uint32_t* hs = hist + (size_t)t.sys * kMaxRadixPasses * kRadixBins;
   for (int i = threadIdx.x; i < kRadixPasses * kRadixBins; i += kTileThreads)
     if (sh[i]) atomicAdd(&hs[i], sh[i]);
 }
@@ -196,13 +237,8 @@ __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __re
 void launch_sort_passes(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_tmp,
                         uint32_t* vals_tmp, const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist,
                         uint32_t* status, uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
-  const uint32_t* kin[kRadixPasses] = {keys_in, keys_tmp, keys_out, keys_tmp};
-  uint32_t* kout[kRadixPasses] = {keys_tmp, keys_out, keys_tmp, keys_out};
-  const uint32_t* vin[kRadixPasses] = {nullptr, vals_tmp, vals_out, vals_tmp};
-  uint32_t* vout[kRadixPasses] = {vals_tmp, vals_out, vals_tmp, vals_out};
-  for (int p = 0; p < kRadixPasses; ++p)
-    k_onesweep<<<ntiles, kTileThreads, 0, st>>>(p, kin[p], vin[p], kout[p], vout[p], tiles, sys, hist, status,
-                                                 counters, ntiles, ctl);
+  run_passes<uint32_t>(kRadixPasses, keys_in, keys_out, vals_out, keys_tmp, vals_tmp, tiles, sys, hist, status,
+                       counters, ntiles, ctl, st);
 }
 
 void launch_code_hist(const StepBufs& b, cudaStream_t st) {
@@ -210,15 +246,14 @@ void launch_code_hist(const StepBufs& b, cudaStream_t st) {
 }
 
 void launch_sort(const StepBufs& b, cudaStream_t st) {
-  // pass 0: codes -> keys_alt (values: identity); 1: keys_alt -> codes;
-  // 2: codes -> keys_alt; 3: keys_alt -> codes. Final: (codes, order).
-  const uint32_t* kin[kRadixPasses] = {b.codes, b.keys_alt, b.codes, b.keys_alt};
-  uint32_t* kout[kRadixPasses] = {b.keys_alt, b.codes, b.keys_alt, b.codes};
-  const uint32_t* vin[kRadixPasses] = {nullptr, b.vals_alt, b.order, b.vals_alt};
-  uint32_t* vout[kRadixPasses] = {b.vals_alt, b.order, b.vals_alt, b.order};
-  for (int p = 0; p < kRadixPasses; ++p)
-    k_onesweep<<<b.ntiles, kTileThreads, 0, st>>>(p, kin[p], vin[p], kout[p], vout[p], b.tiles, b.sys, b.hist,
-                                                   b.sort_status, b.counters, b.ntiles, b.ctl);
+  // (codes, identity) -> (codes sorted, order) through (keys_alt, vals_alt).
+  if (b.key64)
+    run_passes<uint64_t>(kRadixPasses63, reinterpret_cast<const uint64_t*>(b.codes), reinterpret_cast<uint64_t*>(b.codes),
+                         b.order, reinterpret_cast<uint64_t*>(b.keys_alt), b.vals_alt, b.tiles, b.sys, b.hist,
+                         b.sort_status, b.counters, b.ntiles, b.ctl, st);
+  else
+    run_passes<uint32_t>(kRadixPasses, b.codes, b.codes, b.order, b.keys_alt, b.vals_alt, b.tiles, b.sys, b.hist,
+                         b.sort_status, b.counters, b.ntiles, b.ctl, st);
 }
 
 }  // namespace gx

@@ -112,6 +112,7 @@ __device__ __forceinline__ void make_bounds(const unsigned long long* e, Bounds&
   }
   b.size = dmul(2.0, half);
   b.scale = ddiv(1024.0, b.size);
+  b.scale63 = ddiv(2097152.0, b.size);
   // The float-float split keeps ~2^-48 of a coordinate; below that, distance
   // comparisons are re-done in FP64.
   double t = amax * 0x1p-40;
@@ -119,9 +120,10 @@ __device__ __forceinline__ void make_bounds(const unsigned long long* e, Bounds&
 }
 
 // One CTA per tile: Morton code of every particle of the tile (original order) and
-// the tile's contribution to the per-system digit histograms of all four radix
-// passes. The tile's system cube is rebuilt from the reduced lo/hi by every CTA (a
-// few flops), and the system's first tile publishes it for the host.
+// the tile's contribution to the per-system digit histograms of all radix passes
+// (4 for 30-bit keys, 8 for 63-bit). The tile's system cube is rebuilt from the
+// reduced lo/hi by every CTA (a few flops), and the system's first tile publishes it.
+template <bool K64>
 __global__ void __launch_bounds__(kTileThreads) k_morton_hist(const TileDesc* __restrict__ tiles,
                                                               const double* __restrict__ pos,
                                                               const unsigned long long* __restrict__ enc,
@@ -129,33 +131,43 @@ __global__ void __launch_bounds__(kTileThreads) k_morton_hist(const TileDesc* __
                                                               Bounds* __restrict__ bounds, uint32_t* __restrict__ codes,
                                                               uint32_t* __restrict__ lanes_out,
                                                               uint32_t* __restrict__ hist) {
-  __shared__ uint32_t sh[kRadixPasses][kRadixBins];
+  constexpr int P = K64 ? kRadixPasses63 : kRadixPasses;
+  __shared__ uint32_t sh[P][kRadixBins];
   __shared__ Bounds sb;
   const TileDesc t = tiles[blockIdx.x];
-  for (int i = threadIdx.x; i < kRadixPasses * kRadixBins; i += kTileThreads) (&sh[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < P * kRadixBins; i += kTileThreads) (&sh[0][0])[i] = 0;
   if (threadIdx.x == 0) {
     make_bounds(enc + 6 * (size_t)t.sys, sb);
     if (sys[t.sys].first_tile == blockIdx.x) bounds[t.sys] = sb;
   }
   __syncthreads();
-  const double bx = sb.bmin[0], by = sb.bmin[1], bz = sb.bmin[2], scale = sb.scale;
+  const double bx = sb.bmin[0], by = sb.bmin[1], bz = sb.bmin[2];
+  const double scale = K64 ? sb.scale63 : sb.scale;
   for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += kTileThreads) {
-    const uint32_t lx = quantize_lane(dmul(dsub(pos[3 * (size_t)i + 0], bx), scale));
-    const uint32_t ly = quantize_lane(dmul(dsub(pos[3 * (size_t)i + 1], by), scale));
-    const uint32_t lz = quantize_lane(dmul(dsub(pos[3 * (size_t)i + 2], bz), scale));
-    const uint32_t code = morton3(lx, ly, lz);
-    codes[i] = code;
-    if (lanes_out) {
-      lanes_out[3 * (size_t)i + 0] = lx;
-      lanes_out[3 * (size_t)i + 1] = ly;
-      lanes_out[3 * (size_t)i + 2] = lz;
-    }
+    const double vx = dmul(dsub(pos[3 * (size_t)i + 0], bx), scale);
+    const double vy = dmul(dsub(pos[3 * (size_t)i + 1], by), scale);
+    const double vz = dmul(dsub(pos[3 * (size_t)i + 2], bz), scale);
+    if (K64) {
+      const uint64_t code = morton3_63(quantize_lane21(vx), quantize_lane21(vy), quantize_lane21(vz));
+      reinterpret_cast<uint64_t*>(codes)[i] = code;
 #pragma unroll
-    for (int p = 0; p < kRadixPasses; ++p) atomicAdd(&sh[p][(code >> (p * kRadixBits)) & (kRadixBins - 1)], 1u);
+      for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(code >> (p * kRadixBits)) & (kRadixBins - 1)], 1u);
+    } else {
+      const uint32_t lx = quantize_lane(vx), ly = quantize_lane(vy), lz = quantize_lane(vz);
+      const uint32_t code = morton3(lx, ly, lz);
+      codes[i] = code;
+      if (lanes_out) {
+        lanes_out[3 * (size_t)i + 0] = lx;
+        lanes_out[3 * (size_t)i + 1] = ly;
+        lanes_out[3 * (size_t)i + 2] = lz;
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(code >> (p * kRadixBits)) & (kRadixBins - 1)], 1u);
+    }
   }
   __syncthreads();
-  uint32_t* hs = hist + (size_t)t.sys * kRadixPasses * kRadixBins;
-  for (int i = threadIdx.x; i < kRadixPasses * kRadixBins; i += kTileThreads) {
+  uint32_t* hs = hist + (size_t)t.sys * kMaxRadixPasses * kRadixBins;
+  for (int i = threadIdx.x; i < P * kRadixBins; i += kTileThreads) {
     const uint32_t c = (&sh[0][0])[i];
     if (c) atomicAdd(&hs[i], c);
   }
@@ -171,8 +183,12 @@ void launch_kick_half(const StepBufs& b, cudaStream_t st) {
 }
 
 void launch_morton_hist(const StepBufs& b, uint32_t* lanes_out, cudaStream_t st) {
-  k_morton_hist<<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds, b.codes, lanes_out,
-                                                    b.hist);
+  if (b.key64)
+    k_morton_hist<true><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds, b.codes,
+                                                            nullptr, b.hist);
+  else
+    k_morton_hist<false><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds, b.codes,
+                                                             lanes_out, b.hist);
 }
 
 }  // namespace gx

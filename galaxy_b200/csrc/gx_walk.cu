@@ -11,8 +11,8 @@
 // pairs kept in registers, entry j in lane j % 32); every node record is loaded once
 // per warp (a broadcast load) and each lane applies its OWN opening decision, so
 // every lane takes exactly the reference's set of terms for its target. A tree over
-// 30-bit codes with a 32-bit position tie-break is at most 63 levels deep, so 64
-// stack entries always suffice (overflow raises the device error word).
+// 30-bit (63-bit) codes with a 32-bit position tie-break is at most 63 (96) levels
+// deep, so 96 stack entries always suffice (overflow raises the device error word).
 //
 // FP32 mode: node centres of mass and leaf positions are float-float (hi + lo), so
 // dx = (c_hi - x_hi) + (c_lo - x_lo) keeps ~48 bits of the f64 coordinates; the
@@ -72,25 +72,25 @@ __device__ __noinline__ bool exact_accept(const Agg64* __restrict__ agg, uint32_
   return !inside && dmul(theta, dsub(d, delta)) >= s;
 }
 
+// Stack of (node, lane mask) entries shared by the warp: entry j lives in lane j % 32
+// of slot j / 32. 96 entries cover the deepest tree (kMaxDepth levels of at most one
+// pending sibling each, bounded by 30 + 32 or 63 + 32 prefix bits).
+constexpr int kStackCap = 96;
+
 struct WarpStack {
-  uint32_t u0, m0, u1, m1;
+  uint32_t u0, m0, u1, m1, u2, m2;
   int sp;
 };
 
 __device__ __forceinline__ bool stack_push(WarpStack& s, uint32_t u, uint32_t m, int lane) {
-  if (s.sp < 32) {
-    if (lane == s.sp) {
-      s.u0 = u;
-      s.m0 = m;
-    }
-  } else if (s.sp < 64) {
-    if (lane == s.sp - 32) {
-      s.u1 = u;
-      s.m1 = m;
-    }
-  } else {
-    return false;
-  }
+  if (s.sp >= kStackCap) return false;
+  const bool w0 = lane == s.sp, w1 = lane == s.sp - 32, w2 = lane == s.sp - 64;
+  s.u0 = w0 ? u : s.u0;
+  s.m0 = w0 ? m : s.m0;
+  s.u1 = w1 ? u : s.u1;
+  s.m1 = w1 ? m : s.m1;
+  s.u2 = w2 ? u : s.u2;
+  s.m2 = w2 ? m : s.m2;
   ++s.sp;
   return true;
 }
@@ -98,9 +98,9 @@ __device__ __forceinline__ bool stack_push(WarpStack& s, uint32_t u, uint32_t m,
 __device__ __forceinline__ void stack_pop(WarpStack& s, uint32_t& u, uint32_t& m) {
   --s.sp;
   const int src = s.sp & 31;
-  const bool lo = s.sp < 32;
-  u = __shfl_sync(0xffffffffu, lo ? s.u0 : s.u1, src);
-  m = __shfl_sync(0xffffffffu, lo ? s.m0 : s.m1, src);
+  const int slot = s.sp >> 5;
+  u = __shfl_sync(0xffffffffu, slot == 0 ? s.u0 : (slot == 1 ? s.u1 : s.u2), src);
+  m = __shfl_sync(0xffffffffu, slot == 0 ? s.m0 : (slot == 1 ? s.m1 : s.m2), src);
 }
 
 __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) k_walk_f64(StepBufs b, int persistent) {
       }
       double a64[3] = {0.0, 0.0, 0.0};
       unsigned long long n_leaf = 0, n_far = 0, n_open = 0, n_vis = 0;
-      WarpStack stk{0, 0, 0, 0, 0};
+      WarpStack stk{0, 0, 0, 0, 0, 0, 0};
       uint32_t u = n_total + sd.off;
       uint32_t mask = __ballot_sync(0xffffffffu, valid);
       const uint32_t max_iters = 2u * sd.n + 64u;
@@ -380,7 +380,8 @@ __global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int 
 #pragma unroll
         for (int c = 0; c < 3; ++c) L.xh[c] = L.xl[c] = 0.f;
       }
-      uint32_t sx0 = 0, sy0 = 0, sm0 = 0, sx1 = 0, sy1 = 0, sm1 = 0;  // pair stack, entry j in lane j%32
+      // pair stack of kStackCap entries: entry j in lane j % 32 of slot j / 32
+      uint32_t sx0 = 0, sy0 = 0, sm0 = 0, sx1 = 0, sy1 = 0, sm1 = 0, sx2 = 0, sy2 = 0, sm2 = 0;
       int sp = 0;
       const float4 r2 = __ldg(&rec[4 * (size_t)root + 2]);
       uint32_t cx = __float_as_uint(r2.x), cy = __float_as_uint(r2.y);
@@ -425,17 +426,20 @@ __global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int 
         const uint32_t n1x = __float_as_uint(k1.x), n1y = __float_as_uint(k1.y);
         if (m0 && m1) {
           // push the right child's pair; continue with the left child's
-          if (sp >= 64) {
+          if (sp >= kStackCap) {
             bad = true;
             break;
           }
-          const bool w0 = lane == sp, w1 = lane == sp - 32;
+          const bool w0 = lane == sp, w1 = lane == sp - 32, w2 = lane == sp - 64;
           sx0 = w0 ? n1x : sx0;
           sy0 = w0 ? n1y : sy0;
           sm0 = w0 ? m1 : sm0;
           sx1 = w1 ? n1x : sx1;
           sy1 = w1 ? n1y : sy1;
           sm1 = w1 ? m1 : sm1;
+          sx2 = w2 ? n1x : sx2;
+          sy2 = w2 ? n1y : sy2;
+          sm2 = w2 ? m1 : sm2;
           ++sp;
         }
         if (m0) {
@@ -450,10 +454,10 @@ __global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int 
           if (sp == 0) break;
           --sp;
           const int src = sp & 31;
-          const bool lo = sp < 32;
-          cx = __shfl_sync(0xffffffffu, lo ? sx0 : sx1, src);
-          cy = __shfl_sync(0xffffffffu, lo ? sy0 : sy1, src);
-          mask = __shfl_sync(0xffffffffu, lo ? sm0 : sm1, src);
+          const int slot = sp >> 5;
+          cx = __shfl_sync(0xffffffffu, slot == 0 ? sx0 : (slot == 1 ? sx1 : sx2), src);
+          cy = __shfl_sync(0xffffffffu, slot == 0 ? sy0 : (slot == 1 ? sy1 : sy2), src);
+          mask = __shfl_sync(0xffffffffu, slot == 0 ? sm0 : (slot == 1 ? sm1 : sm2), src);
         }
       }
     }

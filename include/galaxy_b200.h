@@ -47,6 +47,10 @@ extern "C" {
 #define GX_FLAG_NO_KAHAN 1u     /* plain FP32 accumulation in the F32 walk */
 #define GX_FLAG_STATS 2u        /* count interactions/openings per call (slower) */
 #define GX_FLAG_STAGE_TIMES 4u  /* time each stage with CUDA events (eager launches) */
+#define GX_FLAG_MORTON63 8u     /* 63-bit Morton keys (21 bits per axis) instead of the reference's
+                                   30-bit keys: the refinement the reference defers
+                                   (solvers/src/lbvh.rs:29-32) for dense cores and heavy tails;
+                                   changes the tree, so it is not a reference-parity mode */
 
 typedef struct gx_options {
   uint32_t struct_size;    /* sizeof(gx_options); 0 means "all defaults" */

@@ -122,6 +122,18 @@ inline int64_t delta(const uint32_t* codes, int64_t n, int64_t a, int64_t b) {
   return __builtin_clz(ca ^ cb);
 }
 
+// The same prefix over 63-bit codes (extension with no reference counterpart: the
+// 21-bit-per-axis keys the reference defers, solvers/src/lbvh.rs:29-32).
+inline int64_t delta(const uint64_t* codes, int64_t n, int64_t a, int64_t b) {
+  if (b < 0 || b >= n) return -1;
+  uint64_t ca = codes[a], cb = codes[b];
+  if (ca == cb) {
+    uint32_t x = static_cast<uint32_t>(a) ^ static_cast<uint32_t>(b);
+    return 64 + (x == 0 ? 32 : __builtin_clz(x));
+  }
+  return __builtin_clzll(ca ^ cb);
+}
+
 struct ChildRef {
   bool leaf;
   int64_t idx;
@@ -129,7 +141,8 @@ struct ChildRef {
 
 // solvers/src/lbvh.rs:195-240 -- Karras 2012 determineRange + findSplit with
 // signed indices.
-void karras_node(const uint32_t* codes, int64_t n, int64_t i, ChildRef* left, ChildRef* right) {
+template <typename K>
+void karras_node(const K* codes, int64_t n, int64_t i, ChildRef* left, ChildRef* right) {
   auto d0 = [&](int64_t a, int64_t b) { return delta(codes, n, a, b); };
   int64_t dir = d0(i, i + 1) > d0(i, i - 1) ? 1 : -1;
   int64_t delta_min = d0(i, i - dir);
@@ -179,7 +192,8 @@ struct Tree {
 };
 
 // solvers/src/lbvh.rs:276-306
-Tree reference_karras(const uint32_t* sorted_codes, size_t n) {
+template <typename K>
+Tree reference_karras(const K* sorted_codes, size_t n) {
   Tree t;
   t.n = n;
   t.left.assign(n - 1, 0);
@@ -296,7 +310,8 @@ Flat reference_flatten(const Tree& t, const AggOut& a, const uint32_t* order) {
 }
 
 // solvers/src/lbvh.rs:143-147 -- stable by (code, original index).
-std::vector<uint32_t> reference_sort(const uint32_t* codes, size_t n) {
+template <typename K>
+std::vector<uint32_t> reference_sort(const K* codes, size_t n) {
   std::vector<uint32_t> order(n);
   std::iota(order.begin(), order.end(), 0u);
   std::stable_sort(order.begin(), order.end(),
@@ -304,8 +319,27 @@ std::vector<uint32_t> reference_sort(const uint32_t* codes, size_t n) {
   return order;
 }
 
-// solvers/src/lbvh.rs:440-463
-Flat lbvh_build(const double* pos, const double* mass, size_t n) {
+// 63-bit Morton code of a position (21-bit lanes; same cube as the 30-bit codes).
+uint64_t expand21(uint32_t v) {
+  uint64_t x = v & 0x1fffffu;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+uint32_t quantize_lane21(double v) {
+  double f = std::fmax(std::floor(v), 0.0);
+  uint32_t q = f >= 4294967295.0 ? 0xFFFFFFFFu : static_cast<uint32_t>(f);
+  return std::min(q, (1u << 21) - 1);
+}
+
+template <typename K>
+std::vector<K> morton_codes(const double* pos, size_t n);
+
+template <>
+std::vector<uint32_t> morton_codes<uint32_t>(const double* pos, size_t n) {
   Bounds b = morton_bounds(pos, n);
   std::vector<uint32_t> codes(n);
   for (size_t i = 0; i < n; ++i) {
@@ -313,8 +347,29 @@ Flat lbvh_build(const double* pos, const double* mass, size_t n) {
     codes[i] = morton3(quantize_lane((p.x - b.bmin.x) * b.scale), quantize_lane((p.y - b.bmin.y) * b.scale),
                        quantize_lane((p.z - b.bmin.z) * b.scale));
   }
+  return codes;
+}
+
+template <>
+std::vector<uint64_t> morton_codes<uint64_t>(const double* pos, size_t n) {
+  Bounds b = morton_bounds(pos, n);
+  const double scale = 2097152.0 / b.size;
+  std::vector<uint64_t> codes(n);
+  for (size_t i = 0; i < n; ++i) {
+    V3 p = load3(pos, i);
+    codes[i] = expand21(quantize_lane21((p.x - b.bmin.x) * scale)) |
+               (expand21(quantize_lane21((p.y - b.bmin.y) * scale)) << 1) |
+               (expand21(quantize_lane21((p.z - b.bmin.z) * scale)) << 2);
+  }
+  return codes;
+}
+
+// solvers/src/lbvh.rs:440-463 (K = uint32_t is the reference; uint64_t the 63-bit extension)
+template <typename K = uint32_t>
+Flat lbvh_build(const double* pos, const double* mass, size_t n) {
+  std::vector<K> codes = morton_codes<K>(pos, n);
   std::vector<uint32_t> order = reference_sort(codes.data(), n);
-  std::vector<uint32_t> sc(n);
+  std::vector<K> sc(n);
   std::vector<V3> sp(n);
   std::vector<double> sm(n);
   for (size_t k = 0; k < n; ++k) {
@@ -591,6 +646,29 @@ int or_lbvh_accelerations(size_t n, const double* pos, const double* mass, doubl
       tf += st.far;
       to += st.open;
     }
+  }
+  if (stats) {
+    stats[0] = tl;
+    stats[1] = tf;
+    stats[2] = to;
+  }
+  return 0;
+}
+
+// The same solver over 63-bit Morton keys (extension: no reference counterpart).
+int or_lbvh_accelerations_k63(size_t n, const double* pos, const double* mass, double g, double softening,
+                              double theta, double* acc_out, int threads, uint64_t* stats) {
+  if (n == 0) return 0;
+  Flat f = lbvh_build<uint64_t>(pos, mass, n);
+  const double eps2 = softening * softening;
+  uint64_t tl = 0, tf = 0, to = 0;
+#pragma omp parallel for num_threads(threads > 1 ? threads : 1) schedule(dynamic, 256) reduction(+ : tl, tf, to)
+  for (long long i = 0; i < static_cast<long long>(n); ++i) {
+    WalkStats st{0, 0, 0};
+    store3(acc_out, i, lbvh_accel(f, i, pos, mass, theta, eps2, stats ? &st : nullptr) * g);
+    tl += st.leaf;
+    tf += st.far;
+    to += st.open;
   }
   if (stats) {
     stats[0] = tl;

@@ -53,6 +53,7 @@ def lib():
             "or_lbvh_flat": (i, [sz, _f64p, _f64p, _f64p, _u32p, _u32p]),
             "or_lbvh_accelerations": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i, C.c_void_p]),
             "or_lbvh_accelerations_subset": (i, [sz, _f64p, _f64p, d, d, d, sz, _u32p, _f64p, i]),
+            "or_lbvh_accelerations_k63": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i, C.c_void_p]),
             "or_lbvh_accelerations_quad": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i]),
             "or_direct_sum": (None, [sz, _f64p, _f64p, d, d, _f64p]),
             "or_direct_sum_targets": (None, [sz, _f64p, _f64p, d, d, sz, _u32p, _f64p, i]),
@@ -169,6 +170,19 @@ def lbvh_accelerations(pos, mass, g, softening, theta, threads: int = 1, stats: 
     st = np.zeros(3, np.uint64)
     lib().or_lbvh_accelerations(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g, softening, theta,
                                 acc.reshape(-1), threads, st.ctypes.data if stats else None)
+    if stats:
+        return acc, {"leaf": int(st[0]), "far": int(st[1]), "open": int(st[2])}
+    return acc
+
+
+def lbvh_accelerations_k63(pos, mass, g, softening, theta, threads: int = 1, stats: bool = False):
+    """The same solver over 63-bit Morton keys (extension; no reference counterpart)."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3))
+    st = np.zeros(3, np.uint64)
+    lib().or_lbvh_accelerations_k63(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g, softening, theta,
+                                    acc.reshape(-1), threads, st.ctypes.data if stats else None)
     if stats:
         return acc, {"leaf": int(st[0]), "far": int(st[1]), "open": int(st[2])}
     return acc
