@@ -43,7 +43,7 @@ def _compile(src: str, verbose_ptxas: bool) -> str:
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), _deps_mtime()):
         return obj
-    cmd = [_nvcc(), "-ccbin", _host_cxx(), "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC",
+    cmd = [_nvcc(), "-ccbin", _host_cxx(), "-std=c++17", "-O3", "-lineinfo", "-ftz=true", *ARCH, "-Xcompiler", "-fPIC",
            "-Xcompiler", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
     if src.endswith(".cu"):
         cmd[1:1] = ["-x", "cu"]

@@ -84,9 +84,9 @@ size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
   size_t s = 0;
   s += 3 * 3 * n * 8 + n * 8;                 // pos, vel, acc, mass
   s += 6 * n * 4;                             // codes, keys_alt (u64-capable), order, vals_alt
-  s += n * 32 + 2 * n * 64;                   // leaf64, walk records (leaves + internal)
+  s += n * 32 + n * 80;                       // leaf64, sibling-pair walk records
   s += n * 8 + 2 * n * 4 + n * sizeof(Agg64); // kids, parent, agg64
-  s += n * 16;                                // nodeD
+  s += 2 * n * 16;                            // nodeC, nodeD
   s += n * 8;                                 // slots
   if (quad) s += 2 * n * 16 + 6 * n * 8;
   if (f64rec) s += n * sizeof(Node64);
@@ -133,10 +133,11 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   GX_A(b.order, nn, uint32_t);
   GX_A(b.vals_alt, nn, uint32_t);
   GX_A(b.leaf64, nn, double4);
-  GX_A(b.rec, 8 * nn, float4);  // 4 per unified node, 2n nodes
+  GX_A(b.pairs, 5 * nn, float4);  // sibling-pair walk records, one per internal node
   GX_A(b.kids, nn, uint2);
   GX_A(b.parent, 2 * nn, uint32_t);
   GX_A(b.agg64, nn, Agg64);
+  GX_A(b.nodeC, nn, float4);
   GX_A(b.nodeD, nn, float4);
   if (q) {
     GX_A(b.nodeQ, 2 * nn, float4);
@@ -784,7 +785,7 @@ int gx_stage_morton(gx_handle* h, size_t n, const double* pos, uint32_t* lanes_o
   GX_CK(h, cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, h->stream));
   launch_kick_drift_bbox(b, 0, 0, h->stream);
   // Lanes (3n u32) are staged in the walk records, unused by this stage.
-  uint32_t* d_lanes = lanes_out ? reinterpret_cast<uint32_t*>(b.rec) : nullptr;
+  uint32_t* d_lanes = lanes_out ? reinterpret_cast<uint32_t*>(b.pairs) : nullptr;
   launch_morton_hist(b, d_lanes, h->stream);
   GX_CK(h, cudaMemcpyAsync(codes_out, b.codes, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   if (lanes_out)

@@ -56,6 +56,54 @@ __device__ __forceinline__ void quad_shift_add(const double q[6], double m, cons
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
+// One child's half of its parent's sibling-pair walk record (FP32).
+struct ChildRec {
+  float hx, hy, hz, lx, ly, lz, m, take, open;
+};
+
+// Geometry of an aggregate as reference_flatten derives it (solvers/src/lbvh.rs:602-613).
+__device__ __forceinline__ void node_geometry(const AggR& a, double ctr[3], double hf[3], double& delta, double& s) {
+  double dv[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    ctr[c] = dmul(dadd(a.mn[c], a.mx[c]), 0.5);
+    hf[c] = dmul(dsub(a.mx[c], a.mn[c]), 0.5);
+    dv[c] = dsub(a.com[c], ctr[c]);
+  }
+  delta = dsqrt(dlen2(dv[0], dv[1], dv[2]));
+  s = dmul(2.0, fmax(hf[0], fmax(hf[1], hf[2])));
+}
+
+// FP32 record of a child: float-float centre of mass, mass, and the d^2 thresholds.
+// A leaf is always a term (take -1, open -2). An internal node is taken above
+// rcrit^2 (1 + band) + tiny2 and opened below rcrit^2 (1 - band) - tiny2, rcrit =
+// s/theta + delta; in between the walk re-decides in FP64. NaN thresholds (theta = 0,
+// a zero-size or a massless node; a massless leaf) send every visit to the FP64 path,
+// which applies the reference's rules exactly.
+__device__ __forceinline__ ChildRec child_record(const AggR& a, bool leaf, double theta, double tiny2) {
+  ChildRec r;
+  split_ff(a.com[0], r.hx, r.lx);
+  split_ff(a.com[1], r.hy, r.ly);
+  split_ff(a.com[2], r.hz, r.lz);
+  r.m = __double2float_rn(a.m);
+  const float nan = __int_as_float(0x7fffffff);
+  if (leaf) {
+    r.take = a.m > 0.0 ? -1.f : nan;
+    r.open = -2.f;
+  } else {
+    double ctr[3], hf[3], delta, s;
+    node_geometry(a, ctr, hf, delta, s);
+    r.take = r.open = nan;
+    if (theta > 0.0 && s > 0.0 && a.m > 0.0) {
+      const double rc = s / theta + delta;
+      const double rc2 = rc * rc;
+      r.take = __double2float_ru(rc2 * (1.0 + kOpenBand) + tiny2);
+      r.open = __double2float_rd(rc2 * (1.0 - kOpenBand) - tiny2);
+    }
+  }
+  return r;
+}
+
 }  // namespace
 
 template <bool QUAD, typename K>
@@ -82,15 +130,6 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
     for (int c = 0; c < 3; ++c) cur.com[c] = pos[3 * (size_t)o + c];
     cur.m = mass[o];
     b.leaf64[k] = make_double4(cur.com[0], cur.com[1], cur.com[2], cur.m);
-    {
-      float h[3], l[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) split_ff(cur.com[c], h[c], l[c]);
-      b.rec[4 * (size_t)k] = make_float4(h[0], h[1], h[2], __double2float_rn(cur.m));
-      // Take threshold -1: below any squared distance, so the walk always takes a leaf
-      // as a term (the reference's leaf rule) without an opening test.
-      b.rec[4 * (size_t)k + 1] = make_float4(l[0], l[1], l[2], -1.f);
-    }
     if (ns == 1) {
       b.parent[k] = kNoParent;
       continue;
@@ -101,6 +140,7 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
     uint32_t l = k - off, r = k - off;  // local leaf range of the current node
     uint32_t cur_u = k;                 // unified index of the current node
     uint32_t lc = 0, rc = 0;            // children of the current node (if internal)
+    ChildRec pl, pr;                    // their halves of the node's walk record
     bool internal = false;
     for (int level = 0; level < kMaxDepth; ++level) {
       const bool root = (l == 0 && r == ns - 1);
@@ -133,35 +173,15 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
         }
         a.m = cur.m;
         b.agg64[gi] = a;
-        // Geometry as reference_flatten derives it (solvers/src/lbvh.rs:602-613).
-        double ctr[3], hf[3], dv[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          ctr[c] = dmul(dadd(cur.mn[c], cur.mx[c]), 0.5);
-          hf[c] = dmul(dsub(cur.mx[c], cur.mn[c]), 0.5);
-          dv[c] = dsub(cur.com[c], ctr[c]);
-        }
-        const double delta = dsqrt(dlen2(dv[0], dv[1], dv[2]));
-        const double s = dmul(2.0, fmax(hf[0], fmax(hf[1], hf[2])));
-        // Opening thresholds on d^2 for the FP32 walk: take the monopole above
-        // rcrit^2 (1 + band) + tiny2, open below rcrit^2 (1 - band) - tiny2, and
-        // re-decide in FP64 in between, with rcrit = s/theta + delta. NaN (theta = 0
-        // or a zero-size node) sends every visit to the FP64 re-check.
-        float take = __int_as_float(0x7fffffff), open = __int_as_float(0x7fffffff);
-        if (theta > 0.0 && s > 0.0) {
-          const double rc = s / theta + delta;
-          const double rc2 = rc * rc;
-          take = __double2float_ru(rc2 * (1.0 + kOpenBand) + tiny2);
-          open = __double2float_rd(rc2 * (1.0 - kOpenBand) - tiny2);
-        }
-        float hh[3], ll[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) split_ff(cur.com[c], hh[c], ll[c]);
-        float4* rp = b.rec + 4 * (size_t)u;
-        rp[0] = make_float4(hh[0], hh[1], hh[2], __double2float_rn(cur.m));
-        rp[1] = make_float4(ll[0], ll[1], ll[2], take);
-        rp[2] = make_float4(__uint_as_float(lc), __uint_as_float(rc), open, 0.f);
-        rp[3] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
+        double ctr[3], hf[3], delta, s;
+        node_geometry(cur, ctr, hf, delta, s);
+        float4* pp = b.pairs + 5 * (size_t)gi;
+        pp[0] = make_float4(pl.hx, pr.hx, pl.hy, pr.hy);
+        pp[1] = make_float4(pl.hz, pr.hz, pl.m, pr.m);
+        pp[2] = make_float4(pl.lx, pr.lx, pl.ly, pr.ly);
+        pp[3] = make_float4(pl.lz, pr.lz, pl.take, pr.take);
+        pp[4] = make_float4(pl.open, pr.open, __uint_as_float(lc), __uint_as_float(rc));
+        b.nodeC[gi] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
         b.nodeD[gi] = make_float4(__double2float_rn(hf[0]), __double2float_rn(hf[1]), __double2float_rn(hf[2]), 0.f);
         if (f64rec) {
           Node64 nd;
@@ -235,6 +255,12 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
         lc = sib_u;
         rc = cur_u;
         l = sib_far;
+      }
+      {
+        const AggR& CL = is_left ? cur : sib;
+        const AggR& CR = is_left ? sib : cur;
+        pl = child_record(CL, lc < n_total, theta, tiny2);
+        pr = child_record(CR, rc < n_total, theta, tiny2);
       }
       if (QUAD) {
         // Q_parent = shift(Q_left) + shift(Q_right), left first (oracle order).

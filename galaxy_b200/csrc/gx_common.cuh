@@ -8,16 +8,14 @@
 //   sorted leaves (leaf k = k-th particle in (code, index) order):
 //     leaf64[k] = double4(x, y, z, m)          FP64 payload for folds and rechecks
 //     order[k]  original index
-//   walk records, 4 float4 per unified node u (leaves [0, N), internal i at N + i):
-//     rec[4u+0] = (com_hi.xyz, mass)     float-float split of the centre of mass
-//     rec[4u+1] = (com_lo.xyz, take)     take: d^2 threshold to take the monopole
-//     rec[4u+2] = (left, right, open, 0) children and the d^2 threshold to open
-//     rec[4u+3] = (center.xyz, 0)        AABB centre (opening test, theta >= 1/sqrt 3)
+//   sibling-pair walk records, 5 float4 per internal node i: both children side by
+//   side (L, R) -- hi/lo float-float centre of mass, mass, the FP32 d^2 thresholds to
+//   take / to open, and the children's unified indices (see StepBufs::pairs)
 //   internal node i (Karras numbering, unified index N + i):
 //     kids[i]   = uint2(left, right) unified children
 //     parent[u] unified parent of every node (root: 0xFFFFFFFF)
 //     agg64[i]  = {aabb_min[3], aabb_max[3], com[3], mass} FP64 (bit-exact fold)
-//     nodeD[i]  = float4(half.xyz, 0)  AABB half extents (theta >= 1/sqrt 3)
+//     nodeC[i], nodeD[i] = AABB centre, half extents (FP32; theta >= 1/sqrt 3)
 //     nodeQ[i]  = 2 x float4 traceless quadrupole (xx, xy, xz, yy), (yz, zz, 0, 0)
 //     node64[i] = {center[3], half[3], com[3], mass, delta, s}  FP64 walk record
 #pragma once

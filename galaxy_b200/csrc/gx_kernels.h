@@ -35,16 +35,19 @@ struct StepBufs {
   uint32_t* vals_alt = nullptr;
   // leaves, sorted order
   double4* leaf64 = nullptr;
-  // Walk records, 4 float4 per unified node u (leaves [0, n), internal node i at n + i):
-  //   rec[4u+0] = (com_hi.xyz, mass)       rec[4u+1] = (com_lo.xyz, take threshold)
-  //   rec[4u+2] = (left, right, open threshold, 0)   rec[4u+3] = (center.xyz, 0)
-  // A leaf has only the first two (take threshold -1: always a term).
-  float4* rec = nullptr;
+  // Sibling-pair walk records, 5 float4 per internal node i: its two children side by
+  // side (L, R), so a float4 load yields float2 (L, R) operand pairs:
+  //   pairs[5i+0] = (x_hi L, R, y_hi L, R)   pairs[5i+1] = (z_hi L, R, mass L, R)
+  //   pairs[5i+2] = (x_lo L, R, y_lo L, R)   pairs[5i+3] = (z_lo L, R, take L, R)
+  //   pairs[5i+4] = (open L, R, child L, child R)   (children as unified indices)
+  // take / open: d^2 thresholds of the FP32 opening test (leaf: take -1, open -2).
+  float4* pairs = nullptr;
   // internal nodes
   uint2* kids = nullptr;
   uint32_t* parent = nullptr;
   Agg64* agg64 = nullptr;
-  float4* nodeD = nullptr;   // half extents (opening test for theta >= 1/sqrt 3)
+  float4* nodeC = nullptr;   // AABB centre (opening test for theta >= 1/sqrt 3)
+  float4* nodeD = nullptr;   // AABB half extents (same)
   float4* nodeQ = nullptr;   // 2 per node (quadrupole mode)
   double* q64 = nullptr;     // 6 per node (quadrupole mode)
   Node64* node64 = nullptr;  // FP64 walk mode

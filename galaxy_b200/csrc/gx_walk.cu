@@ -50,11 +50,13 @@ __device__ __forceinline__ void acc_add(Acc32& a, float tx, float ty, float tz) 
   }
 }
 
-// The reference's opening test (solvers/src/lbvh.rs:505-514) in f64 on the node's
-// f64 aggregate, geometry derived as in reference_flatten (lbvh.rs:602-613).
-__device__ __noinline__ bool exact_accept(const Agg64* __restrict__ agg, uint32_t gi, const double x[3],
-                                          double theta) {
+// The reference's decision for internal node gi (solvers/src/lbvh.rs:485-514) in f64
+// on the node's f64 aggregate, geometry derived as in reference_flatten
+// (lbvh.rs:602-613): 1 = take the monopole, 0 = open, -1 = skip (massless subtree).
+__device__ __noinline__ int exact_decision(const Agg64* __restrict__ agg, uint32_t gi, const double x[3],
+                                           double theta) {
   const Agg64& a = agg[gi];
+  if (!(a.m > 0.0)) return -1;
   double ctr[3], hf[3], dv[3], dx[3];
   bool inside = true;
 #pragma unroll
@@ -69,7 +71,7 @@ __device__ __noinline__ bool exact_accept(const Agg64* __restrict__ agg, uint32_
   const double d2 = dlen2(dx[0], dx[1], dx[2]);
   const double s = dmul(2.0, fmax(hf[0], fmax(hf[1], hf[2])));
   const double d = dsqrt(d2);
-  return !inside && dmul(theta, dsub(d, delta)) >= s;
+  return (!inside && dmul(theta, dsub(d, delta)) >= s) ? 1 : 0;
 }
 
 // Stack of (node, lane mask) entries shared by the warp: entry j lives in lane j % 32
@@ -237,238 +239,250 @@ __global__ void __launch_bounds__(256) k_walk_f64(StepBufs b, int persistent) {
 
 namespace {
 
-// Per-lane state of the FP32 walk.
-struct Lane32 {
-  float xh[3], xl[3];
-  uint32_t k;
-  float eps2f;
-  double theta;
-};
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-// FP32 opening decision state of one child for one lane.
-struct Child32 {
-  float dx, dy, dz, d2;
-  bool take, open, amb;
-};
-
-// Distance and threshold tests of node u (A = rec[4u], B = rec[4u+1], open_thr =
-// rec[4u+2].z, -2 for leaves) for a lane; no branches. take: a term; open: descend;
-// amb: the FP32 value is inside the guard band and must be re-decided in FP64.
-template <bool INSIDE>
-__device__ __forceinline__ Child32 classify(const StepBufs& b, const Lane32& L, bool act, uint32_t u,
-                                            const float4& A, const float4& B, float open_thr, uint32_t n_total) {
-  Child32 c;
-  c.dx = (A.x - L.xh[0]) + (B.x - L.xl[0]);
-  c.dy = (A.y - L.xh[1]) + (B.y - L.xl[1]);
-  c.dz = (A.z - L.xh[2]) + (B.z - L.xl[2]);
-  c.d2 = fmaf(c.dx, c.dx, fmaf(c.dy, c.dy, c.dz * c.dz));
-  // The target itself and massless subtrees are skipped (lbvh.rs:485-496).
-  const bool ok = act && (u != L.k) && (A.w > 0.f);
-  c.take = ok && (c.d2 > B.w);  // B.w: take threshold (-1 for leaves)
-  c.open = ok && (c.d2 < open_thr);
-  c.amb = ok && !c.take && !c.open;
-  if (INSIDE && u >= n_total) {
-    const float4 nc = __ldg(&b.rec[4 * (size_t)u + 3]);
-    const float4 nd4 = __ldg(&b.nodeD[u - n_total]);
-    const float q0 = fabsf(L.xh[0] - nc.x) - nd4.x;
-    const float q1 = fabsf(L.xh[1] - nc.y) - nd4.y;
-    const float q2 = fabsf(L.xh[2] - nc.z) - nd4.z;
-    const float t0 = 0x1p-20f * (fabsf(nc.x) + nd4.x) + 1e-30f;
-    const float t1 = 0x1p-20f * (fabsf(nc.y) + nd4.y) + 1e-30f;
-    const float t2 = 0x1p-20f * (fabsf(nc.z) + nd4.z) + 1e-30f;
-    const bool near_face = fabsf(q0) <= t0 || fabsf(q1) <= t1 || fabsf(q2) <= t2;
-    const bool inside = q0 < 0.f && q1 < 0.f && q2 < 0.f;
-    const bool t = c.take;
-    c.take = t && !near_face && !inside;
-    c.open = c.open || (t && !near_face && inside);
-    c.amb = c.amb || (t && near_face);
-  }
-  return c;
-}
-
-// The term of a taken node (Plummer-softened monopole, plus the quadrupole of an
-// internal node in QUAD mode), scaled by `take` (0 or 1) and added to t[].
-template <bool QUAD>
-__device__ __forceinline__ void add_term(const StepBufs& b, const Lane32& L, const Child32& c, bool take, float m,
-                                         uint32_t u, uint32_t n_total, float t[3]) {
-  const float r2 = c.d2 + L.eps2f;
-  const float inv = rsqrtf(r2);
+// FP32 term of one taken internal child's quadrupole (r = x - com = -d):
+// a += Q r / r^5 - 2.5 (r.Q r) r / r^7, with r^2 softened like the monopole.
+__device__ __forceinline__ void quad_term(const float4& qa, const float4& qb, float dx, float dy, float dz, float inv,
+                                          float t[3]) {
   const float inv2 = inv * inv;
-  const float inv3 = inv * inv2;
-  const float f = take ? m * inv3 : 0.f;
-  t[0] = fmaf(c.dx, f, t[0]);
-  t[1] = fmaf(c.dy, f, t[1]);
-  t[2] = fmaf(c.dz, f, t[2]);
-  if (QUAD && u >= n_total) {
-    const uint32_t gi = u - n_total;
-    const float4 qa = __ldg(&b.nodeQ[2 * (size_t)gi]);
-    const float4 qb = __ldg(&b.nodeQ[2 * (size_t)gi + 1]);
-    // r = x - com = -d;  a += Q r / r^5 - 2.5 (r.Q r) r / r^7
-    const float rx = -c.dx, ry = -c.dy, rz = -c.dz;
-    const float qx = qa.x * rx + qa.y * ry + qa.z * rz;
-    const float qy = qa.y * rx + qa.w * ry + qb.x * rz;
-    const float qz = qa.z * rx + qb.x * ry + qb.y * rz;
-    const float rqr = rx * qx + ry * qy + rz * qz;
-    const float inv5 = take ? inv3 * inv2 : 0.f;
-    const float c7 = 2.5f * rqr * inv5 * inv2;
-    t[0] += qx * inv5 - rx * c7;
-    t[1] += qy * inv5 - ry * c7;
-    t[2] += qz * inv5 - rz * c7;
-  }
+  const float inv5 = inv2 * inv2 * inv;
+  const float rx = -dx, ry = -dy, rz = -dz;
+  const float qx = qa.x * rx + qa.y * ry + qa.z * rz;
+  const float qy = qa.y * rx + qa.w * ry + qb.x * rz;
+  const float qz = qa.z * rx + qb.x * ry + qb.y * rz;
+  const float rqr = rx * qx + ry * qy + rz * qz;
+  const float c7 = 2.5f * rqr * inv5 * inv2;
+  t[0] += qx * inv5 - rx * c7;
+  t[1] += qy * inv5 - ry * c7;
+  t[2] += qz * inv5 - rz * c7;
 }
 
-__device__ __forceinline__ void resolve_amb(const StepBufs& b, const Lane32& L, Child32& c, uint32_t u,
-                                            uint32_t n_total) {
-  if (c.amb) {
-    const double4 p = b.leaf64[L.k];
+// Opening test for theta >= 1/sqrt(3): the target inside the child's AABB must open it.
+// Returns the adjusted (take, open, amb) of a child whose distance test said "take".
+__device__ __forceinline__ void inside_test(const StepBufs& b, const float xh[3], uint32_t gi, bool& take, bool& open,
+                                            bool& amb) {
+  const float4 nc = __ldg(&b.nodeC[gi]);
+  const float4 nd4 = __ldg(&b.nodeD[gi]);
+  const float q0 = fabsf(xh[0] - nc.x) - nd4.x;
+  const float q1 = fabsf(xh[1] - nc.y) - nd4.y;
+  const float q2 = fabsf(xh[2] - nc.z) - nd4.z;
+  const float t0 = 0x1p-20f * (fabsf(nc.x) + nd4.x) + 1e-30f;
+  const float t1 = 0x1p-20f * (fabsf(nc.y) + nd4.y) + 1e-30f;
+  const float t2 = 0x1p-20f * (fabsf(nc.z) + nd4.z) + 1e-30f;
+  const bool near_face = fabsf(q0) <= t0 || fabsf(q1) <= t1 || fabsf(q2) <= t2;
+  const bool inside = q0 < 0.f && q1 < 0.f && q2 < 0.f;
+  const bool t = take;
+  take = t && !near_face && !inside;
+  open = open || (t && !near_face && inside);
+  amb = amb || (t && near_face);
+}
+
+// FP64 decision of an undecided child u (a leaf is undecided only when massless: skip).
+__device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double theta, uint32_t u, uint32_t n_total,
+                                        bool& take, bool& open) {
+  int dec = -1;
+  if (u >= n_total) {
+    const double4 p = b.leaf64[k];
     const double x[3] = {p.x, p.y, p.z};
-    const bool acc = exact_accept(b.agg64, u - n_total, x, L.theta);
-    c.take = acc;
-    c.open = !acc;
+    dec = exact_decision(b.agg64, u - n_total, x, theta);
   }
+  take = dec == 1;
+  open = dec == 0;
 }
 
 }  // namespace
 
-// FP32 walk: each iteration decides the two children of one opened node for every
-// lane that opened it; their terms are summed and added to the lane's Kahan-
-// compensated accumulator. A node's record carries its children and both FP32
-// thresholds, so the next pair to decide is known from the records just loaded (one
-// dependent load per iteration), and the stack holds ready-to-load child pairs. The
-// decisions are predicated (no per-lane branches); the rare FP64 re-check runs only
-// when some lane of the warp needs it. Indices are clamped into the record array, so
-// even a corrupt tree cannot read out of bounds; a clamp or an exhausted iteration
-// budget raises the device error word. Each lane takes exactly the reference's set of
-// terms; only the order of summation differs from the FP64 walk.
 #ifndef GX_WALK_MINB
 #define GX_WALK_MINB 3  // resident 256-thread blocks per SM the register budget is sized for
 #endif
 
+// FP32 walk over sibling-pair records. Each iteration decides both children of one
+// opened internal node for every lane that opened it: the pair's record is five
+// float4 loads, laid out so that every component pair is a float2 (left, right), and
+// the distance, threshold and force arithmetic of the two children runs as sm_100
+// packed FP32 instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn). Terms of two
+// iterations are summed and added to the lane's Kahan-compensated accumulator. The
+// record carries the children's indices, so the next pair is known from the record
+// just loaded (one dependent load per iteration); the warp's stack of pending pairs
+// lives in shared memory. Indices are clamped into the record array, so even a
+// corrupt tree cannot read out of bounds; a clamp or an exhausted iteration budget
+// raises the device error word. Each lane takes exactly the reference's set of
+// terms; only the order of summation differs from the FP64 walk.
 template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
 __global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int persistent) {
+  __shared__ uint2 s_stack[256 / 32][kStackCap];  // (internal node, lane mask)
   const int lane = threadIdx.x & 31;
+  uint2* stack = s_stack[threadIdx.x >> 5];
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
   uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_total = b.n;
-  const uint32_t umax = 2 * n_total - 2;  // largest unified node index
-  const float4* __restrict__ rec = b.rec;
+  const float4* __restrict__ pairs = b.pairs;
   while (item < b.nitems) {
     const WalkItem it = b.items[item];
     const SysDesc sd = b.sys[it.sys];
     const uint32_t end = sd.off + sd.n;
-    Lane32 L;
-    L.k = it.begin + lane;
-    const bool valid = L.k < end;
-    Acc32 acc = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    const uint32_t k = it.begin + lane;
+    const bool valid = k < end;
+    // Kahan state: (x, y) packed, z scalar.
+    float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
+    float sz = 0.f, cz = 0.f;
     unsigned long long n_leaf = 0, n_far = 0, n_open = 0, n_re = 0, n_vis = 0;
-    const uint32_t root = n_total + sd.off;
     bool bad = false;
     // The root's box is the system's box, so every target is inside it and every lane
     // opens it -- unless the whole system is massless, when nothing is added.
-    if (sd.n > 1 && __ldg(&rec[4 * (size_t)root]).w > 0.f) {
-      L.eps2f = __double2float_rn(dmul(sd.eps, sd.eps));
-      L.theta = sd.theta;
+    const uint32_t root = sd.off;  // internal node 0 of the system
+    if (sd.n > 1 && __ldg(&b.agg64[root].m) > 0.0) {
+      const float eps2f = __double2float_rn(dmul(sd.eps, sd.eps));
+      const float2 eps2 = f2(eps2f, eps2f);
+      float xh[3] = {0.f, 0.f, 0.f}, xl[3] = {0.f, 0.f, 0.f};
       if (valid) {
-        const float4 ha = rec[4 * (size_t)L.k], hb = rec[4 * (size_t)L.k + 1];
-        L.xh[0] = ha.x;
-        L.xh[1] = ha.y;
-        L.xh[2] = ha.z;
-        L.xl[0] = hb.x;
-        L.xl[1] = hb.y;
-        L.xl[2] = hb.z;
-      } else {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) L.xh[c] = L.xl[c] = 0.f;
+        const double4 p = b.leaf64[k];
+        split_ff(p.x, xh[0], xl[0]);
+        split_ff(p.y, xh[1], xl[1]);
+        split_ff(p.z, xh[2], xl[2]);
       }
-      // pair stack of kStackCap entries: entry j in lane j % 32 of slot j / 32
-      uint32_t sx0 = 0, sy0 = 0, sm0 = 0, sx1 = 0, sy1 = 0, sm1 = 0, sx2 = 0, sy2 = 0, sm2 = 0;
+      // negated target coordinates, duplicated for both children
+      const float2 nxh = f2(-xh[0], -xh[0]), nyh = f2(-xh[1], -xh[1]), nzh = f2(-xh[2], -xh[2]);
+      const float2 nxl = f2(-xl[0], -xl[0]), nyl = f2(-xl[1], -xl[1]), nzl = f2(-xl[2], -xl[2]);
+      const uint32_t gmax = n_total - 1;
       int sp = 0;
-      const float4 r2 = __ldg(&rec[4 * (size_t)root + 2]);
-      uint32_t cx = __float_as_uint(r2.x), cy = __float_as_uint(r2.y);
+      uint32_t g = root;
       uint32_t mask = __ballot_sync(0xffffffffu, valid);
       const uint32_t max_iters = sd.n + 64u;
       uint32_t iters = 0;
+      float2 tx = f2(0.f, 0.f), ty = f2(0.f, 0.f), tz = f2(0.f, 0.f);  // per-child term sums
       for (;;) {
-        bad |= (cx > umax) | (cy > umax);
         if (++iters > max_iters) {
           bad = true;
           break;
         }
-        cx = min(cx, umax);
-        cy = min(cy, umax);
+        bad |= g > gmax;
+        g = min(g, gmax);
         if (STATS) ++n_vis;
-        const float4* p0 = rec + 4 * (size_t)cx;
-        const float4* p1 = rec + 4 * (size_t)cy;
-        const float4 a0 = __ldg(p0), b0 = __ldg(p0 + 1);
-        const float4 a1 = __ldg(p1), b1 = __ldg(p1 + 1);
-        const float4 k0 = cx >= n_total ? __ldg(p0 + 2) : make_float4(0.f, 0.f, -2.f, 0.f);
-        const float4 k1 = cy >= n_total ? __ldg(p1 + 2) : make_float4(0.f, 0.f, -2.f, 0.f);
+        const float4* pr = pairs + 5 * (size_t)g;
+        const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3), r4 = __ldg(pr + 4);
+        const uint32_t uL = __float_as_uint(r4.z), uR = __float_as_uint(r4.w);
         const bool act = (mask >> lane) & 1u;
-        Child32 c0 = classify<INSIDE>(b, L, act, cx, a0, b0, k0.z, n_total);
-        Child32 c1 = classify<INSIDE>(b, L, act, cy, a1, b1, k1.z, n_total);
-        if (__any_sync(0xffffffffu, c0.amb || c1.amb)) {
-          if (STATS) n_re += (c0.amb ? 1 : 0) + (c1.amb ? 1 : 0);
-          resolve_amb(b, L, c0, cx, n_total);
-          resolve_amb(b, L, c1, cy, n_total);
+        // d = (c_hi - x_hi) + (c_lo - x_lo) for both children at once
+        const float2 dx = __fadd2_rn(__fadd2_rn(f2(r0.x, r0.y), nxh), __fadd2_rn(f2(r2.x, r2.y), nxl));
+        const float2 dy = __fadd2_rn(__fadd2_rn(f2(r0.z, r0.w), nyh), __fadd2_rn(f2(r2.z, r2.w), nyl));
+        const float2 dz = __fadd2_rn(__fadd2_rn(f2(r1.x, r1.y), nzh), __fadd2_rn(f2(r3.x, r3.y), nzl));
+        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        bool tL = act && d2.x > r3.z, tR = act && d2.y > r3.w;
+        bool oL = act && d2.x < r4.x, oR = act && d2.y < r4.y;
+        bool aL = act && !tL && !oL, aR = act && !tR && !oR;
+        if (INSIDE) {
+          if (tL && uL >= n_total) inside_test(b, xh, uL - n_total, tL, oL, aL);
+          if (tR && uR >= n_total) inside_test(b, xh, uR - n_total, tR, oR, aR);
         }
-        float t[3] = {0.f, 0.f, 0.f};
-        add_term<QUAD>(b, L, c0, c0.take, a0.w, cx, n_total, t);
-        add_term<QUAD>(b, L, c1, c1.take, a1.w, cy, n_total, t);
-        acc_add<KAHAN>(acc, t[0], t[1], t[2]);
-        if (STATS) {
-          n_leaf += (c0.take && cx < n_total ? 1 : 0) + (c1.take && cy < n_total ? 1 : 0);
-          n_far += (c0.take && cx >= n_total ? 1 : 0) + (c1.take && cy >= n_total ? 1 : 0);
-          n_open += (c0.open ? 1 : 0) + (c1.open ? 1 : 0);
+        if (__any_sync(0xffffffffu, aL || aR)) {
+          if (STATS) n_re += (aL ? 1 : 0) + (aR ? 1 : 0);
+          if (aL) resolve(b, k, sd.theta, uL, n_total, tL, oL);
+          if (aR) resolve(b, k, sd.theta, uR, n_total, tR, oR);
         }
-        const uint32_t m0 = __ballot_sync(0xffffffffu, c0.open);
-        const uint32_t m1 = __ballot_sync(0xffffffffu, c1.open);
-        const uint32_t n0x = __float_as_uint(k0.x), n0y = __float_as_uint(k0.y);
-        const uint32_t n1x = __float_as_uint(k1.x), n1y = __float_as_uint(k1.y);
-        if (m0 && m1) {
-          // push the right child's pair; continue with the left child's
-          if (sp >= kStackCap) {
-            bad = true;
-            break;
+        // Plummer-softened monopole terms; r^2 > 0 keeps the target's own leaf (d = 0)
+        // an exact zero term.
+        const float2 r2s = __fadd2_rn(d2, eps2);
+        const float invL = rsqrtf(fmaxf(r2s.x, 1e-30f)), invR = rsqrtf(fmaxf(r2s.y, 1e-30f));
+        const float2 inv = f2(invL, invR);
+        const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
+        float2 f = __fmul2_rn(f2(r1.z, r1.w), inv3);
+        f.x = tL ? f.x : 0.f;
+        f.y = tR ? f.y : 0.f;
+        tx = __ffma2_rn(dx, f, tx);
+        ty = __ffma2_rn(dy, f, ty);
+        tz = __ffma2_rn(dz, f, tz);
+        if (QUAD) {
+          float tq[3] = {0.f, 0.f, 0.f};
+          if (tL && uL >= n_total) {
+            const size_t gi = uL - n_total;
+            quad_term(__ldg(&b.nodeQ[2 * gi]), __ldg(&b.nodeQ[2 * gi + 1]), dx.x, dy.x, dz.x, invL, tq);
           }
-          const bool w0 = lane == sp, w1 = lane == sp - 32, w2 = lane == sp - 64;
-          sx0 = w0 ? n1x : sx0;
-          sy0 = w0 ? n1y : sy0;
-          sm0 = w0 ? m1 : sm0;
-          sx1 = w1 ? n1x : sx1;
-          sy1 = w1 ? n1y : sy1;
-          sm1 = w1 ? m1 : sm1;
-          sx2 = w2 ? n1x : sx2;
-          sy2 = w2 ? n1y : sy2;
-          sm2 = w2 ? m1 : sm2;
-          ++sp;
+          if (tR && uR >= n_total) {
+            const size_t gi = uR - n_total;
+            quad_term(__ldg(&b.nodeQ[2 * gi]), __ldg(&b.nodeQ[2 * gi + 1]), dx.y, dy.y, dz.y, invR, tq);
+          }
+          tx.x += tq[0];
+          ty.x += tq[1];
+          tz.x += tq[2];
         }
+        if ((iters & 1u) == 0) {
+          // fold the children's sums and add them with compensation
+          const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
+          const float tzz = tz.x + tz.y;
+          if (KAHAN) {
+            const float2 y = __fadd2_rn(txy, f2(-cxy.x, -cxy.y));
+            const float2 u = __fadd2_rn(sxy, y);
+            cxy = __fadd2_rn(__fadd2_rn(u, f2(-sxy.x, -sxy.y)), f2(-y.x, -y.y));
+            sxy = u;
+            const float yz = tzz - cz;
+            const float uz = sz + yz;
+            cz = (uz - sz) - yz;
+            sz = uz;
+          } else {
+            sxy = __fadd2_rn(sxy, txy);
+            sz += tzz;
+          }
+          tx = ty = tz = f2(0.f, 0.f);
+        }
+        if (STATS) {
+          n_leaf += (tL && uL < n_total && uL != k ? 1 : 0) + (tR && uR < n_total && uR != k ? 1 : 0);
+          n_far += (tL && uL >= n_total ? 1 : 0) + (tR && uR >= n_total ? 1 : 0);
+          n_open += (oL ? 1 : 0) + (oR ? 1 : 0);
+        }
+        const uint32_t m0 = __ballot_sync(0xffffffffu, oL);
+        const uint32_t m1 = __ballot_sync(0xffffffffu, oR);
         if (m0) {
-          cx = n0x;
-          cy = n0y;
+          if (m1) {
+            // push the right child; continue with the left one
+            if (sp >= kStackCap) {
+              bad = true;
+              break;
+            }
+            if (lane == 0) stack[sp] = make_uint2(uR - n_total, m1);
+            ++sp;
+          }
+          g = uL - n_total;
           mask = m0;
         } else if (m1) {
-          cx = n1x;
-          cy = n1y;
+          g = uR - n_total;
           mask = m1;
         } else {
           if (sp == 0) break;
-          --sp;
-          const int src = sp & 31;
-          const int slot = sp >> 5;
-          cx = __shfl_sync(0xffffffffu, slot == 0 ? sx0 : (slot == 1 ? sx1 : sx2), src);
-          cy = __shfl_sync(0xffffffffu, slot == 0 ? sy0 : (slot == 1 ? sy1 : sy2), src);
-          mask = __shfl_sync(0xffffffffu, slot == 0 ? sm0 : (slot == 1 ? sm1 : sm2), src);
+          __syncwarp();
+          const uint2 e = stack[--sp];
+          g = e.x;
+          mask = e.y;
         }
       }
+      // fold what is left
+      const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
+      const float tzz = tz.x + tz.y;
+      if (KAHAN) {
+        const float2 y = __fadd2_rn(txy, f2(-cxy.x, -cxy.y));
+        const float2 u = __fadd2_rn(sxy, y);
+        cxy = __fadd2_rn(__fadd2_rn(u, f2(-sxy.x, -sxy.y)), f2(-y.x, -y.y));
+        sxy = u;
+        const float yz = tzz - cz;
+        const float uz = sz + yz;
+        cz = (uz - sz) - yz;
+        sz = uz;
+      } else {
+        sxy = __fadd2_rn(sxy, txy);
+        sz += tzz;
+      }
+      __syncwarp();  // the next item's pushes must not race this item's last pop
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) raise_err(b.ctl, kErrBadIndex);
     if (valid) {
-      const uint32_t o = b.order[L.k];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float v = KAHAN ? __fsub_rn(acc.s[c], acc.c[c]) : acc.s[c];
-        b.acc[3 * (size_t)o + c] = dmul(static_cast<double>(v), sd.g);
-      }
+      const uint32_t o = b.order[k];
+      const float ax = KAHAN ? __fsub_rn(sxy.x, cxy.x) : sxy.x;
+      const float ay = KAHAN ? __fsub_rn(sxy.y, cxy.y) : sxy.y;
+      const float az = KAHAN ? __fsub_rn(sz, cz) : sz;
+      b.acc[3 * (size_t)o + 0] = dmul(static_cast<double>(ax), sd.g);
+      b.acc[3 * (size_t)o + 1] = dmul(static_cast<double>(ay), sd.g);
+      b.acc[3 * (size_t)o + 2] = dmul(static_cast<double>(az), sd.g);
     }
     if (STATS) {
       n_leaf = warp_sum64(n_leaf);
