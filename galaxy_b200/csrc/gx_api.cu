@@ -259,7 +259,7 @@ WalkCfg walk_cfg(const gx_handle* h) {
   c.kahan = (h->opt.flags & GX_FLAG_NO_KAHAN) ? 0 : 1;
   c.stats = (h->opt.flags & GX_FLAG_STATS) ? 1 : 0;
   c.inside_test = h->theta >= 0.57 ? 1 : 0;
-  c.block = h->opt.walk_block ? static_cast<int>(h->opt.walk_block) : 256;
+  c.block = h->opt.walk_block ? static_cast<int>(h->opt.walk_block) : kWalkThreads;
   c.persistent_ctas = h->opt.walk_ctas_per_sm ? static_cast<int>(h->opt.walk_ctas_per_sm) * h->sm_count : 0;
   return c;
 }
@@ -377,7 +377,7 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
     o = *opt;
   }
   if (o.precision > GX_PREC_F64 || o.multipole > GX_MULTIPOLE_QUAD ||
-      (o.walk_block && (o.walk_block % 32 || o.walk_block > 256))) {
+      (o.walk_block && (o.walk_block % 32 || o.walk_block > static_cast<uint32_t>(kWalkThreads)))) {
     set_global_err("invalid gx_options");
     return GX_ERR_INVALID_ARG;
   }

@@ -70,9 +70,9 @@ WalkCfg bcfg(const gx_batch* bt, bool inside) {
   c.kahan = (bt->opt.flags & GX_FLAG_NO_KAHAN) ? 0 : 1;
   c.stats = (bt->opt.flags & GX_FLAG_STATS) ? 1 : 0;
   c.inside_test = inside ? 1 : 0;
-  c.block = bt->opt.walk_block ? static_cast<int>(bt->opt.walk_block) : 256;
+  c.block = bt->opt.walk_block ? static_cast<int>(bt->opt.walk_block) : kWalkThreads;
   c.persistent_ctas = bt->sm_count * (bt->opt.walk_ctas_per_sm ? static_cast<int>(bt->opt.walk_ctas_per_sm)
-                                                               : 2048 / c.block / 2);
+                                                               : walk_resident_ctas(c));
   return c;
 }
 
@@ -203,7 +203,7 @@ int gx_batch_create(size_t budget_bytes, const gx_options* opt, gx_batch** out) 
     o = *opt;
   }
   if (o.precision > GX_PREC_F64 || o.multipole > GX_MULTIPOLE_QUAD ||
-      (o.walk_block && (o.walk_block % 32 || o.walk_block > 256))) {
+      (o.walk_block && (o.walk_block % 32 || o.walk_block > static_cast<uint32_t>(kWalkThreads)))) {
     set_global_err("invalid gx_options");
     return GX_ERR_INVALID_ARG;
   }

@@ -113,12 +113,15 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
                                                         const uint32_t* __restrict__ order,
                                                         const double* __restrict__ pos,
                                                         const double* __restrict__ mass, StepBufs b, int f64rec) {
-  const TileDesc t = tiles[blockIdx.x];
+  // One leaf per thread: block j covers leaves [256 (j % 16), 256 (j % 16) + 256) of
+  // tile j / 16, so every leaf climbs concurrently (the loop below runs at most once).
+  const TileDesc t = tiles[blockIdx.x / kItemsPerThread];
   const SysDesc sd = sys[t.sys];
   const uint32_t off = sd.off, ns = sd.n;
   const double theta = sd.theta;
   const double tiny2 = b.bounds[t.sys].tiny2;
-  for (uint32_t k = t.begin + threadIdx.x; k < t.end; k += kTileThreads) {
+  const uint32_t first = t.begin + (blockIdx.x % kItemsPerThread) * kTileThreads;
+  for (uint32_t k = first + threadIdx.x; k < t.end && k < first + kTileThreads; k += kTileThreads) {
     // ---- leaf: gather the particle into sorted order ----
     const uint32_t o = order[k];
     if (o >= n_total) {
@@ -294,17 +297,17 @@ void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st)
   const uint64_t* c64 = reinterpret_cast<const uint64_t*>(b.codes);
   if (b.key64) {
     if (quad)
-      k_build<true, uint64_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, c64, b.order, b.pos, b.mass, b,
+      k_build<true, uint64_t><<<b.ntiles * kItemsPerThread, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, c64, b.order, b.pos, b.mass, b,
                                                                   f64_records);
     else
-      k_build<false, uint64_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, c64, b.order, b.pos, b.mass,
+      k_build<false, uint64_t><<<b.ntiles * kItemsPerThread, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, c64, b.order, b.pos, b.mass,
                                                                    b, f64_records);
   } else {
     if (quad)
-      k_build<true, uint32_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos, b.mass,
+      k_build<true, uint32_t><<<b.ntiles * kItemsPerThread, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos, b.mass,
                                                                   b, f64_records);
     else
-      k_build<false, uint32_t><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos,
+      k_build<false, uint32_t><<<b.ntiles * kItemsPerThread, kTileThreads, 0, st>>>(b.tiles, b.sys, b.n, b.codes, b.order, b.pos,
                                                                    b.mass, b, f64_records);
   }
 }

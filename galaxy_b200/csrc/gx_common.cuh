@@ -74,6 +74,8 @@ struct Bounds {
 // bbox, Morton, sort and build kernels each run one CTA per tile.
 constexpr int kTile = 4096;
 constexpr int kTileThreads = 256;
+// Threads per block of the tree walks (and the largest walk block accepted).
+constexpr int kWalkThreads = 128;
 constexpr int kItemsPerThread = kTile / kTileThreads;  // 16
 constexpr int kRadixBits = 8;
 constexpr int kRadixBins = 1 << kRadixBits;

@@ -61,7 +61,7 @@ struct WalkCfg {
   int kahan = 1;
   int stats = 0;
   int inside_test = 0;  // some system has theta >= 1/sqrt(3)
-  int block = 256;
+  int block = kWalkThreads;
   int persistent_ctas = 0;  // 0 = one warp per item (no stealing)
 };
 
@@ -82,6 +82,8 @@ void launch_code_hist(const StepBufs& b, cudaStream_t st);
 void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st);
 // gx_walk.cu: tree walk, acc in original order
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st);
+// Blocks of cfg.block threads of the selected walk kernel resident on one SM.
+int walk_resident_ctas(const WalkCfg& cfg);
 // gx_diag.cu
 void launch_direct_sum_f64(uint32_t n, const double* pos, const double* mass, double g, double eps,
                            uint32_t n_targets, const uint32_t* targets, double* acc, cudaStream_t st);

@@ -117,7 +117,7 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 // order, so each lane adds its terms in the reference's order with the reference's
 // arithmetic.
 template <bool STATS>
-__global__ void __launch_bounds__(256) k_walk_f64(StepBufs b, int persistent) {
+__global__ void __launch_bounds__(kWalkThreads) k_walk_f64(StepBufs b, int persistent) {
   const int lane = threadIdx.x & 31;
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
   uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -294,14 +294,14 @@ __device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double th
 }  // namespace
 
 #ifndef GX_WALK_MINB
-#define GX_WALK_MINB 3  // resident 256-thread blocks per SM the register budget is sized for
+#define GX_WALK_MINB 7  // resident kWalkThreads-thread blocks per SM (72 registers a thread)
 #endif
 
 // FP32 walk over sibling-pair records. Each iteration decides both children of one
 // opened internal node for every lane that opened it: the pair's record is five
 // float4 loads, laid out so that every component pair is a float2 (left, right), and
 // the distance, threshold and force arithmetic of the two children runs as sm_100
-// packed FP32 instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn). Terms of two
+// packed FP32 instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn). Terms of four
 // iterations are summed and added to the lane's Kahan-compensated accumulator. The
 // record carries the children's indices, so the next pair is known from the record
 // just loaded (one dependent load per iteration); the warp's stack of pending pairs
@@ -310,8 +310,8 @@ __device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double th
 // raises the device error word. Each lane takes exactly the reference's set of
 // terms; only the order of summation differs from the FP64 walk.
 template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
-__global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int persistent) {
-  __shared__ uint2 s_stack[256 / 32][kStackCap];  // (internal node, lane mask)
+__global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBufs b, int persistent) {
+  __shared__ uint2 s_stack[kWalkThreads / 32][kStackCap];  // (internal node, lane mask)
   const int lane = threadIdx.x & 31;
   uint2* stack = s_stack[threadIdx.x >> 5];
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(256, GX_WALK_MINB) k_walk_f32(StepBufs b, int 
           ty.x += tq[1];
           tz.x += tq[2];
         }
-        if ((iters & 1u) == 0) {
+        if ((iters & 3u) == 0) {
           // fold the children's sums and add them with compensation
           const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
           const float tzz = tz.x + tz.y;
@@ -538,6 +538,24 @@ void dispatch_f32(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
 }
 
 }  // namespace
+
+namespace {
+
+template <class K>
+int resident(K kern, int block) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, block, 0) != cudaSuccess) n = 1;
+  return n > 0 ? n : 1;
+}
+
+}  // namespace
+
+int walk_resident_ctas(const WalkCfg& cfg) {
+  const int block = cfg.block > 0 ? cfg.block : kWalkThreads;
+  if (cfg.precision == 1) return resident(k_walk_f64<false>, block);
+  if (cfg.quad) return resident(k_walk_f32<true, true, false, false>, block);
+  return resident(k_walk_f32<false, true, false, false>, block);
+}
 
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
   if (cfg.precision == 1) {

@@ -58,7 +58,8 @@ typedef struct gx_options {
   uint32_t multipole;      /* GX_MULTIPOLE_* */
   uint32_t flags;          /* GX_FLAG_* */
   int32_t device;          /* CUDA ordinal, -1 = current device */
-  uint32_t walk_block;     /* threads per block of the tree walk, 0 = tuned default */
+  uint32_t walk_block;     /* threads per block of the tree walk: 0 = default (128), else a
+                              multiple of 32 up to 128 */
   uint32_t walk_ctas_per_sm; /* >0: persistent work-stealing walk with this many CTAs per SM;
                                 0: tuned default (one warp per 32 targets for a single system) */
 } gx_options;
