@@ -82,6 +82,10 @@ constexpr int kRadixBins = 1 << kRadixBits;
 constexpr int kRadixPasses = 4;     // 30-bit codes: 8 + 8 + 8 + 6 bits
 constexpr int kRadixPasses63 = 8;   // 63-bit codes: 7 x 8 + 7 bits
 constexpr int kMaxRadixPasses = 8;  // histogram / look-back arrays are sized for this
+// Slot of the per-step counters that the persistent walk steals items from; slots
+// [0, kMaxRadixPasses) are the sort passes' tile counters.
+constexpr int kWalkItemCounter = kMaxRadixPasses;
+static_assert(kWalkItemCounter < 16, "the per-step counter block holds 16 words");
 // Tree depth bound: the augmented key is (code, 32-bit position), so a root-to-leaf path
 // has at most 30 + 32 (30-bit codes) or 63 + 32 (63-bit codes) internal levels.
 constexpr int kMaxDepth = 100;

@@ -24,7 +24,7 @@ struct StepBufs {
   unsigned long long* bbox_enc = nullptr;  // 6 per system
   uint32_t* hist = nullptr;                // nsys * kMaxRadixPasses * 256
   uint32_t* sort_status = nullptr;         // kMaxRadixPasses * ntiles * 256
-  uint32_t* counters = nullptr;            // [0..3] sort tile counters, [4] walk item counter
+  uint32_t* counters = nullptr;            // 16 words: [0..7] sort tile counters, [8] walk item counter
   void* zero_begin = nullptr;
   size_t zero_bytes = 0;
   Bounds* bounds = nullptr;  // per system

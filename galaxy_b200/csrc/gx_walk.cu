@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_f64(StepBufs b, int persi
     }
     if (persistent) {
       uint32_t nxt = 0;
-      if (lane == 0) nxt = atomicAdd(&b.counters[4], 1u) + warps_total;
+      if (lane == 0) nxt = atomicAdd(&b.counters[kWalkItemCounter], 1u) + warps_total;
       item = __shfl_sync(0xffffffffu, nxt, 0);
     } else {
       item = b.nitems;
@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
     }
     if (persistent) {
       uint32_t nxt = 0;
-      if (lane == 0) nxt = atomicAdd(&b.counters[4], 1u) + warps_total;
+      if (lane == 0) nxt = atomicAdd(&b.counters[kWalkItemCounter], 1u) + warps_total;
       item = __shfl_sync(0xffffffffu, nxt, 0);
     } else {
       item = b.nitems;

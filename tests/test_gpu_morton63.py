@@ -59,3 +59,19 @@ def test_batch_equals_alone_k63():
         r.upload(st)
         r.step_many(1e-3, 4)
         assert np.array_equal(b.snapshot(sid).pos, r.snapshot().pos)
+
+
+@pytest.mark.parametrize("k63", [True, False])
+def test_batch_work_stealing(k63):
+    """More walk items than persistent warps, so warps steal items after the sort
+    passes (eight with 63-bit keys) have used their own tile counters."""
+    sts = [gb.ic.plummer(40_000 + 3_000 * i, 70 + i) for i in range(3)]
+    b = gb.Batch(morton63=k63, walk_ctas_per_sm=1)
+    ids = [b.add(s, 1.0, 0.01, 0.5, 1e-3) for s in sts]
+    b.step(2)
+    for sid, st in zip(ids, sts):
+        r = gb.GpuResidentLeapfrog(1.0, 0.01, 0.5, morton63=k63)
+        r.upload(st)
+        r.step_many(1e-3, 2)
+        assert np.array_equal(b.snapshot(sid).pos, r.snapshot().pos)
+        assert np.array_equal(b.snapshot(sid).vel, r.snapshot().vel)
