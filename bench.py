@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from galaxy_b200 import ranks  # noqa: E402  (rank discovery and reductions; no GPU work)
+
 METRIC = "particle-steps/s at theta=0.5 (resident KDK step, plain single-system path)"
 N_PER_GALAXY = 524_288
 
@@ -94,44 +96,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws <= 1:
-        return None, 0, 1, 0
-    import torch
-    import torch.distributed as dist
-
-    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
-    backend = "nccl" if torch.cuda.is_available() else "gloo"
-    if backend == "nccl":
-        torch.cuda.set_device(local)
-    from datetime import timedelta
-
-    dist.init_process_group(backend, timeout=timedelta(seconds=300))
-    return dist, rank, ws, local
-
-
-def _max_over_ranks(dist, v: float, local: int) -> float:
-    if dist is None:
-        return v
-    import torch
-
-    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
-    t = torch.tensor([v], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def _barrier(dist, local):
-    if dist is not None:
-        import torch
-
-        if torch.cuda.is_available():
-            dist.barrier(device_ids=[local])
-        else:
-            dist.barrier()
-
-
 def workload(config: str, seed: int):
     import galaxy_b200 as gb
 
@@ -187,8 +151,11 @@ def cpu_sample_step(st, params, threads: int, n_targets: int, rng) -> float:
 
 
 def run_reference(args):
-    dist, rank, ws, local = _dist()
+    dist, rank, ws, local = ranks.init()
     if rank != 0:
+        # rank 0 alone times the CPU reference; the other ranks have no work
+        if dist is not None:
+            dist.destroy_process_group()
         return
     from oracle import oracle
 
@@ -213,10 +180,12 @@ def run_reference(args):
                              "sample": sample},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_ours(args):
-    dist, rank, ws, local = _dist()
+    dist, rank, ws, local = ranks.init()
     import galaxy_b200 as gb
 
     st, p = workload(args.config, rank)
@@ -228,13 +197,14 @@ def run_ours(args):
     r = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], device=local)
     r.upload(st)
     r.step_many(dt, args.warmup)
+    tune = r.autotune(repeats=3)  # walk launch for this N bucket (outside the timed region)
     clocks = ClockSampler(local)
     clocks.start()
-    _barrier(dist, local)
+    ranks.barrier(dist, local)
     ms = r.step_many_timed(dt, args.steps)
-    _barrier(dist, local)
+    ranks.barrier(dist, local)
     clk = clocks.stop()
-    ms_max = _max_over_ranks(dist, ms, local)
+    ms_max = ranks.max_over_ranks(dist, ms, local)
     value = n * ws * args.steps / (ms_max / 1e3)
 
     # --- e2e: the reference-facing ForceSolver path (LeapfrogKdk on host arrays) ---
@@ -242,13 +212,13 @@ def run_ours(args):
     h = gb.GpuLbvh(1.0, p["eps"], p["theta"], device=local)
     primed = h.kdk_step_host(pinned, dt, primed=False)  # prime + one step (warm-up)
     k_e2e = max(1, min(args.steps, 10))
-    _barrier(dist, local)
+    ranks.barrier(dist, local)
     t0 = time.perf_counter()
     for _ in range(k_e2e):
         primed = h.kdk_step_host(pinned, dt, primed=primed)
     t_e2e = time.perf_counter() - t0
-    _barrier(dist, local)
-    t_e2e = _max_over_ranks(dist, t_e2e, local)
+    ranks.barrier(dist, local)
+    t_e2e = ranks.max_over_ranks(dist, t_e2e, local)
     e2e = {"value": n * ws * k_e2e / t_e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
            "d2h_bytes_per_step": 24 * n, "steps": k_e2e,
            "path": "LeapfrogKdk on pinned host f64 arrays, gx_accelerations per step (upload pos+mass, download acc)"}
@@ -316,7 +286,8 @@ def run_ours(args):
                 "config": {"workload": p["name"], "particles_per_gpu": n, "theta": p["theta"], "eps": p["eps"],
                            "dt": p["dt"], "precision": "FP32 walk (Kahan), FP64 pos/vel and opening re-checks",
                            "parallelism": "replicas" if ws > 1 else "single system",
-                           "l2": "working set ~330 B/particle > L2 (no flush needed)", "cuda_graph": True},
+                           "l2": "working set ~350 B/particle > L2 (no flush needed)", "cuda_graph": True,
+                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}},
                 "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "walk_counts": counts}
         print(json.dumps(line), flush=True)
@@ -331,25 +302,31 @@ def run_batched(args):
     import galaxy_b200 as gb
     from galaxy_b200 import workloads
 
-    dist, rank, ws, local = _dist()
-    mix = workloads.batched_mix(args.systems, seed=rank)
+    dist, rank, ws, local = ranks.init()
+    # A global mix of systems x ranks systems, partitioned by particle count (no
+    # collective touches the data path); each rank builds only its own systems.
+    sizes = workloads.batched_sizes(args.systems * ws, seed=0)
+    mine = ranks.shard(sizes, ws)[rank]
+    mix = workloads.batched_mix(args.systems * ws, seed=0, indices=mine)
     n_tot = sum(len(m.state) for m in mix)
     k63 = args.morton63
     b = gb.Batch(device=local, morton63=k63)
     for m in mix:
         b.add(m.state, m.g, m.eps, m.theta, m.dt)
     b.step(args.warmup)
+    tune = b.autotune(repeats=2)  # persistent walk launch for this batch (untimed)
     clocks = ClockSampler(local)
     clocks.start()
-    _barrier(dist, local)
+    ranks.barrier(dist, local)
     ms = []
     for _ in range(args.steps):
         b.step(1)
         ms.append(b.stats()["ms_last_step"])
-    _barrier(dist, local)
+    ranks.barrier(dist, local)
     clk = clocks.stop()
-    t = _max_over_ranks(dist, sum(ms) / 1e3, local)
-    value = n_tot * ws * args.steps / t
+    t = ranks.max_over_ranks(dist, sum(ms) / 1e3, local)
+    n_all = ranks.sum_over_ranks(dist, n_tot, local)  # particles on all ranks
+    value = n_all * args.steps / t
     del b
     # plain path: the same systems, each stepped alone by the single-system handle
     hs = []
@@ -357,29 +334,33 @@ def run_batched(args):
         r = gb.GpuResidentLeapfrog(m.g, m.eps, m.theta, device=local, morton63=k63)
         r.upload(m.state)
         r.step_many(m.dt, 1)
+        if gb.tuning_lookup(len(m.state), morton63=k63, device=local) is None:
+            r.autotune(repeats=2)  # the plain path is tuned per N bucket too
         hs.append((r, m))
     k_plain = max(1, min(args.steps, 3))
     t_plain = 0.0
     for _ in range(k_plain):
         for r, m in hs:
             t_plain += r.step_many_timed(m.dt, 1) / 1e3
-    t_plain = _max_over_ranks(dist, t_plain, local)
-    plain = n_tot * ws * k_plain / t_plain
+    t_plain = ranks.max_over_ranks(dist, t_plain, local)
+    plain = n_all * k_plain / t_plain
     del hs
     if rank == 0:
         line = {"metric": "particle-steps/s at theta=0.5, batched uneven systems", "value": value,
                 "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"batched-{args.systems}-systems", "particles_per_gpu": n_tot,
+                "config": {"workload": f"batched-{args.systems}-systems", "particles_per_gpu": n_all / ws,
                            "morton_bits": 63 if k63 else 30,
                            "systems": args.systems, "n_range": [4096, 262144], "theta": 0.5, "eps": 0.01,
-                           "dt": [1e-3, 5e-4], "cuda_graph": True, "parallelism": "replicas" if ws > 1 else "1 GPU"},
+                           "dt": [1e-3, 5e-4], "cuda_graph": True,
+                           "parallelism": f"{args.systems * ws} systems sharded by particle count over {ws} ranks" if ws > 1 else "1 GPU"},
                 "step_ms_p50": float(np.percentile(ms, 50)), "step_ms_p99": float(np.percentile(ms, 99)),
                 "plain_path": {"value": plain, "unit": "particle-steps/s", "steps": k_plain,
                                "how": "same systems, one single-system handle each, stepped one after another "
                                       "(device time of each step summed)"},
-                "batched_over_plain": value / plain, "gpu_launches": 8 * args.steps, "clocks": clk}
+                "batched_over_plain": value / plain, "gpu_launches": (12 if k63 else 8) * args.steps, "clocks": clk,
+                "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -392,7 +373,7 @@ def run_serving(args):
     import galaxy_b200 as gb
     from galaxy_b200 import workloads
 
-    dist, rank, ws, local = _dist()
+    dist, rank, ws, local = ranks.init()
     reqs = workloads.request_stream(args.requests, rate=50.0, seed=rank)
     specs = [r.spec() for r in reqs]  # generated before the clock starts
     srv = gb.Server(budget_bytes=150 << 30, device=local, morton63=args.morton63)
@@ -435,18 +416,93 @@ def run_serving(args):
         dist.destroy_process_group()
 
 
+def run_precision(args):
+    """Precision study: the collision setup at N = 4,194,304 (mass ratio 1:3), for
+    theta in {0.3, 0.5, 0.7}. Force error of the FP32 walk and of the FP64 walk (the
+    reference's own arithmetic, bit-identical to its CPU Lbvh) against an FP64 direct
+    sum on a seeded 65,536-particle subsample; per-particle error of FP32 against the
+    FP64 walk; energy and angular-momentum drift of the FP32 run over --steps steps,
+    and of both runs over the first --fp64-steps steps. Energies use the FP64 O(N^2)
+    potential, evaluated only at the start and at the ends of the runs."""
+    import galaxy_b200 as gb
+
+    dist, rank, ws, local = ranks.init()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    n = 4_194_304
+    eps, dt = 0.02, 5e-4
+    st = gb.ic.collision(n, 0, mass_ratio=3.0, pericentre=4.0, incl1_deg=30.0, incl2_deg=60.0)
+    sub = np.sort(np.random.default_rng(65_536).choice(n, 65_536, replace=False)).astype(np.uint32)
+    ds = gb.GpuLbvh(1.0, eps, 0.5, device=local).direct_sum_f64(st.pos, st.mass, sub)
+    dsn = np.linalg.norm(ds, axis=1)
+
+    def err_vs(a, ref, refn):
+        e = np.linalg.norm(a - ref, axis=1) / refn
+        return {"rms": float(np.sqrt(np.mean(e * e))), "median": float(np.median(e)),
+                "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+
+    def rel(d, d0):
+        return {"dE_rel": float((d["total"] - d0["total"]) / abs(d0["total"])),
+                "dL_rel": float(np.linalg.norm(d["angular_momentum"] - d0["angular_momentum"])
+                                / np.linalg.norm(d0["angular_momentum"]))}
+
+    d0 = None  # the initial state's diagnostics (the same for every theta)
+    results = []
+    for theta in (0.3, 0.5, 0.7):
+        a32 = gb.GpuLbvh(1.0, eps, theta, device=local).accelerations(st)[sub]
+        a64 = gb.GpuLbvh(1.0, eps, theta, precision="f64", device=local).accelerations(st)[sub]
+        k = args.steps
+        k64 = min(args.fp64_steps, k)
+        r = gb.GpuResidentLeapfrog(1.0, eps, theta, device=local)
+        r.upload(st)
+        if d0 is None:
+            d0 = r.diagnostics(True)
+        ms32 = r.step_many_timed(dt, k64)
+        d32_short = r.diagnostics(True)
+        if k > k64:
+            ms32 += r.step_many_timed(dt, k - k64)
+        d32 = r.diagnostics(True)
+        del r
+        r = gb.GpuResidentLeapfrog(1.0, eps, theta, precision="f64", device=local)
+        r.upload(st)
+        ms64 = r.step_many_timed(dt, k64)
+        d64 = r.diagnostics(True)
+        del r
+        results.append({"theta": theta,
+                        "force_err_vs_direct_sum": {"f32_walk": err_vs(a32, ds, dsn),
+                                                    "f64_walk_reference": err_vs(a64, ds, dsn)},
+                        "f32_vs_f64_walk": err_vs(a32, a64, np.linalg.norm(a64, axis=1)),
+                        "drift_f32": {"steps": k, **rel(d32, d0)}, "ms_per_step_f32": ms32 / k,
+                        "drift_at_fp64_horizon": {"steps": k64, "f32": rel(d32_short, d0),
+                                                  "f64_reference": rel(d64, d0)},
+                        "ms_per_step_f64": ms64 / k64})
+    line = {"metric": "force error vs FP64 direct sum and energy drift (precision study)", "value": None,
+            "unit": None, "n_gpus": 1, "steps": args.steps, "warmup": 0, "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "collision-4194304-q3", "particles": n, "mass_ratio": 3.0, "eps": eps, "dt": dt,
+                       "subsample": 65_536, "subsample_seed": 65_536, "thetas": [0.3, 0.5, 0.7],
+                       "fp64_steps": args.fp64_steps},
+            "results": results}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="collision", choices=["collision", "plummer", "batched", "serving"])
+    ap.add_argument("--config", default="collision", choices=["collision", "plummer", "batched", "serving", "precision"])
     ap.add_argument("--systems", type=int, default=256, help="batched: number of systems")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
     ap.add_argument("--horizon", type=float, default=60.0, help="serving: seconds to serve")
     ap.add_argument("--morton63", action="store_true", help="batched/serving: 63-bit Morton keys")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=100, help="precision: horizon of the FP64 run")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -454,6 +510,8 @@ def main():
         run_batched(args)
     elif args.config == "serving":
         run_serving(args)
+    elif args.config == "precision":
+        run_precision(args)
     else:
         run_ours(args)
 

@@ -34,7 +34,7 @@ __all__ = [
     "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "Server", "GxError",
     "PinnedState",
     "stage_morton",
-    "stage_sort", "stage_build", "device_info", "ic",
+    "stage_sort", "stage_build", "device_info", "ic", "tuning_lookup",
 ]
 
 
@@ -236,6 +236,11 @@ class GpuResidentLeapfrog(_Handle):
     def step_many_async(self, dt: float, steps: int):
         self._ck(lib().gx_step_many_async(self._h, float(dt), int(steps)))
 
+    def autotune(self, repeats: int = 3) -> dict:
+        """Pick the walk launch for this N bucket by timing force evaluations on the
+        resident state (which stays bit-identical); see gx_autotune."""
+        return _tune(lambda b, t, n: lib().gx_autotune(self._h, int(repeats), b, t, n), self._ck)
+
     def synchronize(self):
         self._ck(lib().gx_synchronize(self._h))
 
@@ -363,6 +368,10 @@ class Batch:
     def set_graph(self, enable: bool):
         self._ck(lib().gx_batch_set_graph(self._b, int(enable)))
 
+    def autotune(self, repeats: int = 3) -> dict:
+        """gx_batch_autotune: the persistent walk launch for this batch's N bucket."""
+        return _tune(lambda b, t, n: lib().gx_batch_autotune(self._b, int(repeats), b, t, n), self._ck)
+
     def snapshot(self, sid: int) -> State:
         n = C.c_size_t()
         self._ck(lib().gx_system_len(self._b, sid, C.byref(n)))
@@ -486,6 +495,27 @@ def stage_build(sorted_codes, sorted_pos, sorted_mass, handle=None, quad=False):
     if quad:
         out["quad"] = q
     return out
+
+
+def _tune(call, ck) -> dict:
+    best = _lib.Tuning()
+    tried = (_lib.Tuning * _lib.GX_TUNE_MAX_CANDIDATES)()
+    n = C.c_uint32()
+    ck(call(C.byref(best), tried, C.byref(n)))
+    row = lambda t: {"walk_block": t.walk_block, "walk_ctas_per_sm": t.walk_ctas_per_sm, "ms": t.ms}  # noqa: E731
+    return {**row(best), "tried": [row(tried[i]) for i in range(n.value)]}
+
+
+def tuning_lookup(n: int, batched: bool = False, precision: str = "f32", multipole: str = "mono",
+                  morton63: bool = False, device: int = -1):
+    """The tuned walk launch recorded for n particles under these options, or None."""
+    o = _options(precision, multipole, True, False, device, 0, False, 0, morton63)
+    t = _lib.Tuning()
+    rc = lib().gx_tuning_lookup(int(device), int(n), C.byref(o), int(batched), C.byref(t))
+    if rc == _lib.ERRORS_BY_NAME["GX_ERR_STATE"]:
+        return None
+    check(rc, None)
+    return {"walk_block": t.walk_block, "walk_ctas_per_sm": t.walk_ctas_per_sm, "ms": t.ms}
 
 
 def device_info(device: int = 0) -> dict:

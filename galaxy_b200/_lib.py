@@ -25,6 +25,8 @@ ERRORS = {
     -8: "GX_ERR_CAPACITY",
 }
 
+ERRORS_BY_NAME = {v: k for k, v in ERRORS.items()}
+
 GX_PREC_F32, GX_PREC_F64 = 0, 1
 GX_MULTIPOLE_MONO, GX_MULTIPOLE_QUAD = 0, 1
 GX_FLAG_NO_KAHAN, GX_FLAG_STATS, GX_FLAG_STAGE_TIMES, GX_FLAG_MORTON63 = 1, 2, 4, 8
@@ -62,6 +64,17 @@ class Stats(C.Structure):
         ("ms_walk", C.c_float),
         ("ms_total", C.c_float),
     ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("walk_block", C.c_uint32),
+        ("walk_ctas_per_sm", C.c_uint32),
+        ("ms", C.c_float),
+    ]
+
+
+GX_TUNE_MAX_CANDIDATES = 8
 
 
 class BatchStats(C.Structure):
@@ -121,6 +134,8 @@ SIGNATURES = {
     "gx_diagnostics": (_i, [_vp, _i, _vp]),
     "gx_get_stats": (_i, [_vp, C.POINTER(Stats)]),
     "gx_step_many_timed": (_i, [_vp, _d, _u64, C.POINTER(C.c_float)]),
+    "gx_autotune": (_i, [_vp, C.c_uint32, C.POINTER(Tuning), C.POINTER(Tuning), C.POINTER(C.c_uint32)]),
+    "gx_tuning_lookup": (_i, [_i, _sz, C.POINTER(Options), _i, C.POINTER(Tuning)]),
     "gx_kdk_step_host": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, C.POINTER(_i), _d]),
     "gx_host_alloc": (_i, [_sz, C.POINTER(_vp)]),
     "gx_host_free": (None, [_vp]),
@@ -139,6 +154,7 @@ SIGNATURES = {
     "gx_system_len": (_i, [_vp, _u64, C.POINTER(_sz)]),
     "gx_batch_stats_get": (_i, [_vp, C.POINTER(BatchStats)]),
     "gx_batch_set_graph": (_i, [_vp, _i]),
+    "gx_batch_autotune": (_i, [_vp, C.c_uint32, C.POINTER(Tuning), C.POINTER(Tuning), C.POINTER(C.c_uint32)]),
     "gx_server_create": (_i, [_sz, C.POINTER(Options), C.POINTER(_vp)]),
     "gx_server_destroy": (None, [_vp]),
     "gx_server_last_error": (C.c_char_p, [_vp]),

@@ -44,7 +44,8 @@ def _compile(src: str, verbose_ptxas: bool) -> str:
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), _deps_mtime()):
         return obj
     cmd = [_nvcc(), "-ccbin", _host_cxx(), "-std=c++17", "-O3", "-lineinfo", "-ftz=true", *ARCH, "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+           "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp", "-I", os.path.join(ROOT, "include"), "-c", src,
+           "-o", obj]
     if src.endswith(".cu"):
         cmd[1:1] = ["-x", "cu"]
         if verbose_ptxas:
@@ -64,7 +65,7 @@ def build(verbose_ptxas: bool = False) -> str:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs,
-               "-Xlinker", "--no-undefined"]
+               "-Xcompiler", "-fopenmp", "-Xlinker", "--no-undefined"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

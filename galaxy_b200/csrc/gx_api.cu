@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -210,6 +212,55 @@ void make_tables(const std::vector<SysDesc>& in, std::vector<SysDesc>& sys, std:
   }
 }
 
+namespace {
+
+struct TuneKey {
+  int device, precision, multipole, key64, batched, bucket;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, precision, multipole, key64, batched, bucket) <
+           std::tie(o.device, o.precision, o.multipole, o.key64, o.batched, o.bucket);
+  }
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, gx_tuning> g_tune;
+
+TuneKey tune_key(int device, const gx_options& opt, int batched, size_t n) {
+  int bucket = 0;
+  while (bucket < 63 && (size_t{2} << bucket) <= n) ++bucket;  // floor(log2 n)
+  return TuneKey{device, static_cast<int>(opt.precision), static_cast<int>(opt.multipole),
+                 (opt.flags & GX_FLAG_MORTON63) ? 1 : 0, batched ? 1 : 0, bucket};
+}
+
+}  // namespace
+
+bool tuned_lookup(int device, const gx_options& opt, int batched, size_t n, gx_tuning* out) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(device, opt, batched, n));
+  if (it == g_tune.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+void tuned_store(int device, const gx_options& opt, int batched, size_t n, const gx_tuning& t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[tune_key(device, opt, batched, n)] = t;
+}
+
+std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid) {
+  std::vector<gx_tuning> out;
+  for (int block : {64, kWalkThreads}) {
+    WalkCfg c = base;
+    c.block = block;
+    const int full = walk_resident_ctas(c);
+    if (with_grid) out.push_back(gx_tuning{static_cast<uint32_t>(block), 0u, 0.f});
+    if (full / 2 >= 1) out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full / 2), 0.f});
+    out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full), 0.f});
+  }
+  if (out.size() > GX_TUNE_MAX_CANDIDATES) out.resize(GX_TUNE_MAX_CANDIDATES);
+  return out;
+}
+
 }  // namespace gx
 
 // ===================================================================================
@@ -261,6 +312,11 @@ WalkCfg walk_cfg(const gx_handle* h) {
   c.inside_test = h->theta >= 0.57 ? 1 : 0;
   c.block = h->opt.walk_block ? static_cast<int>(h->opt.walk_block) : kWalkThreads;
   c.persistent_ctas = h->opt.walk_ctas_per_sm ? static_cast<int>(h->opt.walk_ctas_per_sm) * h->sm_count : 0;
+  gx_tuning t;
+  if (!h->opt.walk_block && !h->opt.walk_ctas_per_sm && tuned_lookup(h->device, h->opt, 0, h->n_layout, &t)) {
+    c.block = static_cast<int>(t.walk_block);
+    c.persistent_ctas = static_cast<int>(t.walk_ctas_per_sm) * h->sm_count;
+  }
   return c;
 }
 
@@ -659,11 +715,44 @@ int gx_kdk_step_host(gx_handle* h, size_t n, double* pos, double* vel, const dou
     *primed = 1;
   }
   const double half = 0.5 * dt;
-  for (size_t i = 0; i < 3 * n; ++i) vel[i] = vel[i] + acc[i] * half;
-  for (size_t i = 0; i < 3 * n; ++i) pos[i] = pos[i] + vel[i] * dt;
-  rc = gx_accelerations(h, n, pos, mass, acc);
-  if (rc) return rc;
-  for (size_t i = 0; i < 3 * n; ++i) vel[i] = vel[i] + acc[i] * half;
+  // Opening half kick and drift (integrator.rs:59-67: v += a h, then x += v dt, each
+  // rounded separately), on all host threads and in chunks, each chunk's positions
+  // copied to the device while the next chunk is computed. Then the force as in
+  // gx_accelerations, and the closing half kick.
+  if (n > 1) {
+    cudaSetDevice(h->device);
+    h->resident = false;
+    rc = layout(h, n, 0.0);
+    if (rc) return rc;
+    StepBufs& b = h->ar.b;
+    const size_t chunk = std::max<size_t>(size_t{1} << 16, (n + 7) / 8);
+    for (size_t c0 = 0; c0 < n; c0 += chunk) {
+      const long long i0 = static_cast<long long>(3 * c0);
+      const long long i1 = static_cast<long long>(3 * std::min(n, c0 + chunk));
+#pragma omp parallel for schedule(static)
+      for (long long i = i0; i < i1; ++i) {
+        vel[i] = vel[i] + acc[i] * half;
+        pos[i] = pos[i] + vel[i] * dt;
+      }
+      GX_CK(h, cudaMemcpyAsync(b.pos + i0, pos + i0, (i1 - i0) * sizeof(double), cudaMemcpyHostToDevice,
+                               h->stream));
+    }
+    GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    enqueue_force(h, b, 0, 0, stats_on(h));
+    GX_CK(h, cudaMemcpyAsync(acc, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    h->stats.n = n;
+    rc = finish(h, stats_on(h));
+    if (rc) return rc;
+  } else {  // a lone particle: no force
+    for (size_t i = 0; i < 3; ++i) {
+      vel[i] = vel[i] + acc[i] * half;
+      pos[i] = pos[i] + vel[i] * dt;
+      acc[i] = 0.0;
+    }
+  }
+  const long long m = static_cast<long long>(3 * n);
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < m; ++i) vel[i] = vel[i] + acc[i] * half;
   return GX_OK;
 }
 
@@ -762,6 +851,63 @@ int gx_diagnostics(gx_handle* h, int with_potential, double* out) {
     for (double v : pp) out[1] += v;
   }
   return finish(h, false);
+}
+
+int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* tried, uint32_t* n_tried) {
+  if (!h || !best) return GX_ERR_INVALID_ARG;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "autotune before upload");
+  if (h->n < 2) return fail(h, GX_ERR_STATE, "autotune needs at least two particles");
+  cudaSetDevice(h->device);
+  int rc = finish(h, false);  // nothing of the caller's may still be in flight
+  if (rc) return rc;
+  const gx_options user = h->opt;
+  const uint32_t reps = repeats ? repeats : 3;
+  WalkCfg base = walk_cfg(h);
+  std::vector<gx_tuning> cand = tune_candidates(base, true);
+  StepBufs& b = h->ar.b;
+  int best_i = -1;
+  for (size_t i = 0; i < cand.size() && rc == GX_OK; ++i) {
+    h->opt.walk_block = cand[i].walk_block;
+    h->opt.walk_ctas_per_sm = cand[i].walk_ctas_per_sm;
+    // Force evaluations on the current positions recompute a(x) bit for bit, so the
+    // resident state is untouched whatever the candidate.
+    enqueue_force(h, b, 0, 0, false);
+    rc = finish(h, false);
+    std::vector<float> ms;
+    for (uint32_t r = 0; r < reps && rc == GX_OK; ++r) {
+      cudaEventRecord(h->ev[5], h->stream);
+      enqueue_force(h, b, 0, 0, false);
+      cudaEventRecord(h->ev[4], h->stream);
+      rc = finish(h, false);
+      float t = 0.f;
+      if (rc == GX_OK) cudaEventElapsedTime(&t, h->ev[5], h->ev[4]);
+      ms.push_back(t);
+    }
+    if (rc) break;
+    std::sort(ms.begin(), ms.end());
+    cand[i].ms = ms[ms.size() / 2];
+    if (best_i < 0 || cand[i].ms < cand[best_i].ms) best_i = static_cast<int>(i);
+  }
+  h->opt = user;
+  if (h->step_graph) {  // captured with the previous launch configuration
+    cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
+  if (rc) return rc;
+  *best = cand[best_i];
+  tuned_store(h->device, user, 0, h->n, *best);
+  if (tried) std::copy(cand.begin(), cand.end(), tried);
+  if (n_tried) *n_tried = static_cast<uint32_t>(cand.size());
+  return GX_OK;
+}
+
+int gx_tuning_lookup(int device, size_t n, const gx_options* opt, int batched, gx_tuning* out) {
+  if (!out) return GX_ERR_INVALID_ARG;
+  gx_options o{};
+  if (opt && opt->struct_size) o = *opt;
+  int dev = device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return GX_ERR_NO_DEVICE;
+  return tuned_lookup(dev, o, batched, n, out) ? GX_OK : GX_ERR_STATE;
 }
 
 int gx_get_stats(const gx_handle* h, gx_stats* out) {

@@ -71,6 +71,12 @@ WalkCfg bcfg(const gx_batch* bt, bool inside) {
   c.stats = (bt->opt.flags & GX_FLAG_STATS) ? 1 : 0;
   c.inside_test = inside ? 1 : 0;
   c.block = bt->opt.walk_block ? static_cast<int>(bt->opt.walk_block) : kWalkThreads;
+  gx_tuning t;
+  if (!bt->opt.walk_block && !bt->opt.walk_ctas_per_sm && tuned_lookup(bt->device, bt->opt, 1, bt->total, &t)) {
+    c.block = static_cast<int>(t.walk_block);
+    c.persistent_ctas = bt->sm_count * static_cast<int>(t.walk_ctas_per_sm);
+    return c;
+  }
   c.persistent_ctas = bt->sm_count * (bt->opt.walk_ctas_per_sm ? static_cast<int>(bt->opt.walk_ctas_per_sm)
                                                                : walk_resident_ctas(c));
   return c;
@@ -336,6 +342,53 @@ int gx_batch_set_graph(gx_batch* bt, int enable) {
   if (!bt) return GX_ERR_INVALID_ARG;
   bt->use_graph = enable != 0;
   if (!bt->use_graph) drop_graph(bt);
+  return GX_OK;
+}
+
+int gx_batch_autotune(gx_batch* bt, uint32_t repeats, gx_tuning* best, gx_tuning* tried, uint32_t* n_tried) {
+  if (!bt || !best) return GX_ERR_INVALID_ARG;
+  if (bt->systems.empty()) return bfail(bt, GX_ERR_STATE, "autotune of an empty batch");
+  cudaSetDevice(bt->device);
+  GB_CK(bt, cudaStreamSynchronize(bt->stream));
+  std::vector<size_t> all(bt->systems.size());
+  for (size_t i = 0; i < all.size(); ++i) all[i] = i;
+  bool inside = false;
+  int rc = upload_tables(bt, all, &inside);
+  if (rc) return rc;
+  bt->tables_dirty = false;
+  const gx_options user = bt->opt;
+  const uint32_t reps = repeats ? repeats : 3;
+  // The batch always walks with a persistent kernel (items of uneven systems).
+  std::vector<gx_tuning> cand = tune_candidates(bcfg(bt, inside), false);
+  int best_i = -1;
+  for (size_t i = 0; i < cand.size() && rc == GX_OK; ++i) {
+    bt->opt.walk_block = cand[i].walk_block;
+    bt->opt.walk_ctas_per_sm = cand[i].walk_ctas_per_sm;
+    // Force evaluations only (no kick or drift): every system's state is unchanged.
+    enqueue_step(bt, 0, inside);
+    rc = bfinish(bt);
+    std::vector<float> ms;
+    for (uint32_t r = 0; r < reps && rc == GX_OK; ++r) {
+      cudaEventRecord(bt->e0, bt->stream);
+      enqueue_step(bt, 0, inside);
+      cudaEventRecord(bt->e1, bt->stream);
+      rc = bfinish(bt);
+      float t = 0.f;
+      if (rc == GX_OK) cudaEventElapsedTime(&t, bt->e0, bt->e1);
+      ms.push_back(t);
+    }
+    if (rc) break;
+    std::sort(ms.begin(), ms.end());
+    cand[i].ms = ms[ms.size() / 2];
+    if (best_i < 0 || cand[i].ms < cand[best_i].ms) best_i = static_cast<int>(i);
+  }
+  bt->opt = user;
+  drop_graph(bt);  // captured with the previous launch configuration
+  if (rc) return rc;
+  *best = cand[best_i];
+  tuned_store(bt->device, user, 1, bt->total, *best);
+  if (tried) std::copy(cand.begin(), cand.end(), tried);
+  if (n_tried) *n_tried = static_cast<uint32_t>(cand.size());
   return GX_OK;
 }
 

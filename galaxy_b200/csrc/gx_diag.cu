@@ -6,7 +6,8 @@
 // U = -sum_{i<j} G m_i m_j / sqrt(r^2 + eps^2), evaluated as half of the full
 // double sum), core/src/diagnostics.rs:8-68 (kinetic energy, momentum, angular
 // momentum). Per-block partials are summed on the host in block order, so every
-// result is deterministic.
+// result is deterministic. Both O(N^2) sums use FMA and the FP64 reciprocal square
+// root (about 15 FP64 operations a pair); they are checks, compared with tolerances.
 #include "gx_kernels.h"
 
 namespace gx {
@@ -53,21 +54,23 @@ __global__ void __launch_bounds__(kDiagThreads) k_direct_sum_f64(uint32_t n, con
     __syncthreads();
     const uint32_t cnt = min((uint32_t)kDiagThreads, n - base);
     for (uint32_t q = 0; q < cnt; ++q) {
-      if (base + q == i) continue;
+      // the pair with itself adds nothing (massless, at unit distance)
+      const bool self = base + q == i;
       const double4 s = src[q];
-      const double dx = dsub(s.x, xi[0]), dy = dsub(s.y, xi[1]), dz = dsub(s.z, xi[2]);
-      const double r2 = dadd(dlen2(dx, dy, dz), eps2);
-      const double f = ddiv(s.w, dmul(r2, dsqrt(r2)));
-      a[0] = dadd(a[0], dmul(dx, f));
-      a[1] = dadd(a[1], dmul(dy, f));
-      a[2] = dadd(a[2], dmul(dz, f));
+      const double dx = s.x - xi[0], dy = s.y - xi[1], dz = s.z - xi[2];
+      const double r2 = self ? 1.0 : fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+      const double inv = rsqrt(r2);
+      const double f = (self ? 0.0 : s.w) * (inv * inv * inv);
+      a[0] = fma(dx, f, a[0]);
+      a[1] = fma(dy, f, a[1]);
+      a[2] = fma(dz, f, a[2]);
     }
   }
   if (valid)
-    for (int c = 0; c < 3; ++c) acc[3 * (size_t)t + c] = dmul(a[c], g);
+    for (int c = 0; c < 3; ++c) acc[3 * (size_t)t + c] = a[c] * g;
 }
 
-// partial[b] = sum over this block's rows i of sum_{j != i} -G m_i m_j / sqrt(r^2+eps^2) / 2.
+// partial[b] = sum over this block's rows i of -G m_i / 2 * sum_{j != i} m_j / sqrt(r^2+eps^2).
 __global__ void __launch_bounds__(kDiagThreads) k_potential_f64(uint32_t n, const double* __restrict__ pos,
                                                                const double* __restrict__ mass, double g, double eps2,
                                                                double* __restrict__ partial) {
@@ -91,14 +94,14 @@ __global__ void __launch_bounds__(kDiagThreads) k_potential_f64(uint32_t n, cons
     __syncthreads();
     const uint32_t cnt = min((uint32_t)kDiagThreads, n - base);
     for (uint32_t q = 0; q < cnt; ++q) {
-      if (base + q == i) continue;
+      const bool self = base + q == i;
       const double4 s = src[q];
-      const double dx = dsub(s.x, xi[0]), dy = dsub(s.y, xi[1]), dz = dsub(s.z, xi[2]);
-      const double r = dsqrt(dadd(dlen2(dx, dy, dz), eps2));
-      u = dsub(u, ddiv(dmul(dmul(g, mi), s.w), r));
+      const double dx = s.x - xi[0], dy = s.y - xi[1], dz = s.z - xi[2];
+      const double r2 = self ? 1.0 : fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+      u = fma(self ? 0.0 : s.w, rsqrt(r2), u);  // sum_j m_j / sqrt(r^2 + eps^2)
     }
   }
-  const double t = block_sum(valid ? 0.5 * u : 0.0, sh);
+  const double t = block_sum(valid ? -0.5 * g * mi * u : 0.0, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 

@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/galaxy_b200.h"
 #include "gx_kernels.h"
 
 namespace gx {
@@ -36,5 +37,13 @@ void make_tables(const std::vector<SysDesc>& in, std::vector<SysDesc>& sys, std:
 bool check_device(int device, std::string& err);
 void set_global_err(const std::string& s);
 const char* global_err();
+
+// Process-wide table of tuned walk launches (see gx_autotune): keyed by device,
+// precision, multipole, Morton key width, batch or single system and floor(log2 n).
+bool tuned_lookup(int device, const gx_options& opt, int batched, size_t n, gx_tuning* out);
+void tuned_store(int device, const gx_options& opt, int batched, size_t n, const gx_tuning& t);
+// Walk launch candidates: blocks of 64 and 128 threads, each as a grid of one warp per
+// item (ctas 0, when with_grid) and as a persistent kernel at half and full residency.
+std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid);
 
 }  // namespace gx

@@ -44,11 +44,13 @@ def batched_sizes(count: int, seed: int, n_min: int = 4096, n_max: int = 262_144
     return np.exp(rng.uniform(np.log(n_min), np.log(n_max), count)).astype(np.int64)
 
 
-def batched_mix(count: int = 256, seed: int = 0, n_min: int = 4096, n_max: int = 262_144) -> list[SystemSpec]:
+def batched_mix(count: int = 256, seed: int = 0, n_min: int = 4096, n_max: int = 262_144,
+                indices=None) -> list[SystemSpec]:
+    """The mix's systems (all of them, or those listed in `indices`)."""
     sizes = batched_sizes(count, seed, n_min, n_max)
     out = []
-    for i, n in enumerate(sizes):
-        n = int(n)
+    for i in (range(count) if indices is None else indices):
+        n = int(sizes[i])
         if i % 2 == 0:
             st = ic.plummer(n, seed * 100_003 + i)
             kind = "plummer"

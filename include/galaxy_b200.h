@@ -134,10 +134,34 @@ int gx_get_stats(const gx_handle* h, gx_stats* out);
  * (CUDA events on the handle's stream around the steps). */
 int gx_step_many_timed(gx_handle* h, double dt, uint64_t steps, float* ms_out);
 
+/* ---- autotuning of the walk launch (no counterpart in the reference) -------------
+ * The walk's block size and its scheduling (one warp per 32 targets over a grid, or a
+ * persistent kernel with CTAs per SM stealing items) are picked per N bucket
+ * (floor(log2 N)) by timing candidates on a resident state: force evaluations only,
+ * so the state, its trajectory and every result stay bit-identical. The winner is
+ * recorded in a process-wide table keyed by (device, precision, multipole, Morton key
+ * width, single system or batch, N bucket); handles and batches created with
+ * walk_block == 0 and walk_ctas_per_sm == 0 use the table's entry for their N. The
+ * radix sort keeps fixed 8-bit digits (4 passes, 8 with 63-bit keys): it is about 1%
+ * of a step at N = 2^20, so its digit width is not a tuning knob. */
+typedef struct gx_tuning {
+  uint32_t walk_block;       /* threads per block of the walk */
+  uint32_t walk_ctas_per_sm; /* 0 = grid of one warp per item; > 0 persistent CTAs per SM */
+  float ms;                  /* median device time of one force evaluation with it */
+} gx_tuning;
+#define GX_TUNE_MAX_CANDIDATES 8
+/* Time every candidate `repeats` times (median) on the handle's resident state; best
+ * (and, if non-NULL, tried[GX_TUNE_MAX_CANDIDATES] with *n_tried) receive the results. */
+int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* tried, uint32_t* n_tried);
+/* The table's entry for n particles under these options (batched != 0: a batch of n
+ * particles in total); GX_ERR_STATE when nothing has been tuned for that bucket. */
+int gx_tuning_lookup(int device, size_t n, const gx_options* opt, int batched, gx_tuning* out);
+
 /* LeapfrogKdk::step (core/src/integrator.rs:38-78) on HOST arrays with this handle as
- * the ForceSolver: half kick and drift on the host in f64, accelerations through
- * gx_accelerations (upload of pos and mass, download of acc). acc[3n] is the
- * integrator's cached acceleration and *primed its `primed` flag. */
+ * the ForceSolver: half kicks and drift on the host in f64 (the reference's operations,
+ * on all host threads), accelerations as gx_accelerations (upload of pos and mass,
+ * download of acc; positions are sent in chunks as soon as they are drifted). acc[3n]
+ * is the integrator's cached acceleration and *primed its `primed` flag. */
 int gx_kdk_step_host(gx_handle* h, size_t n, double* pos, double* vel, const double* mass, double* acc,
                      int* primed, double dt);
 
@@ -206,6 +230,8 @@ int gx_system_len(const gx_batch* b, uint64_t id, size_t* n_out);
 int gx_batch_stats_get(const gx_batch* b, gx_batch_stats* out);
 /* Capture one batched step as a CUDA graph and replay it (1) or launch eagerly (0). */
 int gx_batch_set_graph(gx_batch* b, int enable);
+/* gx_autotune for a batch: persistent walk candidates timed on the live systems. */
+int gx_batch_autotune(gx_batch* b, uint32_t repeats, gx_tuning* best, gx_tuning* tried, uint32_t* n_tried);
 
 /* ---- continuous-batching server ----------------------------------------------- */
 /* A stepping thread admits submitted systems in arrival order as the device budget

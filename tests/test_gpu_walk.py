@@ -167,7 +167,8 @@ def test_direct_sum_f64_matches_oracle(oracle):
     ref = oracle.direct_sum(pos, mass, G, EPS)
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.abs(ref).max()
     t = np.array([5, 17, 2999], np.uint32)
-    assert np.allclose(s.direct_sum_f64(pos, mass, t), ref[t], rtol=1e-12, atol=0)
+    sub = s.direct_sum_f64(pos, mass, t)
+    assert np.all(np.linalg.norm(sub - ref[t], axis=1) <= 1e-12 * np.linalg.norm(ref[t], axis=1))
 
 
 def test_potential_energy_matches_oracle(oracle):
