@@ -543,7 +543,7 @@ int gx_accelerations_device(gx_handle* h, size_t n, const double* d_pos, const d
 int gx_synchronize(gx_handle* h) {
   if (!h) return GX_ERR_INVALID_ARG;
   cudaSetDevice(h->device);
-  return finish(h, false);
+  return finish(h, stats_on(h));  // stage times of the last step when they are on
 }
 
 int gx_potential_energy(gx_handle* h, size_t n, const double* pos, const double* mass, double* out) {
@@ -685,7 +685,7 @@ int gx_step_many(gx_handle* h, double dt, uint64_t steps) {
   cudaSetDevice(h->device);
   int rc = step_enqueue(h, dt, steps);
   if (rc) return rc;
-  return finish(h, false);
+  return finish(h, stats_on(h));  // stage times of the last step when they are on
 }
 
 int gx_step(gx_handle* h, double dt) { return gx_step_many(h, dt, 1); }

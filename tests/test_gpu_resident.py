@@ -121,3 +121,20 @@ def test_step_before_upload_is_an_error():
     r = gb.GpuResidentLeapfrog(1.0, 0.01, 0.5)
     with pytest.raises(gb.GxError):
         r.step(1e-3)
+
+
+def test_stage_times_follow_each_step():
+    """With GX_FLAG_STAGE_TIMES the stage times are those of the latest step, not of
+    the priming force evaluation at upload."""
+    st = gb.ic.collision(65_536, 2)
+    r = gb.GpuResidentLeapfrog(1.0, 0.02, 0.5, stage_times=True)
+    r.upload(st)
+    seen = {r.stats()["ms_total"]}
+    for _ in range(3):
+        r.step(5e-4)
+        s = r.stats()
+        assert s["ms_walk"] > 0 and s["ms_build"] > 0 and s["ms_sort"] > 0
+        parts = s["ms_bbox_morton"] + s["ms_sort"] + s["ms_build"] + s["ms_walk"]
+        assert abs(parts - s["ms_total"]) <= 1e-3 * s["ms_total"] + 1e-3
+        seen.add(s["ms_total"])
+    assert len(seen) == 4
