@@ -61,6 +61,12 @@ struct ChildRec {
   float hx, hy, hz, lx, ly, lz, m, take, open;
 };
 
+// A child as the FP32 walk record names it: an internal node by its index, a leaf by
+// kLeafCode | leaf index (so the walk's next pair needs no offset arithmetic).
+__device__ __forceinline__ uint32_t child_code(uint32_t u, uint32_t n_total) {
+  return u >= n_total ? u - n_total : (kLeafCode | u);
+}
+
 // Geometry of an aggregate as reference_flatten derives it (solvers/src/lbvh.rs:602-613).
 __device__ __forceinline__ void node_geometry(const AggR& a, double ctr[3], double hf[3], double& delta, double& s) {
   double dv[3];
@@ -183,7 +189,8 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
         pp[1] = make_float4(pl.hz, pr.hz, pl.m, pr.m);
         pp[2] = make_float4(pl.lx, pr.lx, pl.ly, pr.ly);
         pp[3] = make_float4(pl.lz, pr.lz, pl.take, pr.take);
-        pp[4] = make_float4(pl.open, pr.open, __uint_as_float(lc), __uint_as_float(rc));
+        pp[4] = make_float4(pl.open, pr.open, __uint_as_float(child_code(lc, n_total)),
+                            __uint_as_float(child_code(rc, n_total)));
         b.nodeC[gi] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
         b.nodeD[gi] = make_float4(__double2float_rn(hf[0]), __double2float_rn(hf[1]), __double2float_rn(hf[2]), 0.f);
         if (f64rec) {

@@ -27,6 +27,8 @@ namespace gx {
 
 constexpr uint32_t kNoParent = 0xFFFFFFFFu;
 constexpr uint64_t kEmptySlot = 0xFFFFFFFFFFFFFFFFull;
+// Leaf flag of a child code in the FP32 walk records (N < 2^30, so it never collides).
+constexpr uint32_t kLeafCode = 0x80000000u;
 
 // Bounded waits: every spin in these kernels gives up after this many polls,
 // raises the device error word and carries on, so no kernel can hang the GPU.

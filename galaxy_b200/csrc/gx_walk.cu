@@ -278,14 +278,15 @@ __device__ __forceinline__ void inside_test(const StepBufs& b, const float xh[3]
   amb = amb || (t && near_face);
 }
 
-// FP64 decision of an undecided child u (a leaf is undecided only when massless: skip).
-__device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double theta, uint32_t u, uint32_t n_total,
-                                        bool& take, bool& open) {
+// FP64 decision of an undecided child with record code c (a leaf is undecided only
+// when massless: skip).
+__device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double theta, uint32_t c, bool& take,
+                                        bool& open) {
   int dec = -1;
-  if (u >= n_total) {
+  if (!(c & kLeafCode)) {
     const double4 p = b.leaf64[k];
     const double x[3] = {p.x, p.y, p.z};
-    dec = exact_decision(b.agg64, u - n_total, x, theta);
+    dec = exact_decision(b.agg64, c, x, theta);
   }
   take = dec == 1;
   open = dec == 0;
@@ -352,17 +353,20 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
       const uint32_t max_iters = sd.n + 64u;
       uint32_t iters = 0;
       float2 tx = f2(0.f, 0.f), ty = f2(0.f, 0.f), tz = f2(0.f, 0.f);  // per-child term sums
-      for (;;) {
+      // One pair: decide both children for every active lane, add the taken terms,
+      // move to the next pair. Returns false when the walk is over (or went wrong).
+      auto pair_step = [&]() -> bool {
         if (++iters > max_iters) {
           bad = true;
-          break;
+          return false;
         }
         bad |= g > gmax;
         g = min(g, gmax);
         if (STATS) ++n_vis;
         const float4* pr = pairs + 5 * (size_t)g;
         const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3), r4 = __ldg(pr + 4);
-        const uint32_t uL = __float_as_uint(r4.z), uR = __float_as_uint(r4.w);
+        // child codes: internal node index, or kLeafCode | leaf index
+        const uint32_t cL = __float_as_uint(r4.z), cR = __float_as_uint(r4.w);
         const bool act = (mask >> lane) & 1u;
         // d = (c_hi - x_hi) + (c_lo - x_lo) for both children at once
         const float2 dx = __fadd2_rn(__fadd2_rn(f2(r0.x, r0.y), nxh), __fadd2_rn(f2(r2.x, r2.y), nxl));
@@ -373,13 +377,13 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         bool oL = act && d2.x < r4.x, oR = act && d2.y < r4.y;
         bool aL = act && !tL && !oL, aR = act && !tR && !oR;
         if (INSIDE) {
-          if (tL && uL >= n_total) inside_test(b, xh, uL - n_total, tL, oL, aL);
-          if (tR && uR >= n_total) inside_test(b, xh, uR - n_total, tR, oR, aR);
+          if (tL && !(cL & kLeafCode)) inside_test(b, xh, cL, tL, oL, aL);
+          if (tR && !(cR & kLeafCode)) inside_test(b, xh, cR, tR, oR, aR);
         }
         if (__any_sync(0xffffffffu, aL || aR)) {
           if (STATS) n_re += (aL ? 1 : 0) + (aR ? 1 : 0);
-          if (aL) resolve(b, k, sd.theta, uL, n_total, tL, oL);
-          if (aR) resolve(b, k, sd.theta, uR, n_total, tR, oR);
+          if (aL) resolve(b, k, sd.theta, cL, tL, oL);
+          if (aR) resolve(b, k, sd.theta, cR, tR, oR);
         }
         // Plummer-softened monopole terms; r^2 > 0 keeps the target's own leaf (d = 0)
         // an exact zero term.
@@ -395,40 +399,18 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         tz = __ffma2_rn(dz, f, tz);
         if (QUAD) {
           float tq[3] = {0.f, 0.f, 0.f};
-          if (tL && uL >= n_total) {
-            const size_t gi = uL - n_total;
-            quad_term(__ldg(&b.nodeQ[2 * gi]), __ldg(&b.nodeQ[2 * gi + 1]), dx.x, dy.x, dz.x, invL, tq);
-          }
-          if (tR && uR >= n_total) {
-            const size_t gi = uR - n_total;
-            quad_term(__ldg(&b.nodeQ[2 * gi]), __ldg(&b.nodeQ[2 * gi + 1]), dx.y, dy.y, dz.y, invR, tq);
-          }
+          if (tL && !(cL & kLeafCode))
+            quad_term(__ldg(&b.nodeQ[2 * (size_t)cL]), __ldg(&b.nodeQ[2 * (size_t)cL + 1]), dx.x, dy.x, dz.x, invL, tq);
+          if (tR && !(cR & kLeafCode))
+            quad_term(__ldg(&b.nodeQ[2 * (size_t)cR]), __ldg(&b.nodeQ[2 * (size_t)cR + 1]), dx.y, dy.y, dz.y, invR, tq);
           tx.x += tq[0];
           ty.x += tq[1];
           tz.x += tq[2];
         }
-        if ((iters & 3u) == 0) {
-          // fold the children's sums and add them with compensation
-          const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
-          const float tzz = tz.x + tz.y;
-          if (KAHAN) {
-            const float2 y = __fadd2_rn(txy, f2(-cxy.x, -cxy.y));
-            const float2 u = __fadd2_rn(sxy, y);
-            cxy = __fadd2_rn(__fadd2_rn(u, f2(-sxy.x, -sxy.y)), f2(-y.x, -y.y));
-            sxy = u;
-            const float yz = tzz - cz;
-            const float uz = sz + yz;
-            cz = (uz - sz) - yz;
-            sz = uz;
-          } else {
-            sxy = __fadd2_rn(sxy, txy);
-            sz += tzz;
-          }
-          tx = ty = tz = f2(0.f, 0.f);
-        }
         if (STATS) {
-          n_leaf += (tL && uL < n_total && uL != k ? 1 : 0) + (tR && uR < n_total && uR != k ? 1 : 0);
-          n_far += (tL && uL >= n_total ? 1 : 0) + (tR && uR >= n_total ? 1 : 0);
+          const uint32_t self = kLeafCode | k;
+          n_leaf += (tL && (cL & kLeafCode) && cL != self ? 1 : 0) + (tR && (cR & kLeafCode) && cR != self ? 1 : 0);
+          n_far += (tL && !(cL & kLeafCode) ? 1 : 0) + (tR && !(cR & kLeafCode) ? 1 : 0);
           n_open += (oL ? 1 : 0) + (oR ? 1 : 0);
         }
         const uint32_t m0 = __ballot_sync(0xffffffffu, oL);
@@ -438,23 +420,47 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
             // push the right child; continue with the left one
             if (sp >= kStackCap) {
               bad = true;
-              break;
+              return false;
             }
-            if (lane == 0) stack[sp] = make_uint2(uR - n_total, m1);
+            if (lane == 0) stack[sp] = make_uint2(cR, m1);
             ++sp;
           }
-          g = uL - n_total;
+          g = cL;
           mask = m0;
         } else if (m1) {
-          g = uR - n_total;
+          g = cR;
           mask = m1;
         } else {
-          if (sp == 0) break;
+          if (sp == 0) return false;
           __syncwarp();
           const uint2 e = stack[--sp];
           g = e.x;
           mask = e.y;
         }
+        return true;
+      };
+      // fold the children's sums of the last four pairs and add them with compensation
+      auto fold = [&]() {
+        const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
+        const float tzz = tz.x + tz.y;
+        if (KAHAN) {
+          const float2 y = __fadd2_rn(txy, f2(-cxy.x, -cxy.y));
+          const float2 u = __fadd2_rn(sxy, y);
+          cxy = __fadd2_rn(__fadd2_rn(u, f2(-sxy.x, -sxy.y)), f2(-y.x, -y.y));
+          sxy = u;
+          const float yz = tzz - cz;
+          const float uz = sz + yz;
+          cz = (uz - sz) - yz;
+          sz = uz;
+        } else {
+          sxy = __fadd2_rn(sxy, txy);
+          sz += tzz;
+        }
+        tx = ty = tz = f2(0.f, 0.f);
+      };
+      for (;;) {
+        if (!pair_step() || !pair_step() || !pair_step() || !pair_step()) break;
+        fold();
       }
       // fold what is left
       const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
