@@ -356,10 +356,6 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
       // One pair: decide both children for every active lane, add the taken terms,
       // move to the next pair. Returns false when the walk is over (or went wrong).
       auto pair_step = [&]() -> bool {
-        if (++iters > max_iters) {
-          bad = true;
-          return false;
-        }
         bad |= g > gmax;
         g = min(g, gmax);
         if (STATS) ++n_vis;
@@ -459,6 +455,12 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         tx = ty = tz = f2(0.f, 0.f);
       };
       for (;;) {
+        // the iteration budget is checked once per four pairs
+        iters += 4;
+        if (iters > max_iters) {
+          bad = true;
+          break;
+        }
         if (!pair_step() || !pair_step() || !pair_step() || !pair_step()) break;
         fold();
       }
