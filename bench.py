@@ -121,13 +121,14 @@ def algorithmic(n: int, counts: dict) -> dict:
             "walk_flops": flops}
 
 
-def profiled_walk_traffic(workload_name: str):
-    """DRAM bytes per walk launch from the committed ncu summary of this workload (or None)."""
+def profiled_walk(workload_name: str, key: str):
+    """A per-launch figure of the walk (`traffic_bytes_per_launch`, `instructions_per_launch`)
+    from the committed ncu summary of this workload, or None."""
     import re
 
     path = os.path.join(ROOT, "profiles", f"k_walk_f32_{workload_name.replace('collision-', 'collision_')}.md")
     try:
-        m = re.search(r"traffic_bytes_per_launch:\s*(\d+)", open(path).read())
+        m = re.search(key + r":\s*(\d+)", open(path).read())
         return int(m.group(1)) if m else None
     except OSError:
         return None
@@ -251,7 +252,8 @@ def run_ours(args):
     sort_gbs = 4 * alg["sort_pass"] / (stage["ms_sort"] / 1e3) / 1e9
     build_gbs = alg["build"] / (stage["ms_build"] / 1e3) / 1e9
     mort_gbs = (alg["kick_bbox"] + alg["morton"]) / (stage["ms_bbox_morton"] / 1e3) / 1e9
-    traffic = profiled_walk_traffic(p["name"])
+    traffic = profiled_walk(p["name"], "traffic_bytes_per_launch")
+    inst = profiled_walk(p["name"], "instructions_per_launch")
     roofline = {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
@@ -260,6 +262,12 @@ def run_ours(args):
                 "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm "
                                "(MEASURED_PEAKS.json has no FP32 figure); no tensor-core work in this path",
                 "flops_per_launch": alg["walk_flops"], "ms_per_launch": stage["ms_walk"],
+                "issue": ({"achieved_ginst_s": inst / walk_s / 1e9,
+                           "peak_ginst_s": 148 * 4 * peaks.get("sm_max_mhz", 1965.0) / 1e3,
+                           "frac": inst / walk_s / 1e9 / (148 * 4 * peaks.get("sm_max_mhz", 1965.0) / 1e3),
+                           "source": "warp instructions per launch from the ncu summary in profiles/ over this "
+                                     "run's walk time; peak = one warp instruction per scheduler per clock"}
+                          if inst else None),
                 "interactions_per_particle": (counts["leaf"] + counts["far"]) / n,
                 "lane_utilisation": (counts["leaf"] + counts["far"] + counts["open"]) / (64.0 * counts["warp_visits"]),
                 "hbm_stages": {
