@@ -112,6 +112,14 @@ __device__ __forceinline__ ChildRec child_record(const AggR& a, bool leaf, doubl
 
 }  // namespace
 
+// Exchange with release (this thread's writes are visible before the new value) and
+// acquire (the previous owner's writes are visible after it) at device scope.
+__device__ __forceinline__ unsigned long long exch_acq_rel(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.exch.b64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
 template <bool QUAD, typename K>
 __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restrict__ tiles,
                                                         const SysDesc* __restrict__ sys, uint32_t n_total,
@@ -221,11 +229,8 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
       const uint32_t gamma = is_left ? r : l - 1;
       unsigned long long* slot = &b.slots[off + gamma];
       const unsigned long long mine = (static_cast<unsigned long long>(cur_u) << 32) | (is_left ? l : r);
-      __threadfence();
-      const unsigned long long old = atomicExch(slot, mine);
+      const unsigned long long old = exch_acq_rel(slot, mine);
       if (old == kEmptySlot) break;  // first to arrive: the sibling folds the parent
-      atomicExch(slot, kEmptySlot);  // both children have arrived: re-arm for the next build
-      __threadfence();
       const uint32_t sib_u = static_cast<uint32_t>(old >> 32);
       const uint32_t sib_far = static_cast<uint32_t>(old);
       if (!((sib_u >= off && sib_u < off + ns) || (sib_u >= n_total + off && sib_u < n_total + off + ns - 1)) ||
@@ -301,6 +306,9 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
 }
 
 void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st) {
+  // Every split's rendezvous slot starts empty (one memset instead of a re-arming
+  // atomic per fold, which the next level's release would have to wait for).
+  cudaMemsetAsync(b.slots, 0xFF, static_cast<size_t>(b.n) * sizeof(unsigned long long), st);
   const uint64_t* c64 = reinterpret_cast<const uint64_t*>(b.codes);
   if (b.key64) {
     if (quad)
