@@ -34,7 +34,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from galaxy_b200 import ranks  # noqa: E402  (rank discovery and reductions; no GPU work)
+from galaxy_b200 import ranks, roofline  # noqa: E402  (rank discovery, reductions, roofline arithmetic)
 
 METRIC = "particle-steps/s at theta=0.5 (resident KDK step, plain single-system path)"
 N_PER_GALAXY = 524_288
@@ -106,21 +106,6 @@ def workload(config: str, seed: int):
 
 
 # ---- algorithmic work per launch (bytes / flops) ----------------------------------------
-def algorithmic(n: int, counts: dict) -> dict:
-    # Per-stage compulsory bytes (inputs read once, outputs written once):
-    #   kick+drift+bbox: pos, vel, acc read (72 B) + pos, vel written (48 B)      = 120 N
-    #   Morton + histograms: pos read (24 B) + code written (4 B)                  =  28 N
-    #   onesweep pass: (key, index) read + written                                 =  16 N per pass
-    #   build: sorted codes + order (8 B) + gathered pos/mass (32 B) read; leaf64 +
-    #          leafA/B (64 B), kids/parent (16 B), agg64 (80 B), node records (64 B)
-    #          written; sibling aggregate read (80 B)                              = 344 N
-    #   walk: node records + leaves read once (96 B), target leaves (48 B), acc (24 B)
-    # Walk FLOPs: 20 per leaf term, 24 per far term (Kahan), 18 per opened node.
-    flops = 20 * counts["leaf"] + 24 * counts["far"] + 18 * counts["open"]
-    return {"kick_bbox": 120 * n, "morton": 28 * n, "sort_pass": 16 * n, "build": 344 * n, "walk_bytes": 168 * n,
-            "walk_flops": flops}
-
-
 def profiled_walk(workload_name: str, key: str):
     """A per-launch figure of the walk (`traffic_bytes_per_launch`, `instructions_per_launch`)
     from the committed ncu summary of this workload, or None."""
@@ -243,28 +228,30 @@ def run_ours(args):
     c = counts_h.stats()
     counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"],
               "warp_visits": c["warp_node_visits"], "f64_rechecks": c["f64_rechecks"]}
-    alg = algorithmic(n, counts)
+    quad = mp == "quad"
+    sb = roofline.stage_bytes(n, key64=False, quad=quad)
+    alg = {"walk_flops": roofline.walk_flops(counts["leaf"], counts["far"], counts["open"], quad=quad)}
     walk_s = stage["ms_walk"] / 1e3
     sm_clock = (clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     achieved = alg["walk_flops"] / walk_s / 1e12
     hbm = peaks.get("hbm_gbs", 6650.0)
-    sort_gbs = 4 * alg["sort_pass"] / (stage["ms_sort"] / 1e3) / 1e9
-    build_gbs = alg["build"] / (stage["ms_build"] / 1e3) / 1e9
-    mort_gbs = (alg["kick_bbox"] + alg["morton"]) / (stage["ms_bbox_morton"] / 1e3) / 1e9
+    sort_gbs = roofline.hbm_fraction(sb["sort"], stage["ms_sort"], hbm)[0]
+    build_gbs = roofline.hbm_fraction(sb["build"], stage["ms_build"], hbm)[0]
+    mort_gbs = roofline.hbm_fraction(sb["kick_drift_bbox"] + sb["morton"], stage["ms_bbox_morton"], hbm)[0]
     traffic = profiled_walk(p["name"], "traffic_bytes_per_launch")
     inst = profiled_walk(p["name"], "instructions_per_launch")
-    roofline = {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+    roof = {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
                                   "profiles/k_walk_f32_collision_2x524288.md" if traffic else None,
-                "algorithmic_bytes_per_launch": alg["walk_bytes"],
+                "algorithmic_bytes_per_launch": sb["walk"],
                 "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm "
                                "(MEASURED_PEAKS.json has no FP32 figure); no tensor-core work in this path",
                 "flops_per_launch": alg["walk_flops"], "ms_per_launch": stage["ms_walk"],
-                "issue": ({"achieved_ginst_s": inst / walk_s / 1e9,
+                "issue": ({"achieved_ginst_s": roofline.issue_fraction(inst, stage["ms_walk"], 148, peaks.get("sm_max_mhz", 1965.0))[0],
                            "peak_ginst_s": 148 * 4 * peaks.get("sm_max_mhz", 1965.0) / 1e3,
-                           "frac": inst / walk_s / 1e9 / (148 * 4 * peaks.get("sm_max_mhz", 1965.0) / 1e3),
+                           "frac": roofline.issue_fraction(inst, stage["ms_walk"], 148, peaks.get("sm_max_mhz", 1965.0))[1],
                            "source": "warp instructions per launch from the ncu summary in profiles/ over this "
                                      "run's walk time; peak = one warp instruction per scheduler per clock"}
                           if inst else None),
@@ -272,12 +259,12 @@ def run_ours(args):
                 "lane_utilisation": (counts["leaf"] + counts["far"] + counts["open"]) / (64.0 * counts["warp_visits"]),
                 "hbm_stages": {
                     "sort (4 onesweep passes)": {"achieved_gbs": sort_gbs, "frac": sort_gbs / hbm,
-                                                 "ms": stage["ms_sort"], "bytes": 4 * alg["sort_pass"]},
+                                                 "ms": stage["ms_sort"], "bytes": sb["sort"]},
                     "build + aggregation": {"achieved_gbs": build_gbs, "frac": build_gbs / hbm,
-                                            "ms": stage["ms_build"], "bytes": alg["build"]},
+                                            "ms": stage["ms_build"], "bytes": sb["build"]},
                     "kick/drift/bbox + Morton": {"achieved_gbs": mort_gbs, "frac": mort_gbs / hbm,
                                                  "ms": stage["ms_bbox_morton"],
-                                                 "bytes": alg["kick_bbox"] + alg["morton"]},
+                                                 "bytes": sb["kick_drift_bbox"] + sb["morton"]},
                     "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
 
     cpu = None
@@ -300,7 +287,7 @@ def run_ours(args):
                                   f"working set ~{352 * n / 1e6:.0f} MB fits in L2: steps replay back to back with the state resident, as a resident integrator runs (not a flushed-cache number)"),
                            "cuda_graph": True,
                            "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}},
-                "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "walk_counts": counts}
         print(json.dumps(line), flush=True)
     if dist is not None:
