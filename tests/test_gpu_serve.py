@@ -69,3 +69,22 @@ def test_oversize_request_rejected():
     small = srv.submit(gb.ic.plummer(2000, 2), 1.0, 0.01, 0.5, 1e-3, 5)
     srv.wait(small, 60)
     assert srv.status(small)[0] == gb.Server.DONE
+
+
+def test_budget_admits_as_room_frees():
+    """A budget that holds two systems at a time: four requests all finish, at most two
+    are resident at once, the later ones wait in the queue, and every result still
+    equals the system stepped alone."""
+    one = gb.Batch().system_bytes(20_000)
+    srv = gb.Server(budget_bytes=int(2.4 * one))
+    reqs = [(gb.ic.plummer(20_000, 300 + i), 12 + 4 * i) for i in range(4)]
+    rids = [srv.submit(st, 1.0, 0.01, 0.5, 1e-3, steps) for st, steps in reqs]
+    for rid in rids:
+        srv.wait(rid, 300)
+    s = srv.stats()
+    assert s["completed"] == 4 and s["max_live"] == 2
+    assert s["queue_s_p99"] > 0.0
+    for rid, (st, steps) in zip(rids, reqs):
+        got = srv.result(rid)
+        ref = _alone(st, 0.01, 0.5, 1e-3, steps)
+        assert np.array_equal(got.pos, ref.pos) and np.array_equal(got.vel, ref.vel)
