@@ -13,6 +13,8 @@
 // of the keys), so each pass reads and writes every (key, index) pair once.
 // Tiles never straddle systems and each system has its own histograms and
 // look-back chain, so a batch of systems is sorted per system in one launch.
+#include <mutex>
+
 #include "gx_kernels.h"
 
 namespace gx {
@@ -191,14 +193,19 @@ template <typename K>
 void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K* keys_tmp, uint32_t* vals_tmp,
                 const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist, uint32_t* status,
                 uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
-  // The dynamic shared-memory opt-in is a per-device function attribute.
+  // The dynamic shared-memory opt-in is a per-device function attribute, set once per
+  // device (handles on several host threads may reach here together).
+  static std::mutex mu;
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(onesweep_smem<K>()));
-    attr_set[dev] = true;
+  if (dev >= 0 && dev < 64) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!attr_set[dev]) {
+      cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(onesweep_smem<K>()));
+      attr_set[dev] = true;
+    }
   }
   const K* kin = keys_in;
   const uint32_t* vin = nullptr;
