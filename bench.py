@@ -188,8 +188,10 @@ def run_ours(args):
     r.step_many(dt, 1)  # re-capture the step graph outside the timed region
     clocks = ClockSampler(local)
     clocks.start()
+    gb.device_synchronize(local)
     ranks.barrier(dist, local)
     ms = r.step_many_timed(dt, args.steps)
+    gb.device_synchronize(local)
     ranks.barrier(dist, local)
     clk = clocks.stop()
     ms_max = ranks.max_over_ranks(dist, ms, local)
@@ -200,10 +202,12 @@ def run_ours(args):
     h = gb.GpuLbvh(1.0, p["eps"], p["theta"], multipole=mp, device=local)
     primed = h.kdk_step_host(pinned, dt, primed=False)  # prime + one step (warm-up)
     k_e2e = max(1, min(args.steps, 10))
+    gb.device_synchronize(local)
     ranks.barrier(dist, local)
     t0 = time.perf_counter()
     for _ in range(k_e2e):
         primed = h.kdk_step_host(pinned, dt, primed=primed)
+    gb.device_synchronize(local)
     t_e2e = time.perf_counter() - t0
     ranks.barrier(dist, local)
     t_e2e = ranks.max_over_ranks(dist, t_e2e, local)
@@ -317,11 +321,13 @@ def run_batched(args):
     b.step(1)  # re-capture the step graph outside the timed region
     clocks = ClockSampler(local)
     clocks.start()
+    gb.device_synchronize(local)
     ranks.barrier(dist, local)
     ms = []
     for _ in range(args.steps):
         b.step(1)
         ms.append(b.stats()["ms_last_step"])
+    gb.device_synchronize(local)
     ranks.barrier(dist, local)
     clk = clocks.stop()
     t = ranks.max_over_ranks(dist, sum(ms) / 1e3, local)

@@ -34,7 +34,7 @@ __all__ = [
     "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "Server", "GxError",
     "PinnedState",
     "stage_morton",
-    "stage_sort", "stage_build", "device_info", "ic", "tuning_lookup",
+    "stage_sort", "stage_build", "device_info", "device_synchronize", "ic", "tuning_lookup",
 ]
 
 
@@ -516,6 +516,11 @@ def tuning_lookup(n: int, batched: bool = False, precision: str = "f32", multipo
         return None
     check(rc, None)
     return {"walk_block": t.walk_block, "walk_ctas_per_sm": t.walk_ctas_per_sm, "ms": t.ms}
+
+
+def device_synchronize(device: int = -1) -> None:
+    """Wait for all device work (cudaDeviceSynchronize), e.g. around a timed region."""
+    check(lib().gx_device_synchronize(int(device)), None)
 
 
 def device_info(device: int = 0) -> dict:

@@ -117,6 +117,7 @@ SIGNATURES = {
     "gx_destroy": (None, [_vp]),
     "gx_last_error": (C.c_char_p, [_vp]),
     "gx_device_info": (_i, [_i, C.c_char_p, _sz, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_sz)]),
+    "gx_device_synchronize": (_i, [_i]),
     "gx_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_accelerations_device": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_potential_energy": (_i, [_vp, _sz, _vp, _vp, C.POINTER(_d)]),

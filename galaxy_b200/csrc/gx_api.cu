@@ -477,6 +477,18 @@ void gx_destroy(gx_handle* h) {
 
 const char* gx_last_error(const gx_handle* h) { return h ? h->err.c_str() : global_err(); }
 
+int gx_device_synchronize(int device) {
+  int dev = device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return GX_ERR_NO_DEVICE;
+  cudaError_t e = cudaSetDevice(dev);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    set_global_err(std::string("device synchronize: ") + cudaGetErrorString(e));
+    return GX_ERR_CUDA;
+  }
+  return GX_OK;
+}
+
 int gx_device_info(int device, char* name_out, size_t name_len, int* sm_count, int* cc_major, int* cc_minor,
                    size_t* total_mem) {
   cudaDeviceProp p;

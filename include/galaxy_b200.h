@@ -89,6 +89,9 @@ void gx_destroy(gx_handle* h);
 const char* gx_last_error(const gx_handle* h);
 int gx_device_info(int device, char* name_out, size_t name_len, int* sm_count, int* cc_major, int* cc_minor,
                    size_t* total_mem);
+/* Wait until all work on the device has finished (every stream, every handle). A timing
+ * helper with no counterpart in the reference. */
+int gx_device_synchronize(int device);
 
 /* ---- ForceSolver (core/src/traits.rs:27, :95) ------------------------------- */
 /* ForceSolver::accelerations -- gpu/src/gpu_lbvh_fused.rs:58-134, solvers/src/lbvh.rs:663-676.
