@@ -74,10 +74,25 @@ class State:
 
 
 class ForceSolver:
-    """core/src/traits.rs:24-157 (the gravity part of the trait)."""
+    """core/src/traits.rs:24-157 (the gravity part of the trait, with its defaults)."""
 
     def accelerations(self, state: State, acc: np.ndarray) -> None:
         raise NotImplementedError
+
+    def accelerations_active(self, state: State, active, acc: np.ndarray):
+        """traits.rs:52-54 default: the full pass (rows outside ``active`` unspecified)."""
+        return self.accelerations(state, acc)
+
+    def rebuild_gravity_cache(self, state: State) -> None:
+        """traits.rs:78 default: nothing to cache."""
+
+    def gravity_active_cached(self, state: State, active, acc: np.ndarray):
+        """traits.rs:89-91 default: a fresh full pass."""
+        return self.accelerations(state, acc)
+
+    def max_stable_dt(self, state: State) -> float:
+        """traits.rs:106-108 default: pure gravity imposes no step limit."""
+        return float("inf")
 
     def potential_energy(self, state: State) -> float:
         raise NotImplementedError
@@ -150,6 +165,33 @@ class GpuLbvh(_Handle, ForceSolver):
             raise ValueError("acc length must match particle count (C-contiguous f64 [n,3])")
         self._ck(lib().gx_accelerations(self._h, n, _ptr(pos), _ptr(m), _ptr(out)))
         return out
+
+    def accelerations_active(self, state, active, acc=None, mass=None):
+        """ForceSolver::accelerations_active (core/src/traits.rs:52-54): fill acc[i] for
+        i in ``active`` with what ``accelerations`` gives particle i, walking the tree for
+        those targets only; other rows of ``acc`` are left as they are."""
+        if isinstance(state, State):
+            pos, m = state.pos, state.mass
+        else:
+            pos, m = _f64(state).reshape(-1, 3), _f64(mass).reshape(-1)
+        n = pos.shape[0]
+        out = acc if acc is not None else np.zeros((n, 3))
+        if out.shape != (n, 3) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("acc length must match particle count (C-contiguous f64 [n,3])")
+        idx = np.ascontiguousarray(active, dtype=np.int64).reshape(-1)
+        if idx.size and (idx.min() < 0 or idx.max() >= n):
+            raise ValueError("active index out of range")
+        idx = idx.astype(np.uint32)
+        self._ck(lib().gx_accelerations_active(self._h, n, _ptr(pos), _ptr(m), idx.size, _ptr(idx), _ptr(out)))
+        return out
+
+    def rebuild_gravity_cache(self, state) -> None:
+        """ForceSolver::rebuild_gravity_cache (core/src/traits.rs:78): Lbvh caches nothing."""
+
+    def gravity_active_cached(self, state, active, acc=None, mass=None):
+        """ForceSolver::gravity_active_cached (core/src/traits.rs:89-91), which Lbvh keeps
+        at its default: the accelerations of a fresh pass, here for the active targets."""
+        return self.accelerations_active(state, active, acc, mass)
 
     def potential_energy(self, state, mass=None) -> float:
         pos, m = (state.pos, state.mass) if isinstance(state, State) else (_f64(state).reshape(-1, 3), _f64(mass))

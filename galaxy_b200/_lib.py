@@ -120,6 +120,7 @@ SIGNATURES = {
     "gx_device_synchronize": (_i, [_i]),
     "gx_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_accelerations_device": (_i, [_vp, _sz, _vp, _vp, _vp]),
+    "gx_accelerations_active": (_i, [_vp, _sz, _vp, _vp, _sz, _vp, _vp]),
     "gx_potential_energy": (_i, [_vp, _sz, _vp, _vp, C.POINTER(_d)]),
     "gx_direct_sum_f64": (_i, [_vp, _sz, _vp, _vp, _sz, _vp, _vp]),
     "gx_upload": (_i, [_vp, _sz, _vp, _vp, _vp]),

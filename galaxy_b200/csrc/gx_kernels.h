@@ -39,7 +39,8 @@ struct StepBufs {
   // side (L, R), so a float4 load yields float2 (L, R) operand pairs:
   //   pairs[5i+0] = (x_hi L, R, y_hi L, R)   pairs[5i+1] = (z_hi L, R, mass L, R)
   //   pairs[5i+2] = (x_lo L, R, y_lo L, R)   pairs[5i+3] = (z_lo L, R, take L, R)
-  //   pairs[5i+4] = (open L, R, child L, child R)   (children as unified indices)
+  //   pairs[5i+4] = (open L, R, child L, child R)   (child codes: internal node index, or
+  //                                                   kLeafCode | leaf index)
   // take / open: d^2 thresholds of the FP32 opening test (leaf: take -1, open -2).
   float4* pairs = nullptr;
   // internal nodes
@@ -53,6 +54,13 @@ struct StepBufs {
   Node64* node64 = nullptr;  // FP64 walk mode
   unsigned long long* slots = nullptr;  // climb exchange words, kEmptySlot between builds
   DevCtl* ctl = nullptr;
+  // Target list of an active-subset walk (nullptr: every particle is a target). Item i
+  // then covers targets[g i .. g i + g - 1] (sorted positions), g = group (a power of two
+  // <= 32: sparse subsets use fewer lanes a warp so each warp's targets stay close);
+  // *ntargets is their count.
+  const uint32_t* targets = nullptr;
+  const uint32_t* ntargets = nullptr;
+  uint32_t group = 32;
 };
 
 struct WalkCfg {
@@ -82,6 +90,15 @@ void launch_code_hist(const StepBufs& b, cudaStream_t st);
 void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st);
 // gx_walk.cu: tree walk, acc in original order
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st);
+// gx_active.cu: the active-subset walk's target list. From the sorted order and the
+// active particles (original indices) it builds, in sorted order, the list of active
+// sorted positions (list, count in *count_out) and one walk item per `group` of them.
+void launch_active_targets(const StepBufs& b, const uint32_t* active, uint32_t n_active, uint32_t group,
+                           uint32_t* inv, uint32_t* flags, uint32_t* chunk_counts, uint32_t* list,
+                           uint32_t* count_out, WalkItem* items, cudaStream_t st);
+size_t active_chunk_count(uint32_t n);
+// out[3i + c] = acc[3 active[i] + c]
+void launch_gather_acc(const double* acc, const uint32_t* active, uint32_t n_active, double* out, cudaStream_t st);
 // Blocks of cfg.block threads of the selected walk kernel resident on one SM.
 int walk_resident_ctas(const WalkCfg& cfg);
 // gx_diag.cu

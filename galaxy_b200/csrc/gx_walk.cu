@@ -116,7 +116,7 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 // Exact FP64 walk: one node per warp iteration in strict depth-first, left-before-right
 // order, so each lane adds its terms in the reference's order with the reference's
 // arithmetic.
-template <bool STATS>
+template <bool STATS, bool LIST>
 __global__ void __launch_bounds__(kWalkThreads) k_walk_f64(StepBufs b, int persistent) {
   const int lane = threadIdx.x & 31;
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
@@ -126,8 +126,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_walk_f64(StepBufs b, int persi
     const WalkItem it = b.items[item];
     const SysDesc sd = b.sys[it.sys];
     const uint32_t end = sd.off + sd.n;
-    const uint32_t k = it.begin + lane;
-    const bool valid = k < end;
+    // a target list (active-subset walk) names the item's targets; else they are the
+    // 32 sorted positions from it.begin
+    const uint32_t li = it.begin + lane;
+    const bool valid = LIST ? (lane < static_cast<int>(b.group) && li < *b.ntargets) : li < end;
+    const uint32_t k = LIST ? (valid ? b.targets[li] : 0u) : li;
     if (sd.n == 1) {
       if (valid) {
         const uint32_t o = b.order[k];
@@ -310,7 +313,7 @@ __device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double th
 // corrupt tree cannot read out of bounds; a clamp or an exhausted iteration budget
 // raises the device error word. Each lane takes exactly the reference's set of
 // terms; only the order of summation differs from the FP64 walk.
-template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE>
+template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE, bool LIST>
 __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBufs b, int persistent) {
   __shared__ uint2 s_stack[kWalkThreads / 32][kStackCap];  // (internal node, lane mask)
   const int lane = threadIdx.x & 31;
@@ -323,8 +326,11 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
     const WalkItem it = b.items[item];
     const SysDesc sd = b.sys[it.sys];
     const uint32_t end = sd.off + sd.n;
-    const uint32_t k = it.begin + lane;
-    const bool valid = k < end;
+    // a target list (active-subset walk) names the item's targets; else they are the
+    // 32 sorted positions from it.begin
+    const uint32_t li = it.begin + lane;
+    const bool valid = LIST ? (lane < static_cast<int>(b.group) && li < *b.ntargets) : li < end;
+    const uint32_t k = LIST ? (valid ? b.targets[li] : 0u) : li;
     // Kahan state: (x, y) packed, z scalar.
     float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
     float sz = 0.f, cz = 0.f;
@@ -530,18 +536,40 @@ void launch_k(K kern, const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
   }
 }
 
-template <bool QUAD, bool KAHAN>
+template <bool QUAD, bool KAHAN, bool LIST>
 void dispatch_f32(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
   if (cfg.stats) {
     if (cfg.inside_test)
-      launch_k(k_walk_f32<QUAD, KAHAN, true, true>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, true, true, LIST>, b, cfg, st);
     else
-      launch_k(k_walk_f32<QUAD, KAHAN, true, false>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, true, false, LIST>, b, cfg, st);
   } else {
     if (cfg.inside_test)
-      launch_k(k_walk_f32<QUAD, KAHAN, false, true>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, false, true, LIST>, b, cfg, st);
     else
-      launch_k(k_walk_f32<QUAD, KAHAN, false, false>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, false, false, LIST>, b, cfg, st);
+  }
+}
+
+template <bool LIST>
+void dispatch(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
+  if (cfg.precision == 1) {
+    // The FP64 walk has no quadrupole or compensation variants: it is the
+    // reference's arithmetic.
+    if (cfg.stats)
+      launch_k(k_walk_f64<true, LIST>, b, cfg, st);
+    else
+      launch_k(k_walk_f64<false, LIST>, b, cfg, st);
+  } else if (cfg.quad) {
+    if (cfg.kahan)
+      dispatch_f32<true, true, LIST>(b, cfg, st);
+    else
+      dispatch_f32<true, false, LIST>(b, cfg, st);
+  } else {
+    if (cfg.kahan)
+      dispatch_f32<false, true, LIST>(b, cfg, st);
+    else
+      dispatch_f32<false, false, LIST>(b, cfg, st);
   }
 }
 
@@ -560,30 +588,18 @@ int resident(K kern, int block) {
 
 int walk_resident_ctas(const WalkCfg& cfg) {
   const int block = cfg.block > 0 ? cfg.block : kWalkThreads;
-  if (cfg.precision == 1) return resident(k_walk_f64<false>, block);
-  if (cfg.quad) return resident(k_walk_f32<true, true, false, false>, block);
-  return resident(k_walk_f32<false, true, false, false>, block);
+  if (cfg.precision == 1) return resident(k_walk_f64<false, false>, block);
+  if (cfg.quad) return resident(k_walk_f32<true, true, false, false, false>, block);
+  return resident(k_walk_f32<false, true, false, false, false>, block);
 }
 
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
-  if (cfg.precision == 1) {
-    // The FP64 walk has no quadrupole or compensation variants: it is the
-    // reference's arithmetic.
-    if (cfg.stats)
-      launch_k(k_walk_f64<true>, b, cfg, st);
-    else
-      launch_k(k_walk_f64<false>, b, cfg, st);
-  } else if (cfg.quad) {
-    if (cfg.kahan)
-      dispatch_f32<true, true>(b, cfg, st);
-    else
-      dispatch_f32<true, false>(b, cfg, st);
-  } else {
-    if (cfg.kahan)
-      dispatch_f32<false, true>(b, cfg, st);
-    else
-      dispatch_f32<false, false>(b, cfg, st);
-  }
+  // A target list (active-subset walk) has its own instantiations, so the full walk's
+  // code is not burdened with it.
+  if (b.targets)
+    dispatch<true>(b, cfg, st);
+  else
+    dispatch<false>(b, cfg, st);
 }
 
 }  // namespace gx

@@ -101,6 +101,14 @@ int gx_accelerations(gx_handle* h, size_t n, const double* pos, const double* ma
 /* Same on device pointers (pos[3n], mass[n], acc_out[3n] f64 in device memory),
  * enqueued on the handle's stream; no host synchronisation. */
 int gx_accelerations_device(gx_handle* h, size_t n, const double* d_pos, const double* d_mass, double* d_acc);
+/* ForceSolver::accelerations_active (core/src/traits.rs:52-54) and gravity_active_cached
+ * (:89-91; Lbvh keeps both defaults: the accelerations of a fresh full pass). For every i in
+ * active[0 .. n_active), acc_out[3i .. 3i+2] receives the acceleration gx_accelerations gives
+ * particle i (FP64 walk: bit for bit; FP32: within the walk's rounding). The tree is built
+ * from all n particles and walked for the active ones only; acc_out entries of inactive
+ * particles are left as they are. Indices >= n are GX_ERR_INVALID_ARG; repeats are allowed. */
+int gx_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
+                            const uint32_t* active, double* acc_out);
 /* ForceSolver::potential_energy -- gpu/src/gpu_lbvh_fused.rs:140-146 delegating to
  * solvers/src/potential.rs:51-58: the exact O(N^2) softened potential, here an FP64
  * GPU reduction. */
