@@ -32,6 +32,15 @@ extern "C" {
     fn gx_destroy(h: *mut GxHandle);
     fn gx_last_error(h: *const GxHandle) -> *const c_char;
     fn gx_accelerations(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, acc: *mut f64) -> c_int;
+    fn gx_accelerations_active(
+        h: *mut GxHandle,
+        n: usize,
+        pos: *const f64,
+        mass: *const f64,
+        n_active: usize,
+        active: *const u32,
+        acc: *mut f64,
+    ) -> c_int;
     fn gx_potential_energy(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, out: *mut f64) -> c_int;
     fn gx_upload(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64) -> c_int;
     fn gx_step_many(h: *mut GxHandle, dt: f64, steps: u64) -> c_int;
@@ -91,6 +100,31 @@ impl ForceSolver for GpuLbvhB200 {
         };
         // A device failure here is a lost GPU, as in GpuLbvhFused: panic rather than corrupt state.
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    // The individual-timestep path: walk the tree for the active targets only; each gets
+    // the acceleration `accelerations` would give it (rows outside `active` untouched).
+    fn accelerations_active(&mut self, state: &State, active: &[usize], acc: &mut [DVec3]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        let idx: Vec<u32> = active.iter().map(|&i| u32::try_from(i).expect("active index fits u32")).collect();
+        let rc = unsafe {
+            gx_accelerations_active(
+                self.h,
+                n,
+                as_f64(&state.pos),
+                state.mass.as_ptr(),
+                idx.len(),
+                idx.as_ptr(),
+                acc.as_mut_ptr() as *mut f64,
+            )
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    // Lbvh caches nothing between calls: the stale-tree walk is a fresh active pass.
+    fn gravity_active_cached(&mut self, state: &State, active: &[usize], acc: &mut [DVec3]) {
+        self.accelerations_active(state, active, acc);
     }
 
     fn potential_energy(&self, state: &State) -> f64 {
