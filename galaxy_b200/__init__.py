@@ -31,7 +31,8 @@ from ._lib import (GX_FLAG_MORTON63, GX_FLAG_NO_KAHAN, GX_FLAG_STAGE_TIMES, GX_F
                    GX_MULTIPOLE_QUAD, GX_PREC_F32, GX_PREC_F64, GxError, check, lib)
 
 __all__ = [
-    "State", "ForceSolver", "GpuLbvh", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch", "Server", "GxError",
+    "State", "ForceSolver", "GpuLbvh", "GpuStaleTreeGravity", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch",
+    "Server", "GxError",
     "PinnedState",
     "stage_morton",
     "stage_sort", "stage_build", "device_info", "device_synchronize", "ic", "tuning_lookup",
@@ -215,6 +216,48 @@ class GpuLbvh(_Handle, ForceSolver):
         nt = pos.shape[0] if t is None else t.shape[0]
         out = np.empty((nt, 3))
         self._ck(lib().gx_direct_sum_f64(self._h, pos.shape[0], _ptr(pos), _ptr(mass), nt, _ptr(t), _ptr(out)))
+        return out
+
+
+class GpuStaleTreeGravity(GpuLbvh):
+    """TreeGravity's stale-tree active walk (solvers/src/barnes_hut.rs:647-711) over the
+    LBVH: ``rebuild_gravity_cache`` freezes the tree at the block-start state;
+    ``gravity_active_cached`` walks it for the active targets at the current positions
+    (leaf sources current, internal aggregates frozen); ``accelerations`` is a fresh
+    full pass, on a second handle so that it leaves the cache alone."""
+
+    def __init__(self, g, softening, theta, **kw):
+        super().__init__(g, softening, theta, **kw)
+        self._kw = dict(kw)
+        self._fresh = None
+        self._cached = False
+
+    def accelerations(self, state, acc=None, mass=None):
+        if self._fresh is None:
+            self._fresh = GpuLbvh(self.g, self.softening, self.theta, **self._kw)
+        return self._fresh.accelerations(state, acc, mass)
+
+    def rebuild_gravity_cache(self, state, mass=None) -> None:
+        pos, m = (state.pos, state.mass) if isinstance(state, State) else (_f64(state).reshape(-1, 3), _f64(mass))
+        self._ck(lib().gx_rebuild_gravity_cache(self._h, pos.shape[0], _ptr(pos), _ptr(m)))
+        self._cached = pos.shape[0] > 0  # an empty system has no tree (the reference's None)
+
+    def gravity_active_cached(self, state, active, acc=None, mass=None):
+        if isinstance(state, State):
+            pos, m = state.pos, state.mass
+        else:
+            pos, m = _f64(state).reshape(-1, 3), _f64(mass).reshape(-1)
+        n = pos.shape[0]
+        out = acc if acc is not None else np.zeros((n, 3))
+        if out.shape != (n, 3) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("acc length must match particle count (C-contiguous f64 [n,3])")
+        if not self._cached:
+            return out  # never rebuilt (or empty): nothing to walk, as the reference
+        idx = np.ascontiguousarray(active, dtype=np.int64).reshape(-1)
+        if idx.size and (idx.min() < 0 or idx.max() >= n):
+            raise ValueError("active index out of range")
+        idx = idx.astype(np.uint32)
+        self._ck(lib().gx_gravity_active_cached(self._h, n, _ptr(pos), _ptr(m), idx.size, _ptr(idx), _ptr(out)))
         return out
 
 

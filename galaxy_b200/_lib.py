@@ -121,6 +121,8 @@ SIGNATURES = {
     "gx_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_accelerations_device": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_accelerations_active": (_i, [_vp, _sz, _vp, _vp, _sz, _vp, _vp]),
+    "gx_rebuild_gravity_cache": (_i, [_vp, _sz, _vp, _vp]),
+    "gx_gravity_active_cached": (_i, [_vp, _sz, _vp, _vp, _sz, _vp, _vp]),
     "gx_potential_energy": (_i, [_vp, _sz, _vp, _vp, C.POINTER(_d)]),
     "gx_direct_sum_f64": (_i, [_vp, _sz, _vp, _vp, _sz, _vp, _vp]),
     "gx_upload": (_i, [_vp, _sz, _vp, _vp, _vp]),

@@ -132,6 +132,42 @@ __global__ void __launch_bounds__(kActThreads) k_gather_acc(const double* __rest
   }
 }
 
+// Stale-tree walk: the leaves take the current positions (and masses, where the leaf
+// had mass when the tree was built, so every skip decision stays the build's): the
+// sorted leaf records and each leaf's half of its parent's pair record. Internal nodes
+// keep the aggregates and thresholds of the build.
+__global__ void __launch_bounds__(kActThreads) k_refresh_leaves(uint32_t n, const uint32_t* __restrict__ order,
+                                                                const double* __restrict__ pos,
+                                                                const double* __restrict__ mass,
+                                                                const uint32_t* __restrict__ parent,
+                                                                const uint2* __restrict__ kids, double4* leaf64,
+                                                                float* __restrict__ pairs) {
+  for (uint32_t k = blockIdx.x * kActThreads + threadIdx.x; k < n; k += gridDim.x * kActThreads) {
+    const uint32_t o = order[k];
+    if (o >= n) continue;
+    const double frozen = leaf64[k].w;
+    const double m = frozen > 0.0 ? mass[o] : frozen;
+    const double4 x = make_double4(pos[3 * (size_t)o], pos[3 * (size_t)o + 1], pos[3 * (size_t)o + 2], m);
+    leaf64[k] = x;
+    const uint32_t p = parent[k];
+    if (p < n || p >= 2 * n - 1) continue;  // the root leaf of a one-particle system
+    const uint32_t gi = p - n;
+    const int side = kids[gi].x == k ? 0 : 1;  // left fields are .x/.z, right .y/.w
+    float hx, lx, hy, ly, hz, lz;
+    split_ff(x.x, hx, lx);
+    split_ff(x.y, hy, ly);
+    split_ff(x.z, hz, lz);
+    float* rec = pairs + 20 * (size_t)gi;  // 5 float4
+    rec[0 + side] = hx;
+    rec[2 + side] = hy;
+    rec[4 + side] = hz;
+    rec[6 + side] = __double2float_rn(m);
+    rec[8 + side] = lx;
+    rec[10 + side] = ly;
+    rec[12 + side] = lz;
+  }
+}
+
 uint32_t grid_for(uint32_t n) { return std::max(1u, std::min((n + kActThreads - 1) / kActThreads, 148u * 16u)); }
 
 }  // namespace
@@ -150,6 +186,11 @@ void launch_active_targets(const StepBufs& b, const uint32_t* active, uint32_t n
   k_chunk_count<<<nchunks, kActThreads, 0, st>>>(n, flags, chunk_counts);
   k_scan_counts<<<1, kActThreads, 0, st>>>(nchunks, chunk_counts, count_out);
   k_chunk_write<<<nchunks, kActThreads, 0, st>>>(n, flags, chunk_counts, list, group, items);
+}
+
+void launch_refresh_leaves(const StepBufs& b, cudaStream_t st) {
+  k_refresh_leaves<<<grid_for(b.n), kActThreads, 0, st>>>(b.n, b.order, b.pos, b.mass, b.parent, b.kids, b.leaf64,
+                                                          reinterpret_cast<float*>(b.pairs));
 }
 
 void launch_gather_acc(const double* acc, const uint32_t* active, uint32_t n_active, double* out, cudaStream_t st) {

@@ -164,7 +164,7 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   const size_t z_bbox = 6 * ns * sizeof(unsigned long long);
   const size_t z_hist = ns * kMaxRadixPasses * kRadixBins * sizeof(uint32_t);
   const size_t z_stat = (size_t)kMaxRadixPasses * nt * kRadixBins * sizeof(uint32_t);
-  const size_t z_ctr = 16 * sizeof(uint32_t);
+  const size_t z_ctr = kCounterWords * sizeof(uint32_t);
   char* z = nullptr;
   GX_A(z, z_bbox + z_hist + z_stat + z_ctr, char);
   b.bbox_enc = reinterpret_cast<unsigned long long*>(z);
@@ -283,6 +283,9 @@ struct gx_handle {
   bool pending_kick = false;
   uint64_t launches = 0;
   gx_stats stats{};
+  // every tree build bumps tree_gen; the stale-tree cache is valid while it holds
+  uint64_t tree_gen = 0, cache_gen = ~0ull;
+  size_t cache_n = 0;
   // active-subset walk (gx_accelerations_active): buffers grown on demand
   struct Active {
     uint32_t* active = nullptr;  // the caller's active indices
@@ -355,7 +358,7 @@ int layout(gx_handle* h, size_t n, double dt) {
   b.ntiles = static_cast<uint32_t>(tiles.size());
   b.nitems = static_cast<uint32_t>(items.size());
   // The per-step zero region: bbox words, histograms, look-back status, counters.
-  b.zero_bytes = reinterpret_cast<char*>(b.counters) - reinterpret_cast<char*>(b.zero_begin) + 16 * sizeof(uint32_t);
+  b.zero_bytes = reinterpret_cast<char*>(b.counters) - reinterpret_cast<char*>(b.zero_begin) + kCounterWords * sizeof(uint32_t);
   GX_CK(h, cudaMemcpyAsync(h->ar.sys_rw, sys.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, h->stream));
   GX_CK(h, cudaMemcpyAsync(h->ar.tiles_rw, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice,
                            h->stream));
@@ -374,6 +377,7 @@ int layout(gx_handle* h, size_t n, double dt) {
 // Enqueue bbox (+kick/drift) -> Morton -> sort -> build on b.
 void enqueue_tree(gx_handle* h, const StepBufs& b, int kick, int pending, bool timed) {
   cudaStream_t st = h->stream;
+  ++h->tree_gen;
   if (timed) cudaEventRecord(h->ev[0], st);
   cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, st);
   launch_kick_drift_bbox(b, kick, pending, st);
@@ -603,31 +607,14 @@ int gx_accelerations_device(gx_handle* h, size_t n, const double* d_pos, const d
   return GX_OK;
 }
 
-int gx_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
-                            const uint32_t* active, double* acc_out) {
-  if (!h) return GX_ERR_INVALID_ARG;
-  if (n == 0 || n_active == 0) return GX_OK;
-  if (!pos || !mass || !active || !acc_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
-  if (n_active > (size_t{1} << 31)) return fail(h, GX_ERR_INVALID_ARG, "too many active indices");
-  for (size_t i = 0; i < n_active; ++i)
-    if (active[i] >= n) return fail(h, GX_ERR_INVALID_ARG, "active index out of range");
-  if (n == 1) {
-    acc_out[0] = acc_out[1] = acc_out[2] = 0.0;  // a lone particle feels no force
-    return GX_OK;
-  }
-  cudaSetDevice(h->device);
-  h->resident = false;  // shares the arena with the resident state
-  int rc = layout(h, n, 0.0);
-  if (rc) return rc;
-  GX_CK(h, ensure_active(h, n, n_active));
+namespace {
+
+// The active targets' walk on the tree in the arena (fresh or cached): list, walk,
+// gather, copy back, scatter into acc_out.
+int walk_active(gx_handle* h, size_t n, size_t n_active, const uint32_t* active, double* acc_out, bool timed) {
   StepBufs& b = h->ar.b;
   auto& a = h->act;
   const uint32_t na = static_cast<uint32_t>(n_active);
-  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  GX_CK(h, cudaMemcpyAsync(a.active, active, n_active * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
-  const bool timed = stats_on(h);
-  enqueue_tree(h, b, 0, 0, timed);
   uint32_t* count = a.chunks + active_chunk_count(static_cast<uint32_t>(n)) + 1;
   // Targets per warp: a sparse subset spreads 32 consecutive active targets over a wide
   // region (a large union walk), so fewer lanes take part the sparser it is. Thresholds
@@ -650,11 +637,91 @@ int gx_accelerations_active(gx_handle* h, size_t n, const double* pos, const dou
   std::vector<double> got(3 * n_active);
   GX_CK(h, cudaMemcpyAsync(got.data(), a.out, 3 * n_active * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   h->stats.n = n;
-  rc = finish(h, timed);
+  const int rc = finish(h, timed);
   if (rc) return rc;
   for (size_t i = 0; i < n_active; ++i)
     for (int c = 0; c < 3; ++c) acc_out[3 * (size_t)active[i] + c] = got[3 * i + c];
   return GX_OK;
+}
+
+int check_active(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
+                 const uint32_t* active, double* acc_out) {
+  if (!pos || !mass || !active || !acc_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  if (n_active > (size_t{1} << 31)) return fail(h, GX_ERR_INVALID_ARG, "too many active indices");
+  for (size_t i = 0; i < n_active; ++i)
+    if (active[i] >= n) return fail(h, GX_ERR_INVALID_ARG, "active index out of range");
+  return GX_OK;
+}
+
+}  // namespace
+
+int gx_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
+                            const uint32_t* active, double* acc_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n == 0 || n_active == 0) return GX_OK;
+  int rc = check_active(h, n, pos, mass, n_active, active, acc_out);
+  if (rc) return rc;
+  if (n == 1) {
+    acc_out[0] = acc_out[1] = acc_out[2] = 0.0;  // a lone particle feels no force
+    return GX_OK;
+  }
+  cudaSetDevice(h->device);
+  h->resident = false;  // shares the arena with the resident state
+  rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  GX_CK(h, ensure_active(h, n, n_active));
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->act.active, active, n_active * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  const bool timed = stats_on(h);
+  enqueue_tree(h, b, 0, 0, timed);
+  return walk_active(h, n, n_active, active, acc_out, timed);
+}
+
+int gx_rebuild_gravity_cache(gx_handle* h, size_t n, const double* pos, const double* mass) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  h->cache_gen = ~0ull;
+  h->cache_n = n;
+  if (n < 2) return GX_OK;  // nothing to cache: the walks of 0 or 1 particle are trivial
+  if (!pos || !mass) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  cudaSetDevice(h->device);
+  h->resident = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  enqueue_tree(h, b, 0, 0, false);
+  rc = finish(h, false);
+  if (rc) return rc;
+  h->cache_gen = h->tree_gen;
+  return GX_OK;
+}
+
+int gx_gravity_active_cached(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
+                             const uint32_t* active, double* acc_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n != h->cache_n) return fail(h, GX_ERR_STATE, "no cached tree for this many particles");
+  if (n == 0 || n_active == 0) return GX_OK;
+  int rc = check_active(h, n, pos, mass, n_active, active, acc_out);
+  if (rc) return rc;
+  if (n == 1) {
+    acc_out[0] = acc_out[1] = acc_out[2] = 0.0;
+    return GX_OK;
+  }
+  if (h->cache_gen != h->tree_gen)
+    return fail(h, GX_ERR_STATE, "the cached tree was replaced: call gx_rebuild_gravity_cache");
+  cudaSetDevice(h->device);
+  GX_CK(h, ensure_active(h, n, n_active));
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h->act.active, active, n_active * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+  // the walk's own per-step counters start at zero (the tree is not rebuilt)
+  GX_CK(h, cudaMemsetAsync(b.counters, 0, kCounterWords * sizeof(uint32_t), h->stream));
+  launch_refresh_leaves(b, h->stream);
+  return walk_active(h, n, n_active, active, acc_out, false);
 }
 
 int gx_synchronize(gx_handle* h) {

@@ -118,7 +118,7 @@ int upload_tables(gx_batch* bt, const std::vector<size_t>& which, bool* inside) 
   b.nsys = static_cast<uint32_t>(sys.size());
   b.ntiles = static_cast<uint32_t>(tiles.size());
   b.nitems = static_cast<uint32_t>(items.size());
-  b.zero_bytes = reinterpret_cast<char*>(b.counters) - reinterpret_cast<char*>(b.zero_begin) + 16 * sizeof(uint32_t);
+  b.zero_bytes = reinterpret_cast<char*>(b.counters) - reinterpret_cast<char*>(b.zero_begin) + kCounterWords * sizeof(uint32_t);
   GB_CK(bt, cudaMemcpyAsync(bt->ar.sys_rw, sys.data(), sys.size() * sizeof(SysDesc), cudaMemcpyHostToDevice,
                             bt->stream));
   GB_CK(bt, cudaMemcpyAsync(bt->ar.tiles_rw, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice,

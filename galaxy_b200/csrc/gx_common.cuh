@@ -87,7 +87,8 @@ constexpr int kMaxRadixPasses = 8;  // histogram / look-back arrays are sized fo
 // Slot of the per-step counters that the persistent walk steals items from; slots
 // [0, kMaxRadixPasses) are the sort passes' tile counters.
 constexpr int kWalkItemCounter = kMaxRadixPasses;
-static_assert(kWalkItemCounter < 16, "the per-step counter block holds 16 words");
+constexpr int kCounterWords = 16;  // per-step counter block (zeroed with the step's scratch)
+static_assert(kWalkItemCounter < kCounterWords, "the walk's counter is in the block");
 // Tree depth bound: the augmented key is (code, 32-bit position), so a root-to-leaf path
 // has at most 30 + 32 (30-bit codes) or 63 + 32 (63-bit codes) internal levels.
 constexpr int kMaxDepth = 100;

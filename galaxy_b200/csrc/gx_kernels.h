@@ -97,6 +97,9 @@ void launch_active_targets(const StepBufs& b, const uint32_t* active, uint32_t n
                            uint32_t* inv, uint32_t* flags, uint32_t* chunk_counts, uint32_t* list,
                            uint32_t* count_out, WalkItem* items, cudaStream_t st);
 size_t active_chunk_count(uint32_t n);
+// Stale-tree walk: leaf records and the leaves' halves of the pair records take the
+// current pos / mass (single system); internal nodes keep the build's aggregates.
+void launch_refresh_leaves(const StepBufs& b, cudaStream_t st);
 // out[3i + c] = acc[3 active[i] + c]
 void launch_gather_acc(const double* acc, const uint32_t* active, uint32_t n_active, double* out, cudaStream_t st);
 // Blocks of cfg.block threads of the selected walk kernel resident on one SM.

@@ -109,6 +109,19 @@ int gx_accelerations_device(gx_handle* h, size_t n, const double* d_pos, const d
  * particles are left as they are. Indices >= n are GX_ERR_INVALID_ARG; repeats are allowed. */
 int gx_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
                             const uint32_t* active, double* acc_out);
+/* The stale-tree active walk of TreeGravity (solvers/src/barnes_hut.rs:647-711: its
+ * rebuild_gravity_cache and gravity_active_cached) over this LBVH, for individual time
+ * steps. gx_rebuild_gravity_cache builds the tree of (pos, mass) and keeps it: topology,
+ * internal-node aggregates and thresholds, and which leaves are massless.
+ * gx_gravity_active_cached then walks that tree for the active targets at the CURRENT
+ * positions: targets and leaf sources take pos / mass given here, internal nodes keep the
+ * cached aggregates (the reference's "only far cell COMs are stale"). With unchanged
+ * positions the result equals gx_accelerations_active. Any other force call or step on
+ * the handle replaces the cached tree (GX_ERR_STATE until the next rebuild); n must equal
+ * the cached n. */
+int gx_rebuild_gravity_cache(gx_handle* h, size_t n, const double* pos, const double* mass);
+int gx_gravity_active_cached(gx_handle* h, size_t n, const double* pos, const double* mass, size_t n_active,
+                             const uint32_t* active, double* acc_out);
 /* ForceSolver::potential_energy -- gpu/src/gpu_lbvh_fused.rs:140-146 delegating to
  * solvers/src/potential.rs:51-58: the exact O(N^2) softened potential, here an FP64
  * GPU reduction. */

@@ -692,6 +692,24 @@ int or_lbvh_accelerations_subset(size_t n, const double* pos, const double* mass
   return 0;
 }
 
+// Stale-tree active walk, as TreeGravity::gravity_active_cached
+// (solvers/src/barnes_hut.rs:683-710) does over its cached FlatTree, here over the
+// LBVH: the tree (topology, cell aggregates, leaf skip flags) is built from
+// (pos_build, mass_build); each target is walked at its current position and leaf
+// sources are read from (pos_now, mass_now) -- lbvh_accel reads targets and bodies
+// from the arrays it is given, so passing the current ones is exactly that.
+int or_lbvh_accelerations_stale(size_t n, const double* pos_build, const double* mass_build, const double* pos_now,
+                                const double* mass_now, double g, double softening, double theta, size_t n_targets,
+                                const uint32_t* targets, double* acc_out, int threads) {
+  if (n == 0) return 0;
+  Flat f = lbvh_build(pos_build, mass_build, n);
+  const double eps2 = softening * softening;
+#pragma omp parallel for num_threads(threads > 1 ? threads : 1) schedule(dynamic, 64)
+  for (long long k = 0; k < static_cast<long long>(n_targets); ++k)
+    store3(acc_out, k, lbvh_accel(f, targets[k], pos_now, mass_now, theta, eps2, nullptr) * g);
+  return 0;
+}
+
 // Quadrupole walk (extension): identical decisions to the monopole walk; on
 // accept the softened quadrupole correction is added to the monopole term.
 int or_lbvh_accelerations_quad(size_t n, const double* pos, const double* mass, double g, double softening,

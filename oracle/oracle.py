@@ -53,6 +53,7 @@ def lib():
             "or_lbvh_flat": (i, [sz, _f64p, _f64p, _f64p, _u32p, _u32p]),
             "or_lbvh_accelerations": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i, C.c_void_p]),
             "or_lbvh_accelerations_subset": (i, [sz, _f64p, _f64p, d, d, d, sz, _u32p, _f64p, i]),
+            "or_lbvh_accelerations_stale": (i, [sz, _f64p, _f64p, _f64p, _f64p, d, d, d, sz, _u32p, _f64p, i]),
             "or_lbvh_accelerations_k63": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i, C.c_void_p]),
             "or_lbvh_accelerations_quad": (i, [sz, _f64p, _f64p, d, d, d, _f64p, i]),
             "or_direct_sum": (None, [sz, _f64p, _f64p, d, d, _f64p]),
@@ -194,6 +195,19 @@ def lbvh_accelerations_subset(pos, mass, g, softening, theta, targets, threads: 
     acc = np.zeros((t.shape[0], 3))
     lib().or_lbvh_accelerations_subset(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64), g,
                                        softening, theta, t.shape[0], t, acc.reshape(-1), threads)
+    return acc
+
+
+def lbvh_accelerations_stale(pos_build, mass_build, pos_now, mass_now, g, softening, theta, targets,
+                             threads: int = 1):
+    """Stale-tree walk (TreeGravity::gravity_active_cached semantics over the LBVH):
+    the tree of (pos_build, mass_build), targets and leaf sources at (pos_now, mass_now)."""
+    pb, pn = _pos(pos_build), _pos(pos_now)
+    t = np.ascontiguousarray(targets, dtype=np.uint32)
+    acc = np.zeros((t.shape[0], 3))
+    lib().or_lbvh_accelerations_stale(pb.shape[0], pb.reshape(-1), np.ascontiguousarray(mass_build, np.float64),
+                                      pn.reshape(-1), np.ascontiguousarray(mass_now, np.float64), g, softening,
+                                      theta, t.shape[0], t, acc.reshape(-1), threads)
     return acc
 
 

@@ -195,3 +195,22 @@ def test_potential_parallel_matches_serial(oracle):
     s = oracle.potential_serial(pos, mass, G, EPS)
     p = oracle.potential_parallel(pos, mass, G, EPS, threads=4)
     assert abs(p - s) <= 1e-9 * abs(s)
+
+
+def test_stale_tree_walk_fresh_equals_full_and_converges(oracle):
+    """The stale-tree walk (TreeGravity::gravity_active_cached semantics over the LBVH)
+    equals the full pass on a fresh tree, and approaches the fresh pass as the drift
+    since the tree was built shrinks."""
+    pos, _, mass = oracle.fixture_cluster(21, 600)
+    full = oracle.lbvh_accelerations(pos, mass, 1.0, 0.05, 0.5)
+    t = np.arange(600, dtype=np.uint32)
+    assert np.array_equal(oracle.lbvh_accelerations_stale(pos, mass, pos, mass, 1.0, 0.05, 0.5, t), full)
+    rng = np.random.default_rng(4)
+    step = rng.normal(0.0, 1.0, pos.shape)
+    errs = []
+    for h in (1e-2, 1e-3, 1e-4):
+        moved = pos + h * step
+        stale = oracle.lbvh_accelerations_stale(pos, mass, moved, mass, 1.0, 0.05, 0.5, t)
+        fresh = oracle.lbvh_accelerations(moved, mass, 1.0, 0.05, 0.5)
+        errs.append(float(np.max(np.linalg.norm(stale - fresh, axis=1) / np.linalg.norm(fresh, axis=1))))
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-2
