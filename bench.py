@@ -384,6 +384,11 @@ def run_serving(args):
     reqs = workloads.request_stream(args.requests, rate=50.0, seed=rank)
     specs = [r.spec() for r in reqs]  # generated before the clock starts
     srv = gb.Server(budget_bytes=150 << 30, device=local, morton63=args.morton63)
+    snap_dir = None
+    if args.snapshot_every:
+        import tempfile
+
+        snap_dir = tempfile.mkdtemp(prefix="glxysnap_")
     clocks = ClockSampler(local)
     clocks.start()
     t0 = time.perf_counter()
@@ -392,7 +397,12 @@ def run_serving(args):
         delay = r.arrival - (time.perf_counter() - t0)
         if delay > 0:
             time.sleep(delay)
-        rids.append(srv.submit(sp.state, sp.g, sp.eps, sp.theta, sp.dt, r.steps))
+        if args.snapshot_every:
+            rids.append(srv.submit(sp.state, sp.g, sp.eps, sp.theta, sp.dt, r.steps,
+                                   snapshot_every=args.snapshot_every,
+                                   snapshot_prefix=os.path.join(snap_dir, f"req{r.rid}"), rng_seed=r.seed))
+        else:
+            rids.append(srv.submit(sp.state, sp.g, sp.eps, sp.theta, sp.dt, r.steps))
     deadline = t0 + args.horizon
     for rid in rids:
         left = deadline - time.perf_counter()
@@ -405,7 +415,12 @@ def run_serving(args):
     wall = time.perf_counter() - t0
     st = srv.stats()
     clk = clocks.stop()
+    snaps = sum(srv.snapshots_written(rid) for rid in rids) if args.snapshot_every else 0
     srv.close()
+    if snap_dir:
+        import shutil
+
+        shutil.rmtree(snap_dir, ignore_errors=True)
     if rank == 0:
         line = {"metric": "particle-steps/s at theta=0.5, served (continuous batching)",
                 "value": st["particle_steps_per_s_device"], "unit": "particle-steps/s", "n_gpus": ws,
@@ -413,7 +428,8 @@ def run_serving(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"serving-{args.requests}-requests", "rate_per_s": 50.0,
                            "n_range": [16384, 2097152], "steps_range": [100, 1000], "budget_gb": 150,
-                           "horizon_s": args.horizon},
+                           "horizon_s": args.horizon, "snapshot_every": args.snapshot_every},
+                "snapshots_written": snaps,
                 "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],
                 "wall_particle_steps_per_s": st["particle_steps"] / wall, "completed": st["completed"],
                 "submitted": len(rids), "max_live": st["max_live"], "queue_s_p50": st["queue_s_p50"],
@@ -510,6 +526,7 @@ def main():
     ap.add_argument("--morton63", action="store_true", help="batched/serving: 63-bit Morton keys")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=100, help="precision: horizon of the FP64 run")
+    ap.add_argument("--snapshot-every", type=int, default=0, help="serving: emit GLXYSNAP v4 files every K steps")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

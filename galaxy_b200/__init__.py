@@ -500,12 +500,31 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, state: State, g: float, softening: float, theta: float, dt: float, steps: int) -> int:
+    def submit(self, state: State, g: float, softening: float, theta: float, dt: float, steps: int,
+               snapshot_every: int = 0, snapshot_prefix: str | None = None, rng_seed: int = 0, config_hash: int = 0,
+               units: str | None = None) -> int:
+        """Queue a scenario. With snapshot_every > 0 a GLXYSNAP v4 file
+        "<snapshot_prefix>.<step:08d>.glxysnap" is emitted every that many steps and
+        after the last (see gx_server_submit_snapshots)."""
         rid = C.c_uint64()
-        self._ck(lib().gx_server_submit(self._s, len(state), _ptr(state.pos), _ptr(state.vel), _ptr(state.mass), g,
-                                        softening, theta, dt, int(steps), C.byref(rid)))
+        if snapshot_every:
+            if not snapshot_prefix:
+                raise ValueError("snapshot_prefix is required with snapshot_every")
+            o = _lib.SnapOpts(C.sizeof(_lib.SnapOpts), int(snapshot_every), snapshot_prefix.encode(), int(rng_seed),
+                              int(config_hash), units.encode() if units else None)
+            self._ck(lib().gx_server_submit_snapshots(self._s, len(state), _ptr(state.pos), _ptr(state.vel),
+                                                      _ptr(state.mass), g, softening, theta, dt, int(steps),
+                                                      C.byref(o), C.byref(rid)))
+        else:
+            self._ck(lib().gx_server_submit(self._s, len(state), _ptr(state.pos), _ptr(state.vel),
+                                            _ptr(state.mass), g, softening, theta, dt, int(steps), C.byref(rid)))
         self._n[rid.value] = (len(state), state.mass.copy())
         return rid.value
+
+    def snapshots_written(self, rid: int) -> int:
+        v = C.c_uint64()
+        self._ck(lib().gx_server_snapshots_written(self._s, rid, C.byref(v)))
+        return v.value
 
     def status(self, rid: int):
         st, done = C.c_int(), C.c_uint64()

@@ -88,6 +88,17 @@ class BatchStats(C.Structure):
     ]
 
 
+class SnapOpts(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("every", C.c_uint64),
+        ("path_prefix", C.c_char_p),
+        ("rng_seed", C.c_uint64),
+        ("config_hash", C.c_uint64),
+        ("units", C.c_char_p),
+    ]
+
+
 class ServerStats(C.Structure):
     _fields_ = [
         ("steps", C.c_uint64),
@@ -167,6 +178,10 @@ SIGNATURES = {
     "gx_server_wait": (_i, [_vp, _u64, _d]),
     "gx_server_result": (_i, [_vp, _u64, _vp, _vp, C.POINTER(_d)]),
     "gx_server_release": (_i, [_vp, _u64]),
+    "gx_server_submit_snapshots": (_i, [_vp, _sz, _vp, _vp, _vp, _d, _d, _d, _d, _u64, C.POINTER(SnapOpts),
+                                        C.POINTER(_u64)]),
+    "gx_server_snapshots_written": (_i, [_vp, _u64, C.POINTER(_u64)]),
+    "gx_glxysnap_write": (_i, [C.c_char_p, _d, _u64, _d, _u64, _u64, C.c_char_p, _sz, _vp, _vp, _vp]),
     "gx_server_stats_get": (_i, [_vp, C.POINTER(ServerStats)]),
     "gx_ic_plummer": (_i, [_sz, _u64, _d, _d, _d, _vp, _vp, _vp]),
     "gx_ic_collision": (_i, [_sz, _u64, _d, _d, _d, _d, _vp, _vp, _vp]),

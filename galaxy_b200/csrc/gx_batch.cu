@@ -15,6 +15,7 @@
 #include "../../include/galaxy_b200.h"
 #include "gx_kernels.h"
 #include "gx_runtime.h"
+#include "gx_snapshot.h"
 
 using namespace gx;
 
@@ -196,6 +197,61 @@ size_t index_of(const gx_batch* bt, uint64_t id) {
 }
 
 }  // namespace
+
+namespace gx {
+
+namespace {
+
+// One system's snapshot columns: pos, vel (+ the owed closing half kick v + a (0.5 dt),
+// one rounding each, as gx_system_snapshot), mass as f32 (round to nearest).
+__global__ void k_stage_snapshot(uint32_t off, uint32_t n, const double* __restrict__ pos,
+                                 const double* __restrict__ vel, const double* __restrict__ acc,
+                                 const double* __restrict__ mass, int pending, double dt, double* __restrict__ out) {
+  const double h = dmul(0.5, dt);
+  double* o_pos = out;
+  double* o_vel = out + 3 * (size_t)n;
+  float* o_mass = reinterpret_cast<float*>(out + 6 * (size_t)n);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const size_t g = (size_t)off + i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o_pos[3 * (size_t)i + c] = pos[3 * g + c];
+      double v = vel[3 * g + c];
+      if (pending) v = dadd(v, dmul(acc[3 * g + c], h));
+      o_vel[3 * (size_t)i + c] = v;
+    }
+    o_mass[i] = __double2float_rn(mass[g]);
+  }
+}
+
+}  // namespace
+
+int batch_stage_snapshot(gx_batch* bt, uint64_t id, void* d_stage, void* host_dst, cudaStream_t copy_stream,
+                         cudaEvent_t copied, double* time_out, size_t* n_out) {
+  if (!bt || !d_stage || !host_dst) return GX_ERR_INVALID_ARG;
+  const size_t i = index_of(bt, id);
+  if (i == SIZE_MAX) return bfail(bt, GX_ERR_NOT_FOUND, "unknown system id");
+  cudaSetDevice(bt->device);
+  const BatchSys& s = bt->systems[i];
+  const StepBufs& b = bt->ar.b;
+  const uint32_t grid = std::max(1u, std::min((s.n + 255u) / 256u, 148u * 8u));
+  k_stage_snapshot<<<grid, 256, 0, bt->stream>>>(s.off, s.n, b.pos, b.vel, b.acc, b.mass, s.pending ? 1 : 0, s.dt,
+                                                 static_cast<double*>(d_stage));
+  GB_CK(bt, cudaGetLastError());
+  cudaEvent_t staged = nullptr;
+  GB_CK(bt, cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(staged, bt->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(copy_stream, staged, 0);
+  cudaEventDestroy(staged);  // released once the recorded work completes
+  GB_CK(bt, e);
+  GB_CK(bt, cudaMemcpyAsync(host_dst, d_stage, snapshot_stage_bytes(s.n), cudaMemcpyDeviceToHost, copy_stream));
+  GB_CK(bt, cudaEventRecord(copied, copy_stream));
+  if (time_out) *time_out = s.time;
+  if (n_out) *n_out = s.n;
+  return GX_OK;
+}
+
+}  // namespace gx
 
 extern "C" {
 

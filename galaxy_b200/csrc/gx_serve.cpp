@@ -24,7 +24,10 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cuda_runtime_api.h>
+
 #include "../../include/galaxy_b200.h"
+#include "gx_snapshot.h"
 
 namespace {
 
@@ -40,7 +43,33 @@ struct Req {
   int status = GX_REQ_QUEUED;
   Clock::time_point t_submit, t_admit, t_done;
   double time_out = 0.0;
+  // snapshot emission (gx_server_submit_snapshots): one file per `snap_every` steps and
+  // after the last, staged on the device and written by the server's writer thread
+  uint64_t snap_every = 0;
+  std::string snap_prefix;
+  gx::SnapHeader snap_hdr;
+  void* d_stage = nullptr;  // device staging buffer
+  void* h_stage = nullptr;  // pinned copy the writer reads
+  cudaEvent_t snap_ev = nullptr;
+  int snap_pending = 0;  // staged but not yet written (guarded by the server mutex)
+  uint64_t snaps_written = 0;
+  std::string snap_err;
 };
+
+struct SnapJob {
+  Req* r;
+  uint64_t step;
+  double time;
+  size_t n;
+};
+
+void free_snap(Req* r) {
+  if (r->d_stage) cudaFree(r->d_stage);
+  if (r->h_stage) cudaFreeHost(r->h_stage);
+  if (r->snap_ev) cudaEventDestroy(r->snap_ev);
+  r->d_stage = r->h_stage = nullptr;
+  r->snap_ev = nullptr;
+}
 
 double seconds(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); }
 
@@ -73,9 +102,75 @@ struct gx_server {
   uint64_t particle_steps = 0, steps = 0, completed = 0, max_live = 0;
   double busy_s = 0.0;
   Clock::time_point t_start;
+  // snapshot emission
+  int device = 0;
+  cudaStream_t copy_stream = nullptr;
+  std::thread writer;
+  std::deque<SnapJob> jobs;
+  std::condition_variable cv_jobs;
+  bool writer_stop = false, writer_started = false;
 };
 
 namespace {
+
+// Writes staged snapshots as their copies complete (FIFO), outside the server mutex.
+void writer_loop(gx_server* s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    SnapJob j{};
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_jobs.wait(lk, [&] { return s->writer_stop || !s->jobs.empty(); });
+      if (s->jobs.empty()) return;
+      j = s->jobs.front();
+      s->jobs.pop_front();
+    }
+    const cudaError_t e = cudaEventSynchronize(j.r->snap_ev);
+    gx::SnapHeader h = j.r->snap_hdr;
+    h.time = j.time;
+    h.step = j.step;
+    char suffix[48];
+    std::snprintf(suffix, sizeof suffix, ".%08llu.glxysnap", static_cast<unsigned long long>(j.step));
+    std::string err = e == cudaSuccess ? "" : cudaGetErrorString(e);
+    const bool ok = e == cudaSuccess && gx::write_glxysnap_staged(j.r->snap_prefix + suffix, h, j.n, j.r->h_stage, err);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      j.r->snap_pending -= 1;
+      if (ok)
+        j.r->snaps_written += 1;
+      else
+        j.r->snap_err = err;
+    }
+    s->cv_done.notify_all();
+  }
+}
+
+// Stage request r's snapshot at its current step (called by the stepping thread with
+// the server mutex held in lk).
+void stage_snapshot(gx_server* s, Req* r, std::unique_lock<std::mutex>& lk) {
+  if (!r->d_stage) {
+    const size_t bytes = gx::snapshot_stage_bytes(r->n);
+    if (cudaMalloc(&r->d_stage, bytes) != cudaSuccess || cudaHostAlloc(&r->h_stage, bytes, 0) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->snap_ev, cudaEventDisableTiming) != cudaSuccess) {
+      free_snap(r);
+      r->snap_err = "cannot allocate the snapshot buffers";
+      r->snap_every = 0;
+      return;
+    }
+  }
+  // the previous snapshot of r must be written before its buffer is reused
+  s->cv_done.wait(lk, [&] { return r->snap_pending == 0; });
+  double t = 0.0;
+  size_t n = 0;
+  const int rc = gx::batch_stage_snapshot(s->batch, r->sys, r->d_stage, r->h_stage, s->copy_stream, r->snap_ev, &t, &n);
+  if (rc != GX_OK) {
+    r->snap_err = gx_batch_last_error(s->batch);
+    return;
+  }
+  r->snap_pending += 1;
+  s->jobs.push_back(SnapJob{r, r->done, t, n});
+  s->cv_jobs.notify_one();
+}
 
 void run_loop(gx_server* s) {
   for (;;) {
@@ -124,7 +219,7 @@ void run_loop(gx_server* s) {
     const auto t1 = Clock::now();
     gx_batch_stats bs{};
     gx_batch_stats_get(s->batch, &bs);
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::unique_lock<std::mutex> lk(s->mu);
     if (rc != GX_OK) {
       s->loop_error = rc;
       s->err = gx_batch_last_error(s->batch);
@@ -139,7 +234,9 @@ void run_loop(gx_server* s) {
     std::vector<Req*> keep;
     for (Req* r : s->live) {
       s->particle_steps += r->n;
-      if (++r->done < r->steps) {
+      ++r->done;
+      if (r->snap_every && (r->done % r->snap_every == 0 || r->done == r->steps)) stage_snapshot(s, r, lk);
+      if (r->done < r->steps) {
         keep.push_back(r);
         continue;
       }
@@ -169,6 +266,14 @@ int gx_server_create(size_t budget_bytes, const gx_options* opt, gx_server** out
   gx_server* s = new gx_server();
   s->batch = b;
   s->t_start = Clock::now();
+  cudaGetDevice(&s->device);
+  if (cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    gx_batch_destroy(b);
+    delete s;
+    return GX_ERR_CUDA;
+  }
+  s->writer = std::thread(writer_loop, s);
+  s->writer_started = true;
   s->th = std::thread(run_loop, s);
   s->started = true;
   *out = s;
@@ -187,8 +292,18 @@ void gx_server_destroy(gx_server* s) {
   }
   s->cv.notify_all();
   if (s->started) s->th.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->writer_stop = true;  // the writer drains the staged snapshots first
+  }
+  s->cv_jobs.notify_all();
+  if (s->writer_started) s->writer.join();
   gx_batch_destroy(s->batch);
-  for (auto& kv : s->all) delete kv.second;
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+  for (auto& kv : s->all) {
+    free_snap(kv.second);
+    delete kv.second;
+  }
   delete s;
 }
 
@@ -196,6 +311,12 @@ const char* gx_server_last_error(const gx_server* s) { return s ? s->err.c_str()
 
 int gx_server_submit(gx_server* s, size_t n, const double* pos, const double* vel, const double* mass, double g,
                      double softening, double theta, double dt, uint64_t steps, uint64_t* rid_out) {
+  return gx_server_submit_snapshots(s, n, pos, vel, mass, g, softening, theta, dt, steps, nullptr, rid_out);
+}
+
+int gx_server_submit_snapshots(gx_server* s, size_t n, const double* pos, const double* vel, const double* mass,
+                               double g, double softening, double theta, double dt, uint64_t steps,
+                               const gx_snap_opts* snap, uint64_t* rid_out) {
   if (!s || !rid_out || n == 0 || !pos || !vel || !mass || steps == 0) return GX_ERR_INVALID_ARG;
   Req* r = new Req();
   r->n = n;
@@ -208,6 +329,18 @@ int gx_server_submit(gx_server* s, size_t n, const double* pos, const double* ve
   r->dt = dt;
   r->steps = steps;
   r->t_submit = Clock::now();
+  if (snap && snap->struct_size && snap->every) {
+    if (snap->struct_size < sizeof(gx_snap_opts) || !snap->path_prefix) {
+      delete r;
+      return GX_ERR_INVALID_ARG;
+    }
+    r->snap_every = snap->every;
+    r->snap_prefix = snap->path_prefix;
+    r->snap_hdr.softening = softening;
+    r->snap_hdr.rng_seed = snap->rng_seed;
+    r->snap_hdr.config_hash = snap->config_hash;
+    if (snap->units) r->snap_hdr.units = snap->units;
+  }
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) {
@@ -220,6 +353,19 @@ int gx_server_submit(gx_server* s, size_t n, const double* pos, const double* ve
     *rid_out = r->rid;
   }
   s->cv.notify_all();
+  return GX_OK;
+}
+
+int gx_server_snapshots_written(gx_server* s, uint64_t rid, uint64_t* written_out) {
+  if (!s || !written_out) return GX_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(rid);
+  if (it == s->all.end()) return GX_ERR_NOT_FOUND;
+  *written_out = it->second->snaps_written;
+  if (!it->second->snap_err.empty()) {
+    s->err = it->second->snap_err;
+    return GX_ERR_STATE;
+  }
   return GX_OK;
 }
 
@@ -240,7 +386,7 @@ int gx_server_wait(gx_server* s, uint64_t rid, double timeout_s) {
   if (it == s->all.end()) return GX_ERR_NOT_FOUND;
   Req* r = it->second;
   const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
-    return r->status == GX_REQ_DONE || r->status == GX_REQ_REJECTED;
+    return (r->status == GX_REQ_DONE || r->status == GX_REQ_REJECTED) && r->snap_pending == 0;
   });
   if (!ok) return GX_ERR_STATE;
   return r->status == GX_REQ_DONE ? GX_OK : GX_ERR_BUDGET;
@@ -265,6 +411,8 @@ int gx_server_release(gx_server* s, uint64_t rid) {
   auto it = s->all.find(rid);
   if (it == s->all.end()) return GX_ERR_NOT_FOUND;
   if (it->second->status != GX_REQ_DONE && it->second->status != GX_REQ_REJECTED) return GX_ERR_STATE;
+  if (it->second->snap_pending > 0) return GX_ERR_STATE;  // a snapshot is still being written
+  free_snap(it->second);
   delete it->second;
   s->all.erase(it);
   return GX_OK;

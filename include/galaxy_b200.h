@@ -303,6 +303,38 @@ int gx_server_result(gx_server* s, uint64_t rid, double* pos_out, double* vel_ou
 int gx_server_release(gx_server* s, uint64_t rid);
 int gx_server_stats_get(gx_server* s, gx_server_stats* out);
 
+/* ---- GLXYSNAP v4 snapshots (io/src/snapshot.rs:1-60 layout, :130-199 to_writer) ---
+ * Files readable by the reference's io::snapshot::read_file: header (time, step, scale
+ * factor 1, softening, n, rng seed, config hash, units, code version) and the SoA
+ * columns pos, vel (f64), mass (f32), then the columns the gravity path does not evolve
+ * at the reference State's defaults: id = index, progenitor 0, kind collisionless,
+ * u = 0, formation time -inf. */
+int gx_glxysnap_write(const char* path, double time, uint64_t step, double softening, uint64_t rng_seed,
+                      uint64_t config_hash, const char* units, size_t n, const double* pos, const double* vel,
+                      const double* mass);
+
+/* Snapshot emission for a served scenario (the reference's snapshot cadence,
+ * sim/src/lib.rs:110-170, without a host round trip in the step loop): every `every`
+ * steps and after the last one, the system's state is staged on the device (velocities
+ * with the owed closing half kick, as gx_server_result), copied on a side stream while
+ * the batch steps on, and written by a server thread to
+ * "<path_prefix>.<step, 8 digits>.glxysnap". gx_server_wait returns once the request's
+ * files are written. */
+typedef struct gx_snap_opts {
+  uint32_t struct_size;     /* sizeof(gx_snap_opts) */
+  uint64_t every;           /* steps between snapshots; 0 = none */
+  const char* path_prefix;  /* copied at submit */
+  uint64_t rng_seed;        /* header fields */
+  uint64_t config_hash;
+  const char* units;        /* NULL: "nbody-G1" */
+} gx_snap_opts;
+int gx_server_submit_snapshots(gx_server* s, size_t n, const double* pos, const double* vel, const double* mass,
+                               double g, double softening, double theta, double dt, uint64_t steps,
+                               const gx_snap_opts* snap, uint64_t* rid_out);
+/* Snapshots written so far for a request; GX_ERR_STATE (text in gx_server_last_error)
+ * if one could not be written. */
+int gx_server_snapshots_written(gx_server* s, uint64_t rid, uint64_t* written_out);
+
 /* ---- seeded initial conditions (the reference's ic/ crate as input generator) -- */
 /* Plummer::sample (ic/src/plummer.rs:94-140): G, total mass M, scale radius a; seed. */
 int gx_ic_plummer(size_t n, uint64_t seed, double g, double total_mass, double scale_radius, double* pos,

@@ -88,3 +88,35 @@ def test_budget_admits_as_room_frees():
         got = srv.result(rid)
         ref = _alone(st, 0.01, 0.5, 1e-3, steps)
         assert np.array_equal(got.pos, ref.pos) and np.array_equal(got.vel, ref.vel)
+
+
+def test_snapshot_emission_matches_alone(tmp_path):
+    """Served scenarios emit GLXYSNAP v4 files every K steps and after the last; each file
+    holds the state the same system has at that step when stepped alone."""
+    from galaxy_b200 import snapshot as snap
+
+    reqs = [(gb.ic.plummer(5000 + 1000 * i, 400 + i), 12 + i) for i in range(3)]
+    srv = gb.Server()
+    rids = [srv.submit(st, 1.0, 0.01, 0.5, 1e-3, steps, snapshot_every=5, snapshot_prefix=str(tmp_path / f"r{k}"),
+                       rng_seed=k, config_hash=77)
+            for k, (st, steps) in enumerate(reqs)]
+    for rid in rids:
+        srv.wait(rid, 300)
+    for k, (rid, (st, steps)) in enumerate(zip(rids, reqs)):
+        marks = sorted({5, 10, steps})
+        assert srv.snapshots_written(rid) == len(marks)
+        r = gb.GpuResidentLeapfrog(1.0, 0.01, 0.5)
+        r.upload(st)
+        done = 0
+        for m in marks:
+            r.step_many(1e-3, m - done)
+            done = m
+            ref = r.snapshot()
+            h, c = snap.read(tmp_path / f"r{k}.{m:08d}.glxysnap")
+            assert (h["step"], h["n_particles"], h["softening"], h["rng_seed"], h["config_hash"]) == (
+                m, len(st), 0.01, k, 77)
+            assert abs(h["time"] - m * 1e-3) < 1e-15
+            assert np.array_equal(c["pos"], ref.pos) and np.array_equal(c["vel"], ref.vel)
+            assert np.array_equal(c["mass"], st.mass.astype(np.float32).astype(np.float64))
+        final = srv.result(rid)
+        assert np.array_equal(final.pos, ref.pos) and np.array_equal(final.vel, ref.vel)
