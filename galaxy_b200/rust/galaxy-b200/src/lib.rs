@@ -1,7 +1,9 @@
-//! `GpuLbvhB200` and `GpuResidentB200`: galaxy's gravity-solver interface over
-//! libgalaxy_b200 (a B200 LBVH Barnes-Hut). `GpuLbvhB200` implements `ForceSolver`
-//! (core/src/traits.rs) and drops in beside `Lbvh`, `BarnesHut` and `GpuLbvhFused`;
-//! `GpuResidentB200` mirrors `GpuResidentLeapfrog`'s upload / step_many / snapshot.
+//! `GpuLbvhB200`, `GpuStaleTreeB200` and `GpuResidentB200`: galaxy's gravity-solver
+//! interface over libgalaxy_b200 (a B200 LBVH Barnes-Hut). `GpuLbvhB200` implements
+//! `ForceSolver` (core/src/traits.rs) and drops in beside `Lbvh`, `BarnesHut` and
+//! `GpuLbvhFused`; `GpuStaleTreeB200` plays `TreeGravity`'s stale-tree role for individual
+//! time steps; `GpuResidentB200` mirrors `GpuResidentLeapfrog`'s upload / step_many /
+//! snapshot.
 //!
 //! Written against include/galaxy_b200.h; DVec3 is three f64 (`#[repr(C)]`-compatible
 //! in glam), so `&[DVec3]` is passed as `*const f64` with no copy.
@@ -42,6 +44,16 @@ extern "C" {
         acc: *mut f64,
     ) -> c_int;
     fn gx_potential_energy(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, out: *mut f64) -> c_int;
+    fn gx_rebuild_gravity_cache(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64) -> c_int;
+    fn gx_gravity_active_cached(
+        h: *mut GxHandle,
+        n: usize,
+        pos: *const f64,
+        mass: *const f64,
+        n_active: usize,
+        active: *const u32,
+        acc: *mut f64,
+    ) -> c_int;
     fn gx_upload(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64) -> c_int;
     fn gx_step_many(h: *mut GxHandle, dt: f64, steps: u64) -> c_int;
     fn gx_snapshot(h: *mut GxHandle, pos: *mut f64, vel: *mut f64) -> c_int;
@@ -132,6 +144,71 @@ impl ForceSolver for GpuLbvhB200 {
         let rc = unsafe { gx_potential_energy(self.h, state.len(), as_f64(&state.pos), state.mass.as_ptr(), &mut u) };
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
         u
+    }
+}
+
+/// The stale-tree active walk of `TreeGravity` (solvers/src/barnes_hut.rs:647-711) over the
+/// LBVH: `rebuild_gravity_cache` freezes the tree at the block-start state and
+/// `gravity_active_cached` walks it at the current positions (leaf sources current,
+/// internal aggregates frozen). Fresh passes run on a second handle and leave the cache.
+pub struct GpuStaleTreeB200 {
+    cache: *mut GxHandle,
+    fresh: GpuLbvhB200,
+    cached: bool,
+}
+
+impl GpuStaleTreeB200 {
+    pub fn new(g: f64, softening: f64, theta: f64, precision: u32) -> Result<Self, GxError> {
+        let fresh = GpuLbvhB200::new(g, softening, theta, precision)?;
+        let opt = GxOptions { struct_size: std::mem::size_of::<GxOptions>() as u32, precision, device: -1, ..Default::default() };
+        let mut h = std::ptr::null_mut();
+        let rc = unsafe { gx_create(g, softening, theta, &opt, &mut h) };
+        if rc != 0 {
+            return Err(err(std::ptr::null(), rc));
+        }
+        Ok(Self { cache: h, fresh, cached: false })
+    }
+}
+
+impl ForceSolver for GpuStaleTreeB200 {
+    fn accelerations(&mut self, state: &State, acc: &mut [DVec3]) {
+        self.fresh.accelerations(state, acc);
+    }
+
+    fn rebuild_gravity_cache(&mut self, state: &State) {
+        let rc = unsafe { gx_rebuild_gravity_cache(self.cache, state.len(), as_f64(&state.pos), state.mass.as_ptr()) };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.cache, rc));
+        self.cached = !state.is_empty(); // an empty state has no tree: later walks do nothing
+    }
+
+    fn gravity_active_cached(&mut self, state: &State, active: &[usize], acc: &mut [DVec3]) {
+        assert_eq!(acc.len(), state.len(), "acc length must match particle count");
+        if !self.cached {
+            return; // never rebuilt: nothing to walk, as TreeGravity
+        }
+        let idx: Vec<u32> = active.iter().map(|&i| u32::try_from(i).expect("active index fits u32")).collect();
+        let rc = unsafe {
+            gx_gravity_active_cached(
+                self.cache,
+                state.len(),
+                as_f64(&state.pos),
+                state.mass.as_ptr(),
+                idx.len(),
+                idx.as_ptr(),
+                acc.as_mut_ptr() as *mut f64,
+            )
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.cache, rc));
+    }
+
+    fn potential_energy(&self, state: &State) -> f64 {
+        self.fresh.potential_energy(state)
+    }
+}
+
+impl Drop for GpuStaleTreeB200 {
+    fn drop(&mut self) {
+        unsafe { gx_destroy(self.cache) }
     }
 }
 
