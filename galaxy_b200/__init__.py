@@ -475,7 +475,7 @@ class Server:
     from any thread; a native stepping thread admits them against the device budget,
     steps all live systems together and retires each after its steps."""
 
-    QUEUED, RUNNING, DONE, REJECTED = 0, 1, 2, 3
+    QUEUED, RUNNING, DONE, REJECTED, CANCELLED = 0, 1, 2, 3, 4
 
     def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, device=-1,
                  morton63=False):
@@ -520,6 +520,14 @@ class Server:
                                             _ptr(state.mass), g, softening, theta, dt, int(steps), C.byref(rid)))
         self._n[rid.value] = (len(state), state.mass.copy())
         return rid.value
+
+    def cancel(self, rid: int) -> None:
+        """gx_server_cancel: a queued request leaves the queue, a running one the batch."""
+        self._ck(lib().gx_server_cancel(self._s, rid))
+
+    def set_metrics_log(self, path: str | None) -> None:
+        """Append one JSON line per batched step to ``path`` (None stops)."""
+        self._ck(lib().gx_server_set_metrics_log(self._s, path.encode() if path else None))
 
     def snapshots_written(self, rid: int) -> int:
         v = C.c_uint64()

@@ -23,6 +23,7 @@ ERRORS = {
     -6: "GX_ERR_DEVICE_CHECK",
     -7: "GX_ERR_NOT_FOUND",
     -8: "GX_ERR_CAPACITY",
+    -9: "GX_ERR_CANCELLED",
 }
 
 ERRORS_BY_NAME = {v: k for k, v in ERRORS.items()}
@@ -181,6 +182,8 @@ SIGNATURES = {
     "gx_server_submit_snapshots": (_i, [_vp, _sz, _vp, _vp, _vp, _d, _d, _d, _d, _u64, C.POINTER(SnapOpts),
                                         C.POINTER(_u64)]),
     "gx_server_snapshots_written": (_i, [_vp, _u64, C.POINTER(_u64)]),
+    "gx_server_cancel": (_i, [_vp, _u64]),
+    "gx_server_set_metrics_log": (_i, [_vp, C.c_char_p]),
     "gx_glxysnap_write": (_i, [C.c_char_p, _d, _u64, _d, _u64, _u64, C.c_char_p, _sz, _vp, _vp, _vp]),
     "gx_server_stats_get": (_i, [_vp, C.POINTER(ServerStats)]),
     "gx_ic_plummer": (_i, [_sz, _u64, _d, _d, _d, _vp, _vp, _vp]),

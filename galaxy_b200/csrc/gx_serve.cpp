@@ -14,6 +14,7 @@
 // Because a batch steps each system with exactly the single-system arithmetic, a
 // request's result is bit-identical whether it ran alone or in any mix.
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -54,6 +55,7 @@ struct Req {
   int snap_pending = 0;  // staged but not yet written (guarded by the server mutex)
   uint64_t snaps_written = 0;
   std::string snap_err;
+  bool cancel = false;  // leave the batch at the next step boundary
 };
 
 struct SnapJob {
@@ -109,6 +111,8 @@ struct gx_server {
   std::deque<SnapJob> jobs;
   std::condition_variable cv_jobs;
   bool writer_stop = false, writer_started = false;
+  // metrics stream (gx_server_set_metrics_log), written by the stepping thread
+  FILE* metrics = nullptr;
 };
 
 namespace {
@@ -232,8 +236,17 @@ void run_loop(gx_server* s) {
     s->busy_s += seconds(t0, t1);
     s->steps += 1;
     std::vector<Req*> keep;
+    uint64_t step_particles = 0;
+    const size_t stepped = s->live.size();  // systems this step advanced
     for (Req* r : s->live) {
+      if (r->cancel) {  // cancelled while running: leave the batch, no result
+        gx_system_remove(s->batch, r->sys);
+        r->status = GX_REQ_CANCELLED;
+        r->t_done = Clock::now();
+        continue;
+      }
       s->particle_steps += r->n;
+      step_particles += r->n;
       ++r->done;
       if (r->snap_every && (r->done % r->snap_every == 0 || r->done == r->steps)) stage_snapshot(s, r, lk);
       if (r->done < r->steps) {
@@ -249,6 +262,15 @@ void run_loop(gx_server* s) {
       s->completed += 1;
     }
     s->live.swap(keep);
+    if (s->metrics) {
+      std::fprintf(s->metrics,
+                   "{\"step\": %llu, \"ms\": %.6f, \"live\": %zu, \"particles\": %llu, \"queued\": %zu, "
+                   "\"completed\": %llu, \"bytes_in_use\": %llu}\n",
+                   static_cast<unsigned long long>(s->steps), static_cast<double>(bs.ms_last_step), stepped,
+                   static_cast<unsigned long long>(step_particles), s->queue.size(),
+                   static_cast<unsigned long long>(s->completed), static_cast<unsigned long long>(bs.bytes_in_use));
+      std::fflush(s->metrics);
+    }
     s->cv_done.notify_all();
   }
 }
@@ -300,6 +322,7 @@ void gx_server_destroy(gx_server* s) {
   if (s->writer_started) s->writer.join();
   gx_batch_destroy(s->batch);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+  if (s->metrics) std::fclose(s->metrics);
   for (auto& kv : s->all) {
     free_snap(kv.second);
     delete kv.second;
@@ -356,6 +379,44 @@ int gx_server_submit_snapshots(gx_server* s, size_t n, const double* pos, const 
   return GX_OK;
 }
 
+int gx_server_cancel(gx_server* s, uint64_t rid) {
+  if (!s) return GX_ERR_INVALID_ARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(rid);
+    if (it == s->all.end()) return GX_ERR_NOT_FOUND;
+    Req* r = it->second;
+    if (r->status == GX_REQ_QUEUED) {
+      s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
+      r->status = GX_REQ_CANCELLED;
+      r->t_done = Clock::now();
+    } else if (r->status == GX_REQ_RUNNING) {
+      r->cancel = true;
+    } else {
+      return GX_ERR_STATE;
+    }
+  }
+  s->cv_done.notify_all();
+  return GX_OK;
+}
+
+int gx_server_set_metrics_log(gx_server* s, const char* path) {
+  if (!s) return GX_ERR_INVALID_ARG;
+  FILE* f = nullptr;
+  if (path) {
+    f = std::fopen(path, "a");
+    if (!f) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->err = std::string("cannot open ") + path;
+      return GX_ERR_INVALID_ARG;
+    }
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->metrics) std::fclose(s->metrics);
+  s->metrics = f;
+  return GX_OK;
+}
+
 int gx_server_snapshots_written(gx_server* s, uint64_t rid, uint64_t* written_out) {
   if (!s || !written_out) return GX_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(s->mu);
@@ -386,9 +447,11 @@ int gx_server_wait(gx_server* s, uint64_t rid, double timeout_s) {
   if (it == s->all.end()) return GX_ERR_NOT_FOUND;
   Req* r = it->second;
   const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
-    return (r->status == GX_REQ_DONE || r->status == GX_REQ_REJECTED) && r->snap_pending == 0;
+    return (r->status == GX_REQ_DONE || r->status == GX_REQ_REJECTED || r->status == GX_REQ_CANCELLED) &&
+           r->snap_pending == 0;
   });
   if (!ok) return GX_ERR_STATE;
+  if (r->status == GX_REQ_CANCELLED) return GX_ERR_CANCELLED;
   return r->status == GX_REQ_DONE ? GX_OK : GX_ERR_BUDGET;
 }
 
@@ -410,7 +473,8 @@ int gx_server_release(gx_server* s, uint64_t rid) {
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->all.find(rid);
   if (it == s->all.end()) return GX_ERR_NOT_FOUND;
-  if (it->second->status != GX_REQ_DONE && it->second->status != GX_REQ_REJECTED) return GX_ERR_STATE;
+  const int st = it->second->status;
+  if (st != GX_REQ_DONE && st != GX_REQ_REJECTED && st != GX_REQ_CANCELLED) return GX_ERR_STATE;
   if (it->second->snap_pending > 0) return GX_ERR_STATE;  // a snapshot is still being written
   free_snap(it->second);
   delete it->second;

@@ -36,6 +36,7 @@ extern "C" {
 #define GX_ERR_DEVICE_CHECK -6  /* a kernel's bounded wait or bounds check tripped */
 #define GX_ERR_NOT_FOUND -7     /* unknown system / request id */
 #define GX_ERR_CAPACITY -8      /* a fixed-size table is full */
+#define GX_ERR_CANCELLED -9     /* the request was cancelled (gx_server_cancel) */
 
 /* ---- options --------------------------------------------------------------- */
 #define GX_PREC_F32 0  /* FP32 interactions with Kahan-compensated accumulation (default) */
@@ -270,6 +271,7 @@ typedef struct gx_server gx_server;
 #define GX_REQ_RUNNING 1
 #define GX_REQ_DONE 2
 #define GX_REQ_REJECTED 3
+#define GX_REQ_CANCELLED 4
 
 typedef struct gx_server_stats {
   uint64_t steps;            /* batched steps taken */
@@ -302,6 +304,13 @@ int gx_server_wait(gx_server* s, uint64_t rid, double timeout_s);
 int gx_server_result(gx_server* s, uint64_t rid, double* pos_out, double* vel_out, double* time_out);
 int gx_server_release(gx_server* s, uint64_t rid);
 int gx_server_stats_get(gx_server* s, gx_server_stats* out);
+/* Cancel a request: a queued one leaves the queue, a running one leaves the batch at the
+ * next step boundary (the other systems are unaffected); gx_server_wait then returns
+ * GX_ERR_CANCELLED. GX_ERR_STATE if it has already finished. */
+int gx_server_cancel(gx_server* s, uint64_t rid);
+/* Append one JSON line per batched step to `path` (NULL: stop): step, device ms, systems
+ * stepped ("live"), their particles, queued requests, completed requests, device bytes in use. */
+int gx_server_set_metrics_log(gx_server* s, const char* path);
 
 /* ---- GLXYSNAP v4 snapshots (io/src/snapshot.rs:1-60 layout, :130-199 to_writer) ---
  * Files readable by the reference's io::snapshot::read_file: header (time, step, scale

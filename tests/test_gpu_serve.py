@@ -120,3 +120,38 @@ def test_snapshot_emission_matches_alone(tmp_path):
             assert np.array_equal(c["mass"], st.mass.astype(np.float32).astype(np.float64))
         final = srv.result(rid)
         assert np.array_equal(final.pos, ref.pos) and np.array_equal(final.vel, ref.vel)
+
+
+def test_cancel_queued_and_running_leaves_others_exact(tmp_path):
+    """Fault injection on the host: a request cancelled while queued and one cancelled
+    mid-stream; the rest finish bit-identical to running alone, and every step appears
+    in the JSON-lines metrics stream."""
+    import json
+
+    one = gb.Batch().system_bytes(8_000)
+    srv = gb.Server(budget_bytes=int(2.4 * one))  # two resident at a time
+    log = tmp_path / "metrics.jsonl"
+    srv.set_metrics_log(str(log))
+    sts = [gb.ic.plummer(8_000, 500 + i) for i in range(4)]
+    rids = [srv.submit(st, 1.0, 0.01, 0.5, 1e-3, 400 if i == 0 else 30) for i, st in enumerate(sts)]
+    srv.cancel(rids[3])  # still queued behind the two resident ones
+    t0 = time.time()
+    while srv.status(rids[0])[1] < 5 and time.time() - t0 < 60:
+        time.sleep(0.005)
+    srv.cancel(rids[0])  # running: leaves at the next step boundary
+    for rid in (rids[0], rids[3]):
+        with pytest.raises(gb.GxError) as e:
+            srv.wait(rid, 60)
+        assert e.value.code == -9
+        assert srv.status(rid)[0] == gb.Server.CANCELLED
+    for rid, st in zip(rids[1:3], sts[1:3]):
+        srv.wait(rid, 300)
+        ref = _alone(st, 0.01, 0.5, 1e-3, 30)
+        assert np.array_equal(srv.result(rid).pos, ref.pos)
+    with pytest.raises(gb.GxError):
+        srv.cancel(rids[1])  # already finished
+    s = srv.stats()
+    srv.set_metrics_log(None)
+    lines = [json.loads(x) for x in log.read_text().splitlines()]
+    assert len(lines) == s["steps"] and lines[-1]["completed"] == s["completed"]
+    assert all(x["ms"] > 0 and x["live"] >= 1 for x in lines)
