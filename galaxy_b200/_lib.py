@@ -130,6 +130,7 @@ SIGNATURES = {
     "gx_last_error": (C.c_char_p, [_vp]),
     "gx_device_info": (_i, [_i, C.c_char_p, _sz, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_sz)]),
     "gx_device_synchronize": (_i, [_i]),
+    "gx_selftest_bounded_wait": (_i, [_i, C.c_uint32, C.POINTER(C.c_uint32)]),
     "gx_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_accelerations_device": (_i, [_vp, _sz, _vp, _vp, _vp]),
     "gx_accelerations_active": (_i, [_vp, _sz, _vp, _vp, _sz, _vp, _vp]),

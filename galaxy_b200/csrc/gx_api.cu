@@ -379,20 +379,31 @@ void enqueue_tree(gx_handle* h, const StepBufs& b, int kick, int pending, bool t
   cudaStream_t st = h->stream;
   ++h->tree_gen;
   if (timed) cudaEventRecord(h->ev[0], st);
-  cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, st);
-  launch_kick_drift_bbox(b, kick, pending, st);
-  launch_morton_hist(b, nullptr, st);
+  {
+    NvtxRange r("gx.kick_drift_bbox_morton");
+    cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, st);
+    launch_kick_drift_bbox(b, kick, pending, st);
+    launch_morton_hist(b, nullptr, st);
+  }
   if (timed) cudaEventRecord(h->ev[1], st);
-  launch_sort(b, st);
+  {
+    NvtxRange r("gx.sort");
+    launch_sort(b, st);
+  }
   if (timed) cudaEventRecord(h->ev[2], st);
-  launch_build(b, h->opt.multipole == GX_MULTIPOLE_QUAD && h->opt.precision != GX_PREC_F64,
-               h->opt.precision == GX_PREC_F64, st);
+  {
+    NvtxRange r("gx.build");
+    launch_build(b, h->opt.multipole == GX_MULTIPOLE_QUAD && h->opt.precision != GX_PREC_F64,
+                 h->opt.precision == GX_PREC_F64, st);
+  }
   if (timed) cudaEventRecord(h->ev[3], st);
 }
 
 // Enqueue the tree and the walk of every target on b.
 void enqueue_force(gx_handle* h, const StepBufs& b, int kick, int pending, bool timed) {
+  NvtxRange r("gx.step");
   enqueue_tree(h, b, kick, pending, timed);
+  NvtxRange w("gx.walk");
   launch_walk(b, walk_cfg(h), h->stream);
   if (timed) cudaEventRecord(h->ev[4], h->stream);
   h->launches += 1;
@@ -531,6 +542,42 @@ void gx_destroy(gx_handle* h) {
 }
 
 const char* gx_last_error(const gx_handle* h) { return h ? h->err.c_str() : global_err(); }
+
+int gx_selftest_bounded_wait(int device, uint32_t spins, uint32_t* err_word_out) {
+  if (!err_word_out) return GX_ERR_INVALID_ARG;
+  std::string err;
+  if (!check_device(device, err)) {
+    set_global_err(err);
+    return GX_ERR_NO_DEVICE;
+  }
+  int dev = device;
+  if (dev < 0) cudaGetDevice(&dev);
+  cudaSetDevice(dev);
+  DevCtl* ctl = nullptr;
+  uint32_t* word = nullptr;
+  cudaError_t e = cudaMalloc(&ctl, sizeof(DevCtl));
+  if (e == cudaSuccess) e = cudaMalloc(&word, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(ctl, 0, sizeof(DevCtl));
+  if (e == cudaSuccess) e = cudaMemset(word, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    launch_selftest_wait(word, spins, ctl, nullptr);
+    e = cudaDeviceSynchronize();
+  }
+  DevCtl host{};
+  if (e == cudaSuccess) e = cudaMemcpy(&host, ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost);
+  if (ctl) cudaFree(ctl);
+  if (word) cudaFree(word);
+  if (e != cudaSuccess) {
+    set_global_err(std::string("self-test: ") + cudaGetErrorString(e));
+    return GX_ERR_CUDA;
+  }
+  *err_word_out = host.err;
+  if (host.err) {
+    set_global_err("device check tripped (bounded wait ran out)");
+    return GX_ERR_DEVICE_CHECK;
+  }
+  return GX_OK;
+}
 
 int gx_device_synchronize(int device) {
   int dev = device;

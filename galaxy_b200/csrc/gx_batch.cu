@@ -130,6 +130,7 @@ int upload_tables(gx_batch* bt, const std::vector<size_t>& which, bool* inside) 
 }
 
 void enqueue_step(gx_batch* bt, int kick, bool inside) {
+  NvtxRange r("gx.batch_step");
   const StepBufs& b = bt->ar.b;
   cudaStream_t st = bt->stream;
   cudaMemsetAsync(b.zero_begin, 0, b.zero_bytes, st);

@@ -203,4 +203,20 @@ __device__ __forceinline__ void split_ff(double x, float& hi, float& lo) {
 
 __device__ __forceinline__ void raise_err(DevCtl* ctl, uint32_t bit) { atomicOr(&ctl->err, bit); }
 
+// Bounded wait for a status word whose top two bits become non-zero (set by another
+// CTA): at most `limit` re-reads, backing off between them. Returns the word, or 0
+// after raising kErrLookbackTimeout when the limit runs out -- no wait is unbounded.
+__device__ __forceinline__ uint32_t wait_flagged(const uint32_t* p, uint32_t limit, DevCtl* ctl) {
+  uint32_t w = *reinterpret_cast<const volatile uint32_t*>(p);
+  for (uint32_t spins = 0; (w >> 30) == 0u; ++spins) {
+    if (spins >= limit) {
+      raise_err(ctl, kErrLookbackTimeout);
+      return 0u;
+    }
+    __nanosleep(64);
+    w = *reinterpret_cast<const volatile uint32_t*>(p);
+  }
+  return w;
+}
+
 }  // namespace gx

@@ -130,6 +130,16 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_sums(uint32_t n, const do
   }
 }
 
+// Failure-detection self-test: lane 0 waits, through the sort look-back's bounded wait,
+// for a word nothing sets; the wait runs out, raises the error word and returns.
+__global__ void k_selftest_wait(const uint32_t* word, uint32_t spins, DevCtl* ctl) {
+  if (threadIdx.x == 0) (void)wait_flagged(word, spins, ctl);
+}
+
+void launch_selftest_wait(const uint32_t* word, uint32_t spins, DevCtl* ctl, cudaStream_t st) {
+  k_selftest_wait<<<1, 32, 0, st>>>(word, spins, ctl);
+}
+
 void launch_direct_sum_f64(uint32_t n, const double* pos, const double* mass, double g, double eps,
                            uint32_t n_targets, const uint32_t* targets, double* acc, cudaStream_t st) {
   const uint32_t grid = (n_targets + kDiagThreads - 1) / kDiagThreads;

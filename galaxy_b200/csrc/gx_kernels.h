@@ -90,6 +90,8 @@ void launch_code_hist(const StepBufs& b, cudaStream_t st);
 void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st);
 // gx_walk.cu: tree walk, acc in original order
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st);
+// gx_diag.cu: one bounded wait on a word nothing sets (failure-detection self-test)
+void launch_selftest_wait(const uint32_t* word, uint32_t spins, DevCtl* ctl, cudaStream_t st);
 // gx_active.cu: the active-subset walk's target list. From the sorted order and the
 // active particles (original indices) it builds, in sorted order, the list of active
 // sorted positions (list, count in *count_out) and one walk item per `group` of them.

@@ -8,7 +8,17 @@
 #include "../../include/galaxy_b200.h"
 #include "gx_kernels.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace gx {
+
+// An NVTX range over a scope (host enqueue of a stage; free when no tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct Arena {
   StepBufs b;

@@ -44,7 +44,6 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_
   return base + x - v;
 }
 
-__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
 __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *reinterpret_cast<volatile uint32_t*>(p) = v; }
 
 }  // namespace
@@ -135,17 +134,8 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __
     st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagAgg | (total & kValMask));
     uint32_t p = tile - 1;
     for (;;) {
-      uint32_t w = ld_volatile(&st[(size_t)p * kRadixBins + d]);
-      uint32_t spins = 0;
-      while ((w & ~kValMask) == 0) {
-        if (++spins > kSpinLimit) {
-          raise_err(ctl, kErrLookbackTimeout);
-          w = kFlagPrefix;
-          break;
-        }
-        __nanosleep(64);
-        w = ld_volatile(&st[(size_t)p * kRadixBins + d]);
-      }
+      uint32_t w = wait_flagged(&st[(size_t)p * kRadixBins + d], kSpinLimit, ctl);
+      if (w == 0u) w = kFlagPrefix;  // timed out (error raised): end the look-back
       excl += w & kValMask;
       if ((w & ~kValMask) == kFlagPrefix || p == sd.first_tile) break;
       --p;

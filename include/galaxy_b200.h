@@ -93,6 +93,12 @@ int gx_device_info(int device, char* name_out, size_t name_len, int* sm_count, i
 /* Wait until all work on the device has finished (every stream, every handle). A timing
  * helper with no counterpart in the reference. */
 int gx_device_synchronize(int device);
+/* Failure-detection self-test (no counterpart in the reference): one warp waits, through
+ * the same bounded wait as the radix sort's look-back, for a status word nothing ever
+ * sets, re-reading it `spins` times. The wait runs out, the kernel raises its error word
+ * and returns: the call gives GX_ERR_DEVICE_CHECK with the word in *err_word_out (bit 0:
+ * a wait ran out), and the device stays usable. Nothing faults or hangs. */
+int gx_selftest_bounded_wait(int device, uint32_t spins, uint32_t* err_word_out);
 
 /* ---- ForceSolver (core/src/traits.rs:27, :95) ------------------------------- */
 /* ForceSolver::accelerations -- gpu/src/gpu_lbvh_fused.rs:58-134, solvers/src/lbvh.rs:663-676.
