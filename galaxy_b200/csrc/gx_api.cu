@@ -271,6 +271,8 @@ struct gx_handle {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[6] = {};
+  cudaEvent_t chunk_ev[8] = {};  // gx_kdk_step_host: acceleration chunks copied back
+  DevCtl* ctl_host = nullptr;     // pinned copy of the device error word
   std::string err;
   Arena ar;
   // current layout
@@ -519,6 +521,8 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&h->chunk_ev[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaHostAlloc(&h->ctl_host, sizeof(DevCtl), cudaHostAllocDefault);
   if (e != cudaSuccess) {
     set_global_err(std::string("stream/event creation failed: ") + cudaGetErrorString(e));
     delete h;
@@ -535,6 +539,9 @@ void gx_destroy(gx_handle* h) {
   free_active(h);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   h->ar.release();
+  for (auto& e : h->chunk_ev)
+    if (e) cudaEventDestroy(e);
+  if (h->ctl_host) cudaFreeHost(h->ctl_host);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -946,45 +953,55 @@ int gx_kdk_step_host(gx_handle* h, size_t n, double* pos, double* vel, const dou
     *primed = 1;
   }
   const double half = 0.5 * dt;
-  // Opening half kick and drift (integrator.rs:59-67: v += a h, then x += v dt, each
-  // rounded separately), on all host threads and in chunks, each chunk's positions
-  // copied to the device while the next chunk is computed. Then the force as in
-  // gx_accelerations, and the closing half kick.
-  if (n > 1) {
-    cudaSetDevice(h->device);
-    h->resident = false;
-    rc = layout(h, n, 0.0);
-    if (rc) return rc;
-    StepBufs& b = h->ar.b;
-    const size_t chunk = std::max<size_t>(size_t{1} << 16, (n + 7) / 8);
-    for (size_t c0 = 0; c0 < n; c0 += chunk) {
-      const long long i0 = static_cast<long long>(3 * c0);
-      const long long i1 = static_cast<long long>(3 * std::min(n, c0 + chunk));
-#pragma omp parallel for schedule(static)
-      for (long long i = i0; i < i1; ++i) {
-        vel[i] = vel[i] + acc[i] * half;
-        pos[i] = pos[i] + vel[i] * dt;
-      }
-      GX_CK(h, cudaMemcpyAsync(b.pos + i0, pos + i0, (i1 - i0) * sizeof(double), cudaMemcpyHostToDevice,
-                               h->stream));
-    }
-    GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    enqueue_force(h, b, 0, 0, stats_on(h));
-    GX_CK(h, cudaMemcpyAsync(acc, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    h->stats.n = n;
-    rc = finish(h, stats_on(h));
-    if (rc) return rc;
-  } else {  // a lone particle: no force
+  if (n == 1) {  // a lone particle: no force
     for (size_t i = 0; i < 3; ++i) {
       vel[i] = vel[i] + acc[i] * half;
       pos[i] = pos[i] + vel[i] * dt;
       acc[i] = 0.0;
+      vel[i] = vel[i] + acc[i] * half;
     }
+    return GX_OK;
   }
-  const long long m = static_cast<long long>(3 * n);
+  // Opening half kick and drift (integrator.rs:59-67: v += a h, then x += v dt, each
+  // rounded separately), on all host threads and in chunks, each chunk's positions
+  // copied to the device while the next chunk is computed. Then the force as in
+  // gx_accelerations, and the closing half kick of each chunk of accelerations as soon
+  // as that chunk is back (after the error word, so nothing is kicked by a failed step).
+  cudaSetDevice(h->device);
+  h->resident = false;
+  rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const size_t chunk = std::max<size_t>(size_t{1} << 16, (n + 7) / 8);
+  for (size_t c0 = 0; c0 < n; c0 += chunk) {
+    const long long i0 = static_cast<long long>(3 * c0);
+    const long long i1 = static_cast<long long>(3 * std::min(n, c0 + chunk));
 #pragma omp parallel for schedule(static)
-  for (long long i = 0; i < m; ++i) vel[i] = vel[i] + acc[i] * half;
-  return GX_OK;
+    for (long long i = i0; i < i1; ++i) {
+      vel[i] = vel[i] + acc[i] * half;
+      pos[i] = pos[i] + vel[i] * dt;
+    }
+    GX_CK(h, cudaMemcpyAsync(b.pos + i0, pos + i0, (i1 - i0) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  enqueue_force(h, b, 0, 0, stats_on(h));
+  GX_CK(h, cudaMemcpyAsync(h->ctl_host, b.ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
+  int nch = 0;
+  for (size_t c0 = 0; c0 < n; c0 += chunk, ++nch) {
+    const size_t i0 = 3 * c0, i1 = 3 * std::min(n, c0 + chunk);
+    GX_CK(h, cudaMemcpyAsync(acc + i0, b.acc + i0, (i1 - i0) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    GX_CK(h, cudaEventRecord(h->chunk_ev[nch], h->stream));
+  }
+  h->stats.n = n;
+  for (int c = 0; c < nch; ++c) {
+    GX_CK(h, cudaEventSynchronize(h->chunk_ev[c]));
+    if (c == 0 && h->ctl_host->err) return finish(h, stats_on(h));  // the step failed: report, no kick
+    const long long i0 = static_cast<long long>(3 * (size_t)c * chunk);
+    const long long i1 = static_cast<long long>(3 * std::min(n, ((size_t)c + 1) * chunk));
+#pragma omp parallel for schedule(static)
+    for (long long i = i0; i < i1; ++i) vel[i] = vel[i] + acc[i] * half;
+  }
+  return finish(h, stats_on(h));
 }
 
 int gx_host_alloc(size_t bytes, void** out) {
