@@ -12,6 +12,10 @@ project root), each a thin layer over the C ABI of ``libgalaxy_b200.so``:
 * :class:`GpuResidentLeapfrog` -- ``gpu/src/gpu_resident.rs:1685-1960``
   (upload / step / step_many / snapshot / time / len / submits).
 * :class:`Batch` -- many independent systems stepped by one launch per stage.
+* :class:`GpuGravitySph` -- ``solvers/src/sph/gravity_sph.rs`` (gravity + SPH on the gas
+  rows), and the resident gas mode of :class:`GpuResidentLeapfrog`
+  (``gpu_resident.rs:1393-1660``: ``new_with_sph``, ``snapshot_gas_density``,
+  ``snapshot_gas_accel``, ``min_stable_dt``, ``snapshot_gas_dt``, ``snapshot_accel``).
 * stage functions ``stage_morton`` / ``stage_sort`` / ``stage_build`` -- the
   ``reference_*`` oracles' GPU counterparts (``solvers/src/lbvh.rs:105-348``).
 
@@ -31,7 +35,8 @@ from ._lib import (GX_FLAG_MORTON63, GX_FLAG_NO_KAHAN, GX_FLAG_STAGE_TIMES, GX_F
                    GX_MULTIPOLE_QUAD, GX_PREC_F32, GX_PREC_F64, GxError, check, lib)
 
 __all__ = [
-    "State", "ForceSolver", "GpuLbvh", "GpuStaleTreeGravity", "LeapfrogKdk", "GpuResidentLeapfrog", "Batch",
+    "State", "ForceSolver", "GpuLbvh", "GpuStaleTreeGravity", "GpuGravitySph", "LeapfrogKdk", "GpuResidentLeapfrog",
+    "Batch", "sph_params", "GasDensity", "GasCfl", "GAS", "COLLISIONLESS",
     "Server", "GxError",
     "PinnedState",
     "stage_morton",
@@ -50,14 +55,20 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
+GAS, COLLISIONLESS = 1, 0  # core/src/state.rs:17-22 Species
+
+
 @dataclass
 class State:
-    """core/src/state.rs:29 -- positions/velocities [n,3] f64, masses [n] f64, time."""
+    """core/src/state.rs:29 -- positions/velocities [n,3] f64, masses [n] f64, time; the
+    species column ``kind`` [n] u8 (1 = gas) and internal energy ``u`` [n] f64."""
 
     pos: np.ndarray
     vel: np.ndarray
     mass: np.ndarray
     time: float = 0.0
+    kind: np.ndarray = None
+    u: np.ndarray = None
 
     def __post_init__(self):
         self.pos = _f64(self.pos).reshape(-1, 3)
@@ -66,12 +77,21 @@ class State:
         n = self.pos.shape[0]
         if self.vel.shape[0] != n or self.mass.shape[0] != n:
             raise ValueError("vel/mass length must match pos")
+        self.kind = (np.zeros(n, dtype=np.uint8) if self.kind is None
+                     else np.ascontiguousarray(self.kind, dtype=np.uint8).reshape(-1))
+        self.u = np.zeros(n) if self.u is None else _f64(self.u).reshape(-1)
+        if self.kind.shape[0] != n or self.u.shape[0] != n:
+            raise ValueError("kind/u length must match pos")
 
     def __len__(self):
         return self.pos.shape[0]
 
     def copy(self) -> "State":
-        return State(self.pos.copy(), self.vel.copy(), self.mass.copy(), self.time)
+        return State(self.pos.copy(), self.vel.copy(), self.mass.copy(), self.time, self.kind.copy(), self.u.copy())
+
+    def gas(self) -> np.ndarray:
+        """Indices of the gas rows, ascending."""
+        return np.flatnonzero(self.kind == GAS).astype(np.uint32)
 
 
 class ForceSolver:
@@ -261,6 +281,73 @@ class GpuStaleTreeGravity(GpuLbvh):
         return out
 
 
+class GpuGravitySph(GpuLbvh):
+    """GravitySph (solvers/src/sph/gravity_sph.rs:24-402) over this library's LBVH gravity:
+    gravity on every particle, density, smoothing lengths and the hydro force on the gas
+    rows (``state.kind == 1``), h warm-started across calls while the gas count holds.
+    SPH parameters as :func:`sph_params` keywords (``sph=dict(...)``)."""
+
+    def __init__(self, g, softening, theta, sph=None, **kw):
+        super().__init__(g, softening, theta, **kw)
+        self.params = sph_params(**(sph or {}))
+        self._ck(lib().gx_sph_enable(self._h, C.byref(self.params)))
+
+    def accelerations(self, state, acc=None):
+        n = len(state)
+        if acc is None:
+            acc = np.empty((n, 3))
+        elif acc.shape != (n, 3) or not acc.flags.c_contiguous or acc.dtype != np.float64:
+            raise ValueError("acc length must match particle count (C-contiguous f64 [n,3])")
+        self._ck(lib().gx_sph_accelerations(self._h, n, _ptr(state.pos), _ptr(state.vel), _ptr(state.mass),
+                                            _ptr(state.kind), _ptr(state.u), _ptr(acc)))
+        return acc
+
+    def density(self, pos, mass, h_init=None):
+        """density_adaptive (density.rs:86-96) over gas positions: (rho, h)."""
+        pos, mass = _f64(pos).reshape(-1, 3), _f64(mass).reshape(-1)
+        n = pos.shape[0]
+        rho, h = np.zeros(n), np.zeros(n)
+        hi = None if h_init is None else _f64(h_init).reshape(-1)
+        self._ck(lib().gx_sph_density(self._h, n, _ptr(pos), _ptr(mass), _ptr(hi), _ptr(rho), _ptr(h)))
+        return rho, h
+
+    def hydro(self, pos, vel, mass, rho, h, u=None):
+        """hydro_accel_and_dudt (forces.rs:160-172): (acc [n,3], dudt [n])."""
+        pos, vel = _f64(pos).reshape(-1, 3), _f64(vel).reshape(-1, 3)
+        n = pos.shape[0]
+        acc, dudt = np.zeros((n, 3)), np.zeros(n)
+        uu = None if u is None else _f64(u).reshape(-1)
+        self._ck(lib().gx_sph_hydro(self._h, n, _ptr(pos), _ptr(vel), _ptr(_f64(mass)), _ptr(_f64(rho)),
+                                    _ptr(_f64(h)), _ptr(uu), _ptr(acc), _ptr(dudt)))
+        return acc, dudt
+
+    def cfl(self, pos, vel, h, c_cfl, u=None):
+        """The per-particle CFL bound (cfl.rs:134-185 body) with given h: (dt [n], min)."""
+        pos, vel = _f64(pos).reshape(-1, 3), _f64(vel).reshape(-1, 3)
+        n = pos.shape[0]
+        dt, m = np.zeros(n), C.c_double()
+        uu = None if u is None else _f64(u).reshape(-1)
+        self._ck(lib().gx_sph_cfl(self._h, n, _ptr(pos), _ptr(vel), _ptr(_f64(h)), _ptr(uu), float(c_cfl),
+                                  _ptr(dt), C.byref(m)))
+        return dt, m.value
+
+    def max_stable_dt_per_particle(self, state, c_cfl: float = 1.0) -> np.ndarray:
+        """cfl.rs:134-185 (gravity_sph.rs:380-386 at Courant number 1): state-indexed,
+        +inf on collisionless rows; h from a cold-start density solve."""
+        out = np.full(len(state), np.inf)
+        gas = state.gas()
+        if gas.size:
+            gpos, gvel = state.pos[gas], state.vel[gas]
+            _, h = self.density(gpos, state.mass[gas])
+            dt, _ = self.cfl(gpos, gvel, h, c_cfl, state.u[gas])
+            out[gas] = dt
+        return out
+
+    def max_stable_dt(self, state, c_cfl: float = 1.0) -> float:
+        """ForceSolver::max_stable_dt of GravitySph (gravity_sph.rs:371-378; cfl.rs:49-125)."""
+        return float(self.max_stable_dt_per_particle(state, c_cfl).min()) if len(state) else float("inf")
+
+
 class LeapfrogKdk:
     """core/src/integrator.rs:6-78 -- kick-drift-kick with cached accelerations (host arrays)."""
 
@@ -293,18 +380,108 @@ class LeapfrogKdk:
         state.time += dt
 
 
+def sph_params(**kw) -> "_lib.SphParams":
+    """HydroParams (solvers/src/sph/forces.rs:64-87) + DensityConfig (density.rs:33-51) as
+    the C struct: the reference defaults, overridden by keyword (n_ngb, h_tol_rel, eos
+    "isothermal" / "adiabatic", c_s, gamma, alpha, beta, visc_eps2, warm_start)."""
+    p = _lib.SphParams()
+    lib().gx_sph_default_params(C.byref(p))
+    for k, v in kw.items():
+        if k == "eos":
+            v = {"isothermal": _lib.GX_EOS_ISOTHERMAL, "adiabatic": _lib.GX_EOS_ADIABATIC}.get(v, v)
+        if not hasattr(p, k):
+            raise TypeError(f"unknown SPH parameter {k}")
+        setattr(p, k, int(v) if k in ("eos", "warm_start") else float(v))
+    return p
+
+
+@dataclass
+class GasDensity:
+    """gpu_resident.rs GasDensity: the gas map and its (rho, h), ascending gas index."""
+
+    gas_idx: np.ndarray
+    rho: np.ndarray
+    h: np.ndarray
+
+
+@dataclass
+class GasCfl:
+    gas_idx: np.ndarray
+    dt: np.ndarray
+
+
 class GpuResidentLeapfrog(_Handle):
-    """gpu/src/gpu_resident.rs:1685-1960 -- state kept on the device across KDK steps."""
+    """gpu/src/gpu_resident.rs:1685-1960 -- state kept on the device across KDK steps.
+
+    ``sph`` (a dict of :func:`sph_params` keywords, or True for the defaults) is
+    ``new_with_sph`` (gpu_resident.rs:1393): gas mode, SPH on the ``kind == 1`` rows."""
 
     MAX_BATCH = 64  # the reference's submit cap; steps here are graph launches, not submits
 
-    def __init__(self, g, softening, theta, **kw):
+    def __init__(self, g, softening, theta, sph=None, **kw):
         super().__init__(g, softening, theta, **kw)
         self._mass = np.zeros(0)
+        self._kind = np.zeros(0, dtype=np.uint8)
+        self._u = np.zeros(0)
+        self.gas_mode = sph is not None and sph is not False
+        if self.gas_mode:
+            p = sph_params(**(sph if isinstance(sph, dict) else {}))
+            self._ck(lib().gx_sph_enable(self._h, C.byref(p)))
+
+    @classmethod
+    def new_with_sph(cls, g, softening, theta, sph=None, **kw):
+        """GpuResidentLeapfrog::new_with_sph (gpu_resident.rs:1393-1404): ``sph`` holds the
+        :func:`sph_params` keywords (HydroParams + DensityConfig), ``kw`` the handle's."""
+        return cls(g, softening, theta, sph=dict(sph or {}), **kw)
 
     def upload(self, state: State):
         self._mass = state.mass.copy()
-        self._ck(lib().gx_upload(self._h, len(state), _ptr(state.pos), _ptr(state.vel), _ptr(state.mass)))
+        self._kind = state.kind.copy()
+        self._u = state.u.copy()
+        if self.gas_mode:
+            self._ck(lib().gx_upload_species(self._h, len(state), _ptr(state.pos), _ptr(state.vel),
+                                             _ptr(state.mass), _ptr(state.kind), _ptr(state.u)))
+        else:
+            self._ck(lib().gx_upload(self._h, len(state), _ptr(state.pos), _ptr(state.vel), _ptr(state.mass)))
+
+    def gas_count(self) -> int:
+        n = C.c_size_t()
+        self._ck(lib().gx_gas_count(self._h, C.byref(n)))
+        return n.value
+
+    def snapshot_gas_density(self) -> GasDensity:
+        """gpu_resident.rs:1566-1587."""
+        ng = self.gas_count()
+        idx, rho, h = np.zeros(ng, dtype=np.uint32), np.zeros(ng), np.zeros(ng)
+        self._ck(lib().gx_snapshot_gas_density(self._h, _ptr(idx), _ptr(rho), _ptr(h)))
+        return GasDensity(idx, rho, h)
+
+    def snapshot_gas_accel(self, with_dudt: bool = False):
+        """gpu_resident.rs:1593-1607: the hydro acceleration of the gas rows alone."""
+        ng = self.gas_count()
+        acc, dudt = np.zeros((ng, 3)), np.zeros(ng)
+        self._ck(lib().gx_snapshot_gas_accel(self._h, _ptr(acc), _ptr(dudt)))
+        return (acc, dudt) if with_dudt else acc
+
+    def snapshot_accel(self) -> np.ndarray:
+        """gpu_resident.rs:1655: the full acceleration of every particle."""
+        out = np.empty((len(self), 3))
+        self._ck(lib().gx_snapshot_accel(self._h, _ptr(out)))
+        return out
+
+    def min_stable_dt(self, c_cfl: float) -> float:
+        """gpu_resident.rs:1614-1626: min_i c_cfl h_i / v_sig,i, reduced on the device."""
+        out = C.c_double()
+        self._ck(lib().gx_min_stable_dt(self._h, float(c_cfl), C.byref(out)))
+        return out.value
+
+    def snapshot_gas_dt(self, c_cfl: float) -> GasCfl:
+        """gpu_resident.rs:1632-1650."""
+        ng = self.gas_count()
+        dt = np.zeros(ng)
+        if ng:
+            self._ck(lib().gx_snapshot_gas_dt(self._h, float(c_cfl), _ptr(dt)))
+        return GasCfl(self.snapshot_gas_density().gas_idx, dt)
 
     def step(self, dt: float):
         self._ck(lib().gx_step(self._h, float(dt)))
@@ -333,7 +510,7 @@ class GpuResidentLeapfrog(_Handle):
         n = len(self)
         pos, vel = np.empty((n, 3)), np.empty((n, 3))
         self._ck(lib().gx_snapshot(self._h, _ptr(pos), _ptr(vel)))
-        return State(pos, vel, self._mass.copy(), self.time())
+        return State(pos, vel, self._mass.copy(), self.time(), self._kind.copy(), self._u.copy())
 
     def accelerations(self) -> np.ndarray:
         out = np.empty((len(self), 3))

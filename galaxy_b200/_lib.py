@@ -64,6 +64,25 @@ class Stats(C.Structure):
         ("ms_build", C.c_float),
         ("ms_walk", C.c_float),
         ("ms_total", C.c_float),
+        ("ms_sph", C.c_float),
+        ("pad", C.c_float),
+    ]
+
+
+GX_EOS_ISOTHERMAL, GX_EOS_ADIABATIC = 0, 1
+
+
+class SphParams(C.Structure):
+    _fields_ = [
+        ("n_ngb", C.c_double),
+        ("h_tol_rel", C.c_double),
+        ("eos", C.c_int),
+        ("warm_start", C.c_int),
+        ("c_s", C.c_double),
+        ("gamma", C.c_double),
+        ("alpha", C.c_double),
+        ("beta", C.c_double),
+        ("visc_eps2", C.c_double),
     ]
 
 
@@ -190,6 +209,19 @@ SIGNATURES = {
     "gx_ic_plummer": (_i, [_sz, _u64, _d, _d, _d, _vp, _vp, _vp]),
     "gx_ic_collision": (_i, [_sz, _u64, _d, _d, _d, _d, _vp, _vp, _vp]),
     "gx_ic_disk_galaxy": (_i, [_sz, _u64, _vp, _vp, _vp]),
+    "gx_sph_default_params": (None, [C.POINTER(SphParams)]),
+    "gx_sph_enable": (_i, [_vp, C.POINTER(SphParams)]),
+    "gx_upload_species": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp]),
+    "gx_gas_count": (_i, [_vp, C.POINTER(_sz)]),
+    "gx_snapshot_gas_density": (_i, [_vp, _vp, _vp, _vp]),
+    "gx_snapshot_gas_accel": (_i, [_vp, _vp, _vp]),
+    "gx_snapshot_accel": (_i, [_vp, _vp]),
+    "gx_min_stable_dt": (_i, [_vp, _d, C.POINTER(_d)]),
+    "gx_snapshot_gas_dt": (_i, [_vp, _d, _vp]),
+    "gx_sph_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gx_sph_density": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp]),
+    "gx_sph_hydro": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gx_sph_cfl": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _d, _vp, C.POINTER(_d)]),
 }
 
 

@@ -21,6 +21,9 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgalaxy_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Sources whose FP64 arithmetic keeps every product and sum rounded separately, in the
+# reference's operation order (no fused multiply-add contraction).
+NO_FMA = {"gx_sph.cu"}
 
 
 def _host_cxx() -> str:
@@ -48,6 +51,8 @@ def _compile(src: str, verbose_ptxas: bool) -> str:
            "-o", obj]
     if src.endswith(".cu"):
         cmd[1:1] = ["-x", "cu"]
+        if os.path.basename(src) in NO_FMA:
+            cmd.insert(1, "-fmad=false")
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)

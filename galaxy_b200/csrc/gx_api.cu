@@ -10,6 +10,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -19,6 +21,7 @@
 #include "../../include/galaxy_b200.h"
 #include "gx_kernels.h"
 #include "gx_runtime.h"
+#include "gx_sph.h"
 
 using namespace gx;
 
@@ -270,7 +273,7 @@ struct gx_handle {
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[7] = {};  // stage boundaries; [5] gx_step_many_timed, [6] end of SPH
   cudaEvent_t chunk_ev[8] = {};  // gx_kdk_step_host: acceleration chunks copied back
   DevCtl* ctl_host = nullptr;     // pinned copy of the device error word
   std::string err;
@@ -299,6 +302,10 @@ struct gx_handle {
     double* out = nullptr;       // gathered accelerations
     size_t cap_n = 0, cap_a = 0;
   } act;
+  // gas mode (GpuResidentLeapfrog::new_with_sph): SPH on the gas rows after gravity
+  SphState sph;
+  bool resident_gas = false;     // the resident state has gas and runs SPH in each force
+  size_t sph_host_hint_ngas = 0;  // gx_sph_accelerations: gas count of the last call
   // graph of one resident step (pending closing kick + opening kick, drift, force)
   cudaGraphExec_t step_graph = nullptr;
   size_t graph_n = 0;
@@ -408,6 +415,11 @@ void enqueue_force(gx_handle* h, const StepBufs& b, int kick, int pending, bool 
   NvtxRange w("gx.walk");
   launch_walk(b, walk_cfg(h), h->stream);
   if (timed) cudaEventRecord(h->ev[4], h->stream);
+  if (h->resident && h->resident_gas) {
+    NvtxRange g("gx.sph");
+    sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream);
+    if (timed) cudaEventRecord(h->ev[6], h->stream);
+  }
   h->launches += 1;
 }
 
@@ -424,6 +436,8 @@ int finish(gx_handle* h, bool timed) {
     cudaEventElapsedTime(&h->stats.ms_build, h->ev[2], h->ev[3]);
     cudaEventElapsedTime(&h->stats.ms_walk, h->ev[3], h->ev[4]);
     cudaEventElapsedTime(&h->stats.ms_total, h->ev[0], h->ev[4]);
+    h->stats.ms_sph = 0.0f;
+    if (h->resident && h->resident_gas) cudaEventElapsedTime(&h->stats.ms_sph, h->ev[4], h->ev[6]);
   }
   h->stats.leaf_interactions = ctl.stats[0];
   h->stats.far_interactions = ctl.stats[1];
@@ -520,7 +534,7 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
   cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
   for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&h->chunk_ev[i], cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaHostAlloc(&h->ctl_host, sizeof(DevCtl), cudaHostAllocDefault);
   if (e != cudaSuccess) {
@@ -538,6 +552,7 @@ void gx_destroy(gx_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_active(h);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+  sph_free(h->sph);
   h->ar.release();
   for (auto& e : h->chunk_ev)
     if (e) cudaEventDestroy(e);
@@ -834,10 +849,17 @@ int gx_direct_sum_f64(gx_handle* h, size_t n, const double* pos, const double* m
 }
 
 // ---- resident ----------------------------------------------------------------------
-int gx_upload(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass) {
-  if (!h) return GX_ERR_INVALID_ARG;
-  if (n && (!pos || !vel || !mass)) return fail(h, GX_ERR_INVALID_ARG, "null array");
+namespace {
+// GpuResidentLeapfrog::upload (gpu_resident.rs:1685-1800); `gas` (ascending global
+// indices) and u (per particle, nullable) put the state in gas mode.
+int upload_impl(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                const std::vector<uint32_t>* gas, const double* u) {
   cudaSetDevice(h->device);
+  if (h->resident_gas && h->step_graph) {  // captured with the SPH stages
+    cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
+  h->resident_gas = false;
   h->n = n;
   h->time = 0.0;
   h->pending_kick = false;
@@ -849,14 +871,35 @@ int gx_upload(gx_handle* h, size_t n, const double* pos, const double* vel, cons
   GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   GX_CK(h, cudaMemcpyAsync(b.vel, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  h->sph_host_hint_ngas = 0;
+  if (gas && !gas->empty()) {
+    // the gas map is rebuilt from the species at every upload (gpu_resident_sph.rs:170-194)
+    h->sph.gas_idx_host = *gas;
+    GX_CK(h, sph_reserve(h->sph, gas->size(), false, 0.0, h->stream));
+    if (u) {
+      std::vector<double> gu(gas->size());
+      for (size_t k = 0; k < gas->size(); ++k) gu[k] = u[(*gas)[k]];
+      GX_CK(h, cudaMemcpy(h->sph.gu, gu.data(), gu.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    h->resident_gas = true;
+  }
   if (n == 1) {
     GX_CK(h, cudaMemsetAsync(b.acc, 0, 3 * sizeof(double), h->stream));
+    if (h->resident_gas)
+      sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream);
     return finish(h, false);
   }
   // Prime a(x0) (gpu_resident.rs:1793-1799).
   enqueue_force(h, b, 0, 0, stats_on(h));
   h->stats.n = n;
   return finish(h, stats_on(h));
+}
+}  // namespace
+
+int gx_upload(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n && (!pos || !vel || !mass)) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  return upload_impl(h, n, pos, vel, mass, nullptr, nullptr);
 }
 
 namespace {
@@ -1286,6 +1329,281 @@ int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const d
     if (quad_out)
       for (int c = 0; c < 6; ++c) quad_out[6 * u + c] = u < n ? 0.0 : q64[6 * (u - n) + c];
   }
+  return GX_OK;
+}
+
+// ---- SPH on the gas subset ------------------------------------------------------------
+void gx_sph_default_params(gx_sph_params* out) {
+  if (!out) return;
+  out->n_ngb = 48.0;
+  out->h_tol_rel = 1e-3;
+  out->eos = GX_EOS_ISOTHERMAL;
+  out->warm_start = 1;
+  out->c_s = 1.0;
+  out->gamma = 5.0 / 3.0;
+  out->alpha = 1.0;
+  out->beta = 2.0;
+  out->visc_eps2 = 0.01;
+}
+
+namespace {
+
+// Species column -> gas map (ascending global index); kind values other than 0 / 1 are
+// rejected (core/src/state.rs:17-22 has two species).
+int gas_map(gx_handle* h, size_t n, const uint8_t* kind, std::vector<uint32_t>& gas) {
+  gas.clear();
+  if (!kind) return GX_OK;
+  for (size_t i = 0; i < n; ++i) {
+    if (kind[i] > 1) return fail(h, GX_ERR_INVALID_ARG, "kind must be 0 (collisionless) or 1 (gas)");
+    if (kind[i] == 1) gas.push_back(static_cast<uint32_t>(i));
+  }
+  return GX_OK;
+}
+
+int need_sph(gx_handle* h) {
+  if (!h->sph.enabled) return fail(h, GX_ERR_STATE, "SPH call without gas mode (gx_sph_enable)");
+  return GX_OK;
+}
+
+double dec_max_host(unsigned long long e) {
+  const unsigned long long b = (e >> 63) ? (e & 0x7FFFFFFFFFFFFFFFull) : ~e;
+  double d;
+  std::memcpy(&d, &b, sizeof d);
+  return d;
+}
+
+// The arena and gas map of a host-state SPH call on n particles whose gas rows are
+// `gas` (identity when gas is null): the resident state is dropped.
+int host_sph_setup(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                   const std::vector<uint32_t>* gas, bool keep_hint, bool host_s_est) {
+  h->resident = false;
+  h->resident_gas = false;
+  int rc = layout(h, n, 0.0);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  GX_CK(h, cudaMemcpyAsync(b.pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (vel) GX_CK(h, cudaMemcpyAsync(b.vel, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (mass) GX_CK(h, cudaMemcpyAsync(h->ar.mass_rw, mass, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (gas) {
+    h->sph.gas_idx_host = *gas;
+  } else {
+    h->sph.gas_idx_host.resize(n);
+    for (size_t i = 0; i < n; ++i) h->sph.gas_idx_host[i] = static_cast<uint32_t>(i);
+  }
+  const size_t ng = h->sph.gas_idx_host.size();
+  const double s_est = host_s_est ? sph_host_s_est(ng, pos, h->sph.gas_idx_host.data()) : 0.0;
+  GX_CK(h, sph_reserve(h->sph, ng, keep_hint, s_est, h->stream));
+  return GX_OK;
+}
+
+int put_gas(gx_handle* h, double* dst, const double* src, size_t count) {
+  if (src) GX_CK(h, cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return GX_OK;
+}
+
+}  // namespace
+
+int gx_sph_enable(gx_handle* h, const gx_sph_params* params) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (!params) return GX_OK;
+  const gx_sph_params& p = *params;
+  if (!(p.n_ngb > 32.0 / 3.0))
+    return fail(h, GX_ERR_INVALID_ARG, "n_ngb must exceed the self-term floor 32/3 (density.rs:172-176)");
+  if (!(p.h_tol_rel > 0.0) || (p.eos != GX_EOS_ISOTHERMAL && p.eos != GX_EOS_ADIABATIC) || !(p.c_s >= 0.0) ||
+      (p.eos == GX_EOS_ADIABATIC && !(p.gamma > 1.0)) || !(p.visc_eps2 >= 0.0))
+    return fail(h, GX_ERR_INVALID_ARG, "invalid gx_sph_params");
+  h->sph.p = p;
+  h->sph.enabled = true;
+  h->sph_host_hint_ngas = 0;
+  return GX_OK;
+}
+
+int gx_upload_species(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                      const uint8_t* kind, const double* u) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (n && (!pos || !vel || !mass)) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  std::vector<uint32_t> gas;
+  int rc = gas_map(h, n, kind, gas);
+  if (rc) return rc;
+  if (!h->sph.enabled || gas.empty()) return upload_impl(h, n, pos, vel, mass, nullptr, nullptr);
+  if (h->sph.p.eos != GX_EOS_ISOTHERMAL)
+    return fail(h, GX_ERR_INVALID_ARG, "the resident gas mode runs the isothermal EOS (u is not evolved)");
+  return upload_impl(h, n, pos, vel, mass, &gas, u);
+}
+
+int gx_gas_count(const gx_handle* h, size_t* n_gas_out) {
+  if (!h || !n_gas_out) return GX_ERR_INVALID_ARG;
+  *n_gas_out = h->resident_gas ? h->sph.n_gas : 0;
+  return GX_OK;
+}
+
+int gx_snapshot_gas_density(gx_handle* h, uint32_t* gas_idx_out, double* rho_out, double* h_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "no resident state");
+  if (!h->resident_gas) return GX_OK;
+  cudaSetDevice(h->device);
+  const size_t ng = h->sph.n_gas;
+  if (gas_idx_out) std::memcpy(gas_idx_out, h->sph.gas_idx_host.data(), ng * sizeof(uint32_t));
+  if (rho_out) GX_CK(h, cudaMemcpyAsync(rho_out, h->sph.rho, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (h_out) GX_CK(h, cudaMemcpyAsync(h_out, h->sph.hs, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_snapshot_gas_accel(gx_handle* h, double* acc_out, double* dudt_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "no resident state");
+  if (!h->resident_gas) return GX_OK;
+  cudaSetDevice(h->device);
+  const size_t ng = h->sph.n_gas;
+  if (acc_out)
+    GX_CK(h, cudaMemcpyAsync(acc_out, h->sph.gacc, 3 * ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (dudt_out)
+    GX_CK(h, cudaMemcpyAsync(dudt_out, h->sph.dudt, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_snapshot_accel(gx_handle* h, double* acc_out) { return gx_resident_accelerations(h, acc_out); }
+
+namespace {
+int resident_cfl(gx_handle* h, double c_cfl, double* dt_out, double* min_out) {
+  if (int rc = need_sph(h)) return rc;
+  if (!h->resident) return fail(h, GX_ERR_STATE, "no resident state");
+  if (!h->resident_gas || h->sph.n_gas == 0) {
+    if (min_out) *min_out = std::numeric_limits<double>::infinity();
+    return GX_OK;
+  }
+  cudaSetDevice(h->device);
+  apply_pending(h);  // the current velocities
+  const StepBufs& b = h->ar.b;
+  sph_enqueue_cfl(h->sph, b.pos, b.vel, c_cfl, false, b.ctl, h->stream);
+  unsigned long long enc = 0;
+  GX_CK(h, cudaMemcpyAsync(&enc, &h->sph.sc->min_dt_enc, sizeof enc, cudaMemcpyDeviceToHost, h->stream));
+  if (dt_out)
+    GX_CK(h, cudaMemcpyAsync(dt_out, h->sph.dtv, h->sph.n_gas * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  int rc = finish(h, false);
+  if (rc) return rc;
+  if (min_out) *min_out = -dec_max_host(enc);
+  return GX_OK;
+}
+}  // namespace
+
+int gx_min_stable_dt(gx_handle* h, double c_cfl, double* out) {
+  if (!h || !out) return GX_ERR_INVALID_ARG;
+  return resident_cfl(h, c_cfl, nullptr, out);
+}
+
+int gx_snapshot_gas_dt(gx_handle* h, double c_cfl, double* dt_out) {
+  if (!h || !dt_out) return GX_ERR_INVALID_ARG;
+  return resident_cfl(h, c_cfl, dt_out, nullptr);
+}
+
+int gx_sph_accelerations(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                         const uint8_t* kind, const double* u, double* acc_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (n == 0) return GX_OK;
+  if (!pos || !vel || !mass || !acc_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  std::vector<uint32_t> gas;
+  int rc = gas_map(h, n, kind, gas);
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  const bool keep = h->sph.p.warm_start && !gas.empty() && h->sph_host_hint_ngas == gas.size();
+  h->sph_host_hint_ngas = 0;
+  rc = host_sph_setup(h, n, pos, vel, mass, &gas, keep, true);
+  if (rc) return rc;
+  StepBufs& b = h->ar.b;
+  if (n == 1)
+    GX_CK(h, cudaMemsetAsync(b.acc, 0, 3 * sizeof(double), h->stream));
+  else
+    enqueue_force(h, b, 0, 0, stats_on(h));
+  if (!gas.empty()) {
+    if (u) {
+      std::vector<double> gu(gas.size());
+      for (size_t k = 0; k < gas.size(); ++k) gu[k] = u[gas[k]];
+      GX_CK(h, cudaMemcpy(h->sph.gu, gu.data(), gu.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream);
+  }
+  GX_CK(h, cudaMemcpyAsync(acc_out, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  h->stats.n = n;
+  rc = finish(h, stats_on(h));
+  if (rc == GX_OK) h->sph_host_hint_ngas = gas.size();
+  return rc;
+}
+
+int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,
+                   double* rho_out, double* h_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (n == 0) return GX_OK;
+  if (!pos || !mass || !rho_out || !h_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  cudaSetDevice(h->device);
+  h->sph_host_hint_ngas = 0;
+  int rc = host_sph_setup(h, n, pos, nullptr, mass, nullptr, false, true);
+  if (rc) return rc;
+  const int warm = h->sph.p.warm_start;
+  if (h_init) {
+    rc = put_gas(h, h->sph.hs, h_init, n);
+    if (rc) return rc;
+    const uint32_t one = 1u;
+    GX_CK(h, cudaMemcpyAsync(&h->sph.sc->hint_valid, &one, sizeof one, cudaMemcpyHostToDevice, h->stream));
+    h->sph.p.warm_start = 1;
+  }
+  const StepBufs& b = h->ar.b;
+  sph_enqueue_force(h->sph, b.pos, nullptr, b.mass, nullptr, true, false, b.ctl, h->stream);
+  h->sph.p.warm_start = warm;
+  GX_CK(h, cudaMemcpyAsync(rho_out, h->sph.rho, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaMemcpyAsync(h_out, h->sph.hs, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_sph_hydro(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                 const double* rho, const double* hsml, const double* u, double* acc_out, double* dudt_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (n == 0) return GX_OK;
+  if (!pos || !vel || !mass || !rho || !hsml || !acc_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  double h_max = 0.0;
+  for (size_t i = 0; i < n; ++i) h_max = std::fmax(h_max, hsml[i]);
+  if (!(h_max > 0.0) || !std::isfinite(h_max))
+    return fail(h, GX_ERR_INVALID_ARG, "hydro needs positive finite smoothing lengths (forces.rs:282-285)");
+  cudaSetDevice(h->device);
+  h->sph_host_hint_ngas = 0;
+  int rc = host_sph_setup(h, n, pos, vel, mass, nullptr, false, false);
+  if (rc) return rc;
+  if ((rc = put_gas(h, h->sph.rho, rho, n)) || (rc = put_gas(h, h->sph.hs, hsml, n)) || (rc = put_gas(h, h->sph.gu, u, n)))
+    return rc;
+  const StepBufs& b = h->ar.b;
+  sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, nullptr, false, true, b.ctl, h->stream);
+  GX_CK(h, cudaMemcpyAsync(acc_out, h->sph.gacc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (dudt_out) GX_CK(h, cudaMemcpyAsync(dudt_out, h->sph.dudt, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, false);
+}
+
+int gx_sph_cfl(gx_handle* h, size_t n, const double* pos, const double* vel, const double* hsml, const double* u,
+               double c_cfl, double* dt_out, double* min_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (n == 0) {
+    if (min_out) *min_out = std::numeric_limits<double>::infinity();
+    return GX_OK;
+  }
+  if (!pos || !vel || !hsml || !dt_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  cudaSetDevice(h->device);
+  h->sph_host_hint_ngas = 0;
+  int rc = host_sph_setup(h, n, pos, vel, nullptr, nullptr, false, false);
+  if (rc) return rc;
+  if ((rc = put_gas(h, h->sph.hs, hsml, n)) || (rc = put_gas(h, h->sph.gu, u, n))) return rc;
+  const StepBufs& b = h->ar.b;
+  sph_enqueue_cfl(h->sph, b.pos, b.vel, c_cfl, true, b.ctl, h->stream);
+  unsigned long long enc = 0;
+  GX_CK(h, cudaMemcpyAsync(&enc, &h->sph.sc->min_dt_enc, sizeof enc, cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaMemcpyAsync(dt_out, h->sph.dtv, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  rc = finish(h, false);
+  if (rc) return rc;
+  if (min_out) *min_out = -dec_max_host(enc);
   return GX_OK;
 }
 

@@ -43,6 +43,7 @@ constexpr uint32_t kErrLookbackTimeout = 1u << 0;
 constexpr uint32_t kErrStackOverflow = 1u << 1;
 constexpr uint32_t kErrBadIndex = 1u << 2;
 constexpr uint32_t kErrClimb = 1u << 3;
+constexpr uint32_t kErrSphIterations = 1u << 4;  // an SPH root-find ran past its iteration bound
 
 struct Agg64 {
   double mn[3];

@@ -80,6 +80,8 @@ typedef struct gx_stats {
   float ms_build;
   float ms_walk;
   float ms_total;
+  float ms_sph;            /* gas density + hydro + scatter (gas mode), CUDA events */
+  float pad;
 } gx_stats;
 
 /* ---- lifecycle ------------------------------------------------------------- */
@@ -164,6 +166,72 @@ int gx_get_stats(const gx_handle* h, gx_stats* out);
 /* Enqueue `steps` resident steps and return their device time in milliseconds
  * (CUDA events on the handle's stream around the steps). */
 int gx_step_many_timed(gx_handle* h, double dt, uint64_t steps, float* ms_out);
+
+/* ---- SPH on the gas subset (solvers/src/sph, gpu/src/gpu_resident.rs:1393-1660) ----
+ * Species: kind[i] == 1 is gas (core/src/state.rs:17-22 Species::Gas), 0 collisionless.
+ * Gravity acts on every particle; density, smoothing lengths and the hydro force on the
+ * gas rows only, as GravitySph (solvers/src/sph/gravity_sph.rs:172-207). The SPH stages
+ * run in FP64 in the reference's per-pair operation order; neighbour sums are reduced
+ * across a warp, so results agree with the reference to rounding (the CFL bound, a
+ * max/min, agrees bit for bit given the same h). */
+#define GX_EOS_ISOTHERMAL 0 /* P = c_s^2 rho */
+#define GX_EOS_ADIABATIC 1  /* P = (gamma - 1) rho u, c_s = sqrt(gamma (gamma - 1) u) */
+
+/* HydroParams (forces.rs:64-87) + DensityConfig (density.rs:33-51). */
+typedef struct gx_sph_params {
+  double n_ngb;      /* target kernel-weighted neighbour count (48) */
+  double h_tol_rel;  /* bisection tolerance on h (1e-3) */
+  int eos;           /* GX_EOS_* (resident gas mode: isothermal only) */
+  int warm_start;    /* seed each h bracket from the previous evaluation's h (GravitySph) */
+  double c_s;        /* isothermal sound speed (1.0) */
+  double gamma;      /* adiabatic index */
+  double alpha;      /* Monaghan viscosity, linear (1.0) */
+  double beta;       /* Monaghan viscosity, quadratic (2.0) */
+  double visc_eps2;  /* mu denominator regulariser (0.01) */
+} gx_sph_params;
+
+/* The reference defaults (n_ngb 48, tol 1e-3, isothermal c_s 1, alpha 1, beta 2,
+ * eps2 0.01, warm start on). */
+void gx_sph_default_params(gx_sph_params* out);
+/* GpuResidentLeapfrog::new_with_sph: put the handle in gas mode (params == NULL leaves
+ * it). Takes effect at the next gx_upload_species / force call. */
+int gx_sph_enable(gx_handle* h, const gx_sph_params* params);
+/* GpuResidentLeapfrog::upload of a State with species: kind[n] (NULL: no gas) and the
+ * internal energy u[n] (NULL: zero). Builds the gas map (ascending global index) and
+ * primes a(x0) = gravity(all) + hydro(gas). */
+int gx_upload_species(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                      const uint8_t* kind, const double* u);
+int gx_gas_count(const gx_handle* h, size_t* n_gas_out);
+/* snapshot_gas_density (gpu_resident.rs:1566): gas map, rho and h of the last force
+ * evaluation, in ascending gas index order (any pointer may be NULL). */
+int gx_snapshot_gas_density(gx_handle* h, uint32_t* gas_idx_out, double* rho_out, double* h_out);
+/* snapshot_gas_accel (gpu_resident.rs:1593): the hydro acceleration alone (before the
+ * scatter-add), acc_out[3 n_gas]; dudt_out[n_gas] (nullable) its du/dt partner. */
+int gx_snapshot_gas_accel(gx_handle* h, double* acc_out, double* dudt_out);
+/* snapshot_accel (gpu_resident.rs:1655): the full acceleration of every particle. */
+int gx_snapshot_accel(gx_handle* h, double* acc_out);
+/* min_stable_dt (gpu_resident.rs:1614; cfl.rs:49-125): min over gas of c_cfl h_i / v_sig,i
+ * reduced on the device, at the current velocities and the last evaluation's h;
+ * +inf without gas. snapshot_gas_dt (:1632): the per-gas vector, dt_out[n_gas]. */
+int gx_min_stable_dt(gx_handle* h, double c_cfl, double* out);
+int gx_snapshot_gas_dt(gx_handle* h, double c_cfl, double* dt_out);
+
+/* Host-state SPH (the resident state is replaced, as by gx_accelerations). */
+/* GravitySph::accelerations: gravity on all n, hydro added to the gas rows; h is
+ * warm-started across calls while the gas count is unchanged (params.warm_start). */
+int gx_sph_accelerations(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                         const uint8_t* kind, const double* u, double* acc_out);
+/* density_adaptive (density.rs:86-96) over n gas particles: rho_out[n], h_out[n];
+ * h_init[n] (nullable) seeds the brackets. */
+int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,
+                   double* rho_out, double* h_out);
+/* hydro_accel_and_dudt (forces.rs:160-172) with caller rho / h (u nullable). */
+int gx_sph_hydro(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                 const double* rho, const double* hsml, const double* u, double* acc_out, double* dudt_out);
+/* The per-particle CFL bound (cfl.rs:134-185 body) with caller h; *min_out (nullable)
+ * its minimum. */
+int gx_sph_cfl(gx_handle* h, size_t n, const double* pos, const double* vel, const double* hsml, const double* u,
+               double c_cfl, double* dt_out, double* min_out);
 
 /* ---- autotuning of the walk launch (no counterpart in the reference) -------------
  * The walk's block size and its scheduling (one warp per 32 targets over a grid, or a

@@ -2,14 +2,17 @@
 
 The oracle is a CPU f64 restatement of the galaxy reference's LBVH Barnes-Hut
 path (solvers/src/lbvh.rs, solvers/src/direct_sum.rs, solvers/src/potential.rs,
-core/src/integrator.rs, core/src/diagnostics.rs) in ``lbvh_oracle.cpp``.  Only
+core/src/integrator.rs, core/src/diagnostics.rs) in ``lbvh_oracle.cpp``, and of its
+SPH toolkit and gravity + SPH composite (solvers/src/sph/*.rs) in ``sph_oracle.cpp``.  Only
 ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
 it, always as the checker or the timed CPU baseline; the product library
 ``libgalaxy_b200.so`` never calls it.
 
 Parity pinning: the Morton bit-spreading is pinned by the reference's
 known-answer tests (solvers/src/lbvh.rs:691-726, in tests/golden/); the rest by
-the reference's invariant tests (solvers/tests/lbvh.rs:88-312). Bitwise identity
+the reference's invariant tests (solvers/tests/lbvh.rs:88-312). The SPH restatement
+is pinned by the reference's frozen output bits of hydro_accelerations
+(solvers/tests/sph_forces.rs:393-462) and max_stable_dt (solvers/tests/sph_cfl.rs:189-212). Bitwise identity
 with the Rust binary is unpinned beyond those (no Rust toolchain here).
 """
 
@@ -28,6 +31,7 @@ _lib = None
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 
 
 def build() -> None:
@@ -67,6 +71,24 @@ def lib():
             "or_fixture_masses": (None, [u64, sz, _f64p]),
             "or_fixture_random_codes": (None, [u64, sz, _u32p]),
             "or_openmp_max_threads": (i, []),
+            # SPH (sph_oracle.cpp)
+            "or_sph_w": (d, [d, d]),
+            "or_sph_grad_w": (None, [d, d, d, d, _f64p]),
+            "or_sph_neighbours": (sz, [sz, _f64p, d, _f64p, d, _u32p, sz]),
+            "or_sph_reference_density": (None, [sz, _f64p, _f64p, _f64p, _f64p]),
+            "or_sph_density_fixed": (None, [sz, _f64p, _f64p, _f64p, _f64p]),
+            "or_sph_density_adaptive": (None, [sz, _f64p, _f64p, d, d, C.c_void_p, _f64p, _f64p, i]),
+            "or_sph_density_seeds": (None, [sz, _f64p, d, _f64p, _f64p]),
+            "or_sph_hydro": (None, [sz, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, i, d, d, d, d, _f64p,
+                                    C.c_void_p, i]),
+            "or_sph_cfl_given_h": (None, [sz, _f64p, _f64p, _f64p, _f64p, i, d, d, _f64p, i]),
+            "or_sph_max_stable_dt": (d, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, i, d, d, d, d, C.c_void_p, i]),
+            "or_gravity_sph_accelerations": (i, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, d, d, d, i, d, d, d, d, d,
+                                                 d, C.c_void_p, C.c_void_p, C.c_void_p, _f64p, i]),
+            "or_kdk_gravity_sph": (i, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, d, d, d, i, d, d, d, d, d, d,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, _f64p, C.POINTER(C.c_int), d, u64, i]),
+            "or_fixture_gas_star_mix": (None, [u64, sz, sz, _f64p, _f64p, _f64p, _u8p]),
+            "or_fixture_sph_points": (None, [u64, sz, d, d, _f64p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -337,3 +359,184 @@ def per_particle_rel_err(approx, exact) -> np.ndarray:
     num = np.sqrt(np.sum((approx - exact) ** 2, axis=1))
     den = np.maximum(np.sqrt(np.sum(exact * exact, axis=1)), 1e-300)
     return num / den
+
+
+# ---- SPH (solvers/src/sph) -------------------------------------------------------------
+SPH_DEFAULTS = dict(n_ngb=48.0, h_tol_rel=1e-3, eos=0, eos_param=1.0, alpha=1.0, beta=2.0, visc_eps2=0.01)
+
+
+def _sph(kw):
+    p = dict(SPH_DEFAULTS)
+    p.update(kw)
+    return p
+
+
+def sph_w(r: float, h: float) -> float:
+    """kernel.rs:27-38."""
+    return lib().or_sph_w(float(r), float(h))
+
+
+def sph_grad_w(r_ij, h: float) -> np.ndarray:
+    """kernel.rs:40-53."""
+    out = np.zeros(3)
+    lib().or_sph_grad_w(float(r_ij[0]), float(r_ij[1]), float(r_ij[2]), float(h), out)
+    return out
+
+
+def sph_neighbours(pos, center, r: float, cell: float = 0.0) -> np.ndarray:
+    """HashGrid::neighbours_within (grid.rs:57-82) with cells of edge `cell`, or the
+    brute-force reference_neighbours (reference.rs:10-18) when cell <= 0."""
+    pos = _pos(pos)
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    cap = pos.shape[0]
+    out = np.zeros(max(cap, 1), dtype=np.uint32)
+    k = lib().or_sph_neighbours(pos.shape[0], pos.reshape(-1), float(cell), c, float(r), out, cap)
+    return out[:k].copy()
+
+
+def sph_reference_density(pos, mass, h) -> np.ndarray:
+    pos = _pos(pos)
+    out = np.zeros(pos.shape[0])
+    lib().or_sph_reference_density(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                                   np.ascontiguousarray(h, np.float64), out)
+    return out
+
+
+def sph_density_fixed(pos, mass, h) -> np.ndarray:
+    pos = _pos(pos)
+    out = np.zeros(pos.shape[0])
+    lib().or_sph_density_fixed(pos.shape[0], pos.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                               np.ascontiguousarray(h, np.float64), out)
+    return out
+
+
+def sph_density_adaptive(pos, mass, n_ngb=48.0, h_tol_rel=1e-3, h_init=None, threads: int = 0):
+    """density_adaptive (density.rs:86-96): (rho, h)."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    rho, h = np.zeros(n), np.zeros(n)
+    hi = None if h_init is None else np.ascontiguousarray(h_init, dtype=np.float64)
+    lib().or_sph_density_adaptive(n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), float(n_ngb),
+                                  float(h_tol_rel), None if hi is None else hi.ctypes.data, rho, h,
+                                  threads or max_threads())
+    return rho, h
+
+
+def sph_density_seeds(pos, n_ngb=48.0):
+    """The per-particle bracket seeds and the cap of DensitySetup::new (density.rs:166-220)."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    seeds, sc = np.zeros(n), np.zeros(4)
+    lib().or_sph_density_seeds(n, pos.reshape(-1), float(n_ngb), seeds, sc)
+    return seeds, float(sc[0])
+
+
+def sph_hydro(pos, vel, mass, rho, h, u=None, threads: int = 0, **kw):
+    """hydro_accel_and_dudt (forces.rs:160-172): (acc [n,3], dudt [n])."""
+    p = _sph(kw)
+    pos, vel = _pos(pos), _pos(vel)
+    n = pos.shape[0]
+    acc, dudt = np.zeros((n, 3)), np.zeros(n)
+    uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+    lib().or_sph_hydro(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                       np.ascontiguousarray(rho, np.float64), np.ascontiguousarray(h, np.float64), uu,
+                       int(p["eos"]), float(p["eos_param"]), float(p["alpha"]), float(p["beta"]),
+                       float(p["visc_eps2"]), acc.reshape(-1), dudt.ctypes.data, threads or max_threads())
+    return acc, dudt
+
+
+def sph_cfl_given_h(gpos, gvel, h, c_cfl, u=None, threads: int = 0, **kw) -> np.ndarray:
+    """The per-particle CFL bound of cfl.rs:67-121 over a gas subset with given h."""
+    p = _sph(kw)
+    gpos, gvel = _pos(gpos), _pos(gvel)
+    n = gpos.shape[0]
+    out = np.zeros(n)
+    uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+    lib().or_sph_cfl_given_h(n, gpos.reshape(-1), gvel.reshape(-1), np.ascontiguousarray(h, np.float64), uu,
+                             int(p["eos"]), float(p["eos_param"]), float(c_cfl), out, threads or max_threads())
+    return out
+
+
+def sph_max_stable_dt(pos, vel, mass, kind, c_cfl, u=None, per_particle: bool = False, threads: int = 0, **kw):
+    """max_stable_dt (cfl.rs:49-125); with per_particle, also the state-indexed vector of
+    max_stable_dt_per_particle (cfl.rs:134-185)."""
+    p = _sph(kw)
+    pos, vel = _pos(pos), _pos(vel)
+    n = pos.shape[0]
+    uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+    vec = np.zeros(n) if per_particle else None
+    m = lib().or_sph_max_stable_dt(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                                   np.ascontiguousarray(kind, np.uint8), uu, int(p["eos"]), float(p["eos_param"]),
+                                   float(p["n_ngb"]), float(p["h_tol_rel"]), float(c_cfl),
+                                   None if vec is None else vec.ctypes.data, threads or max_threads())
+    return (m, vec) if per_particle else m
+
+
+class GravitySph:
+    """GravitySph (gravity_sph.rs:24-207) over the Lbvh gravity solver: gravity on every
+    particle, hydro on the gas rows (kind == 1), h warm-started across calls. g <= 0
+    turns gravity off (the reference's hydro_only)."""
+
+    def __init__(self, g, softening, theta, threads: int = 0, **kw):
+        self.g, self.softening, self.theta = g, softening, theta
+        self.p = _sph(kw)
+        self.threads = threads or max_threads()
+        self.h_hint = None
+        self.h_valid = C.c_int(0)
+        self.rho = None
+        self.acc = None
+        self.primed = C.c_int(0)
+
+    def _hint(self, n_gas):
+        if self.h_hint is None or self.h_hint.shape[0] != n_gas:
+            self.h_hint = np.zeros(max(n_gas, 1))
+            self.rho = np.zeros(max(n_gas, 1))
+            self.h_valid = C.c_int(0)
+
+    def _args(self):
+        p = self.p
+        return (float(self.g), float(self.softening), float(self.theta), int(p["eos"]), float(p["eos_param"]),
+                float(p["alpha"]), float(p["beta"]), float(p["visc_eps2"]), float(p["n_ngb"]), float(p["h_tol_rel"]))
+
+    def accelerations(self, pos, vel, mass, kind, u=None) -> np.ndarray:
+        pos, vel = _pos(pos), _pos(vel)
+        n = pos.shape[0]
+        kind = np.ascontiguousarray(kind, np.uint8)
+        self._hint(int((kind == 1).sum()))
+        acc = np.zeros((n, 3))
+        uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        lib().or_gravity_sph_accelerations(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                                           kind, uu, *self._args(), self.h_hint.ctypes.data,
+                                           C.addressof(self.h_valid), self.rho.ctypes.data, acc.reshape(-1),
+                                           self.threads)
+        return acc
+
+    def step_many(self, pos, vel, mass, kind, dt, steps, u=None):
+        """LeapfrogKdk (integrator.rs:38-78) driving this composite, in place."""
+        n = pos.shape[0]
+        kind = np.ascontiguousarray(kind, np.uint8)
+        self._hint(int((kind == 1).sum()))
+        if self.acc is None or self.acc.shape[0] != n:
+            self.acc = np.zeros((n, 3))
+            self.primed = C.c_int(0)
+        uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        lib().or_kdk_gravity_sph(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64), kind, uu,
+                                 *self._args(), self.h_hint.ctypes.data, C.addressof(self.h_valid),
+                                 self.rho.ctypes.data, self.acc.reshape(-1), C.byref(self.primed), float(dt),
+                                 int(steps), self.threads)
+
+
+def fixture_gas_star_mix(seed: int, n_gas: int, n_star: int):
+    """gpu/tests/gpu_resident_sph.rs:38-96: (pos, vel, mass, kind), gas interleaved."""
+    n = n_gas + n_star
+    pos, vel, mass, kind = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(n, dtype=np.uint8)
+    lib().or_fixture_gas_star_mix(seed, n_gas, n_star, pos.reshape(-1), vel.reshape(-1), mass, kind)
+    return pos, vel, mass, kind
+
+
+def fixture_sph_points(seed: int, n: int, scale: float, centered: bool = True) -> np.ndarray:
+    """The SPH tests' random_points: (u - 0.5) * scale when centered (sph_forces.rs:18-29,
+    sph_cfl.rs:10-21), u * scale otherwise (sph_density.rs:15-27)."""
+    pos = np.zeros((n, 3))
+    lib().or_fixture_sph_points(seed, n, float(scale), 0.5 if centered else 0.0, pos.reshape(-1))
+    return pos

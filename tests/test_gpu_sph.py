@@ -1,0 +1,296 @@
+"""SPH on the gas subset through the C ABI against the oracle's restatement of the
+reference (solvers/src/sph/*.rs, gpu/tests/gpu_resident_sph.rs gates, restated).
+
+Tolerances: the SPH stages are FP64 in the reference's per-pair operation order, but
+neighbour sums are warp reductions instead of the reference's ascending serial sums, so
+density, h and the hydro force agree to rounding: relative 1e-12 per particle for rho / h
+(an h can move within the bisection tolerance when a rounding difference flips one
+bisection comparison: at most 1 in 1e4 particles, within 2 h_tol), and 1e-10 of the
+RMS acceleration for the hydro force. The CFL bound (a max over pairs, a min over
+targets) is compared bit for bit given the same h. The reference's own GPU gates are
+f32 (1e-3)."""
+
+import json
+import os
+import struct
+
+import numpy as np
+import pytest
+
+import galaxy_b200 as gb
+
+pytestmark = pytest.mark.gpu
+
+PINS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "sph_pins.json")))
+
+
+def f64(h: str) -> float:
+    return struct.unpack("<d", struct.pack("<Q", int(h, 16)))[0]
+
+
+def rel(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+def assert_density_close(rho, h, rho_ref, h_ref, tol=1e-12):
+    rh, rr = rel(h, h_ref), rel(rho, rho_ref)
+    bad = (rh > tol) | (rr > tol)
+    assert bad.sum() <= max(1, h.size // 10000), f"{bad.sum()} particles off (max h {rh.max():.2e}, rho {rr.max():.2e})"
+    assert rh.max() <= 2e-3 and rr.max() <= 8e-3
+
+
+def mix_state(oracle, seed, n_gas, n_star):
+    pos, vel, mass, kind = oracle.fixture_gas_star_mix(seed, n_gas, n_star)
+    return gb.State(pos, vel, mass, kind=kind)
+
+
+@pytest.fixture(scope="module")
+def solver():
+    return gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+
+
+def test_density_matches_oracle(oracle, solver):
+    # solvers/tests/sph_density.rs:135-146 cloud, masses 1 + i % 3.
+    pos = oracle.fixture_sph_points(33, 1500, 2.0, centered=False)
+    mass = np.array([1.0 + (i % 3) for i in range(1500)])
+    rho, h = solver.density(pos, mass)
+    rho_ref, h_ref = oracle.sph_density_adaptive(pos, mass)
+    assert_density_close(rho, h, rho_ref, h_ref)
+    rho2, h2 = solver.density(pos, mass)
+    assert np.array_equal(rho, rho2) and np.array_equal(h, h2)  # deterministic
+
+
+def test_density_warm_start_matches_oracle(oracle, solver):
+    pos = oracle.fixture_sph_points(77, 1000, 1.5, centered=False)
+    mass = np.full(1000, 0.7)
+    _, h_cold = oracle.sph_density_adaptive(pos, mass)
+    hint = 1.5 * h_cold
+    rho, h = solver.density(pos, mass, h_init=hint)
+    rho_ref, h_ref = oracle.sph_density_adaptive(pos, mass, h_init=hint)
+    assert_density_close(rho, h, rho_ref, h_ref)
+
+
+def test_density_clustered_and_underpopulated(oracle, solver):
+    # a centrally concentrated cloud (wide h range, mixed occupancy bins) and n = 1..3
+    st = gb.ic.plummer(20000, 3)
+    rho, h = solver.density(st.pos, st.mass)
+    rho_ref, h_ref = oracle.sph_density_adaptive(st.pos, st.mass)
+    assert_density_close(rho, h, rho_ref, h_ref)
+    for n in (1, 2, 3):
+        pos = oracle.fixture_sph_points(n + 1, n, 1.0, centered=False)
+        rho, h = solver.density(pos, np.ones(n))
+        rho_ref, h_ref = oracle.sph_density_adaptive(pos, np.ones(n))
+        assert np.all(np.isfinite(h)) and np.all(h > 0) and np.all(rho > 0)
+        assert np.allclose(h, h_ref, rtol=1e-12) and np.allclose(rho, rho_ref, rtol=1e-12)
+
+
+def test_hydro_matches_frozen_pin_case(oracle, solver):
+    p = PINS["hydro_isothermal_8"]
+    n = p["n"]
+    pos = oracle.fixture_sph_points(p["pos_seed"], n, p["pos_scale"])
+    vel = oracle.fixture_sph_points(p["vel_seed"], n, p["vel_scale"])
+    mass = np.array([1.0 + i * 0.1 for i in range(n)])
+    rho = np.array([0.8 + i * 0.05 for i in range(n)])
+    h = np.array([0.9 + i * 0.03 for i in range(n)])
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, sph=dict(c_s=p["c_s"]))
+    acc, _ = s.hydro(pos, vel, mass, rho, h)
+    want = np.array([[f64(b) for b in row] for row in p["acc_bits"]])
+    assert np.max(np.abs(acc - want)) <= 1e-13 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("eos", ["isothermal", "adiabatic"])
+def test_hydro_matches_oracle(oracle, eos):
+    pos = oracle.fixture_sph_points(9, 3000, 2.0)
+    vel = oracle.fixture_sph_points(10, 3000, 0.8)
+    mass = 0.5 + np.random.default_rng(1).random(3000)
+    u = 0.5 + np.random.default_rng(2).random(3000)
+    kw = dict(eos=eos, gamma=5.0 / 3.0, c_s=1.1)
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, sph=kw)
+    rho, h = oracle.sph_density_adaptive(pos, mass)
+    acc, dudt = s.hydro(pos, vel, mass, rho, h, u)
+    ref, dref = oracle.sph_hydro(pos, vel, mass, rho, h, u, eos=0 if eos == "isothermal" else 1,
+                                 eos_param=1.1 if eos == "isothermal" else 5.0 / 3.0)
+    scale = np.sqrt(np.mean(np.sum(ref * ref, axis=1)))
+    assert np.max(np.abs(acc - ref)) <= 1e-10 * scale
+    assert np.max(np.abs(dudt - dref)) <= 1e-10 * np.sqrt(np.mean(dref * dref))
+
+
+def test_hydro_momentum_is_conserved(oracle, solver):
+    pos = oracle.fixture_sph_points(17, 2000, 2.0)
+    pos[:1000] *= 0.3  # non-uniform h: asymmetric couplings exist
+    vel = oracle.fixture_sph_points(18, 2000, 0.5)
+    mass = np.full(2000, 0.8)
+    rho, h = solver.density(pos, mass)
+    acc, _ = solver.hydro(pos, vel, mass, rho, h)
+    scale = np.sum(mass[:, None] * np.abs(acc))
+    assert np.linalg.norm((mass[:, None] * acc).sum(axis=0)) < 1e-12 * scale
+
+
+@pytest.mark.parametrize("eos", ["isothermal", "adiabatic"])
+def test_cfl_bit_exact_given_h(oracle, eos):
+    pos = oracle.fixture_sph_points(21, 600, 2.5)
+    vel = oracle.fixture_sph_points(22, 600, 1.5)
+    u = 0.2 + np.random.default_rng(3).random(600)
+    _, h = oracle.sph_density_adaptive(pos, np.ones(600))
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, sph=dict(eos=eos, gamma=1.4))
+    dt, m = s.cfl(pos, vel, h, 0.25, u)
+    ref = oracle.sph_cfl_given_h(pos, vel, h, 0.25, u, eos=0 if eos == "isothermal" else 1,
+                                 eos_param=1.0 if eos == "isothermal" else 1.4)
+    assert np.array_equal(dt, ref) and m == ref.min()
+
+
+def test_cfl_pin_through_the_gpu_density(solver, oracle):
+    # solvers/tests/sph_cfl.rs:189-212 end to end on the GPU: density then CFL.
+    p = PINS["cfl_isothermal_600"]
+    pos = oracle.fixture_sph_points(p["pos_seed"], p["n"], p["pos_scale"])
+    vel = oracle.fixture_sph_points(p["vel_seed"], p["n"], p["vel_scale"])
+    st = gb.State(pos, vel, np.ones(p["n"]), kind=np.ones(p["n"], np.uint8))
+    got = solver.max_stable_dt(st, c_cfl=p["c_cfl"])
+    assert abs(got - f64(p["min_dt_bits"])) <= 1e-12 * f64(p["min_dt_bits"])
+
+
+def test_gravity_sph_matches_oracle_composite(oracle):
+    st = mix_state(oracle, 0xA5F0, 1200, 2400)
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    acc = s.accelerations(st)
+    ref = oracle.GravitySph(1.0, 0.05, 0.5).accelerations(st.pos, st.vel, st.mass, st.kind)
+    stars = st.kind == 0
+    assert np.array_equal(acc[stars], ref[stars])  # FP64 gravity: bit-exact
+    err = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert err.max() < 1e-10
+    # the warm-started second call (GravitySph keeps h as the next bracket seed)
+    g2 = oracle.GravitySph(1.0, 0.05, 0.5)
+    g2.accelerations(st.pos, st.vel, st.mass, st.kind)
+    ref2 = g2.accelerations(st.pos, st.vel, st.mass, st.kind)
+    acc2 = s.accelerations(st)
+    assert (np.linalg.norm(acc2 - ref2, axis=1) / np.linalg.norm(ref2, axis=1)).max() < 1e-10
+
+
+def test_resident_gas_density_matches_oracle(oracle):
+    # gpu/tests/gpu_resident_sph.rs:138-170 (there f32, 1e-3; here FP64)
+    st = mix_state(oracle, 0xA5F0, 120, 240)
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5)
+    r.upload(st)
+    gd = r.snapshot_gas_density()
+    assert np.array_equal(gd.gas_idx, st.gas())
+    gas = st.gas()
+    rho_ref, h_ref = oracle.sph_density_adaptive(st.pos[gas], st.mass[gas])
+    assert_density_close(gd.rho, gd.h, rho_ref, h_ref)
+
+
+def test_resident_gas_map_rebuilt_on_reupload(oracle):
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5)
+    a = mix_state(oracle, 0x1111, 80, 160)
+    r.upload(a)
+    assert np.array_equal(r.snapshot_gas_density().gas_idx, a.gas())
+    b = mix_state(oracle, 0x2222, 100, 100)
+    r.upload(b)
+    assert np.array_equal(r.snapshot_gas_density().gas_idx, b.gas())
+    r.step_many(1e-3, 3)  # the step graph is recaptured for the new gas map
+    assert np.all(np.isfinite(r.snapshot().pos))
+
+
+def test_resident_hydro_accel_matches_oracle(oracle):
+    # gpu_resident_sph.rs:398-437: resident gas_acc vs the oracle fed the device's rho / h
+    st = mix_state(oracle, 0xBEEF, 2000, 4000)
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5)
+    r.upload(st)
+    gd = r.snapshot_gas_density()
+    acc, dudt = r.snapshot_gas_accel(with_dudt=True)
+    gas = st.gas()
+    ref, dref = oracle.sph_hydro(st.pos[gas], st.vel[gas], st.mass[gas], gd.rho, gd.h)
+    scale = np.sqrt(np.mean(np.sum(ref * ref, axis=1)))
+    assert np.max(np.abs(acc - ref)) <= 1e-10 * scale
+
+
+def test_resident_scatter_composition(oracle):
+    # gpu_resident_sph.rs:488-522: star rows untouched, gas rows = gravity + gas_acc
+    st = mix_state(oracle, 0x5EED, 1500, 3000)
+    g_only = gb.GpuResidentLeapfrog(1.0, 0.05, 0.5)
+    g_only.upload(st)
+    a0 = g_only.snapshot_accel()
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5)
+    r.upload(st)
+    a1 = r.snapshot_accel()
+    gas = st.gas()
+    stars = st.kind == 0
+    assert np.array_equal(a1[stars], a0[stars])
+    assert np.array_equal(a1[gas], a0[gas] + r.snapshot_gas_accel())
+
+
+def test_resident_trajectory_matches_oracle_kdk(oracle):
+    # LeapfrogKdk driving GravitySph (warm-started h) vs the resident gas mode, FP64 gravity
+    st = mix_state(oracle, 0xC0DE, 1000, 2000)
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5, precision="f64")
+    r.upload(st)
+    r.step_many(2e-3, 6)
+    snap = r.snapshot()
+    pos, vel = st.pos.copy(), st.vel.copy()
+    og = oracle.GravitySph(1.0, 0.05, 0.5)
+    og.step_many(pos, vel, st.mass, st.kind, 2e-3, 6)
+    assert np.max(np.abs(snap.pos - pos)) <= 1e-10 * np.max(np.abs(pos))
+    assert np.max(np.abs(snap.vel - vel)) <= 1e-9 * np.max(np.abs(vel))
+    gd = r.snapshot_gas_density()
+    assert_density_close(gd.rho, gd.h, og.rho[:gd.rho.size], og.h_hint[:gd.h.size], tol=1e-10)
+
+
+def test_resident_cfl(oracle):
+    # gpu_resident_sph.rs:717-800: the device min and per-gas vector; here bit-exact given
+    # the device's h at the snapshot state, and close to the cold-start CPU bound.
+    st = mix_state(oracle, 0xA5F0, 400, 800)
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5)
+    r.upload(st)
+    r.step_many(1e-3, 4)
+    m = r.min_stable_dt(0.25)
+    gc = r.snapshot_gas_dt(0.25)
+    snap = r.snapshot()
+    gd = r.snapshot_gas_density()
+    gas = st.gas()
+    ref = oracle.sph_cfl_given_h(snap.pos[gas], snap.vel[gas], gd.h, 0.25)
+    assert np.array_equal(gc.dt, ref) and m == ref.min()
+    cold = oracle.sph_max_stable_dt(snap.pos, snap.vel, snap.mass, snap.kind, 0.25)
+    assert abs(m - cold) <= 2e-3 * cold
+
+
+def test_resident_without_gas(oracle):
+    st = mix_state(oracle, 0xA5F0, 120, 240)
+    st.kind[:] = 0
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.05, 0.5)
+    r.upload(st)
+    assert r.gas_count() == 0 and r.min_stable_dt(0.25) == np.inf
+    g = gb.GpuResidentLeapfrog(1.0, 0.05, 0.5)
+    g.upload(st)
+    assert np.array_equal(r.snapshot_accel(), g.snapshot_accel())
+
+
+def test_resident_gas_mode_large_properties(oracle):
+    # 262,144 gas particles in a uniform cube inside a Plummer sphere of as many stars: the
+    # density hits the target count (checked on a sample against brute force) and the
+    # hydro momentum sum is roundoff (equal gas masses).
+    stars = gb.ic.plummer(262144, 11)
+    rng = np.random.default_rng(5)
+    gpos = rng.uniform(-1.0, 1.0, (262144, 3))
+    gvel = rng.normal(0.0, 0.1, (262144, 3))
+    pos = np.empty((524288, 3))
+    vel = np.empty((524288, 3))
+    pos[0::2], pos[1::2] = gpos, stars.pos
+    vel[0::2], vel[1::2] = gvel, stars.vel
+    kind = np.zeros(524288, np.uint8)
+    kind[0::2] = 1
+    st = gb.State(pos, vel, np.full(524288, 1.0 / 524288), kind=kind)
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, 0.01, 0.5)
+    r.upload(st)
+    gd = r.snapshot_gas_density()
+    gas = st.gas()
+    gpos = st.pos[gas]
+    rng = np.random.default_rng(0)
+    for k in rng.choice(gas.size, 64, replace=False):
+        d = np.linalg.norm(gpos[k] - gpos, axis=1)
+        hk = gd.h[k]
+        near = d < 2 * hk
+        n = (4 * np.pi / 3) * (2 * hk) ** 3 * sum(oracle.sph_w(x, hk) for x in d[near])
+        assert abs(n - 48.0) <= 1.0
+    acc = r.snapshot_gas_accel()
+    m = st.mass[gas]
+    scale = np.sum(m[:, None] * np.abs(acc))
+    assert np.linalg.norm((m[:, None] * acc).sum(axis=0)) < 1e-10 * scale
