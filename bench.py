@@ -9,7 +9,7 @@ aggregation, tree walk). The state plus tree (~330 MB) is larger than the 126 MB
 L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config collision|plummer|batched|serving]
+                    [--config collision|plummer|batched|serving|precision|sph]
 
 Under torchrun each rank steps its own replica (a single system does not shard:
 replicas only) and value = all ranks' particle-steps / max-over-ranks device time.
@@ -516,13 +516,116 @@ def run_precision(args):
         dist.destroy_process_group()
 
 
+def run_sph(args):
+    """Resident gas mode (GpuResidentLeapfrog::new_with_sph, gpu_resident.rs:1393-1565):
+    a gas blob of --gas particles inside a field of as many stars. Each step: KDK with
+    gravity on every particle, then FP64 adaptive-h density, hydro force and the
+    scatter-add on the gas rows. Device time over CUDA-graph replays; stage times of
+    eager steps; e2e through GravitySph on host arrays (LeapfrogKdk in numpy); the CPU
+    baseline is the oracle's GravitySph on a bounded 131,072-particle mix."""
+    import galaxy_b200 as gb
+    from galaxy_b200 import workloads
+
+    dist, rank, ws, local = ranks.init()
+    ng = args.gas
+    st = workloads.gas_star_mix(ng, ng, seed=rank)
+    n = len(st)
+    eps, theta, dt = 0.01, 0.5, 1e-4
+    peaks = _peaks()
+    r = gb.GpuResidentLeapfrog.new_with_sph(1.0, eps, theta, device=local)
+    r.upload(st)
+    r.step_many(dt, args.warmup)
+    tune = r.autotune(repeats=3)
+    r.step_many(dt, 1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    gb.device_synchronize(local)
+    ranks.barrier(dist, local)
+    ms = r.step_many_timed(dt, args.steps)
+    gb.device_synchronize(local)
+    ranks.barrier(dist, local)
+    clk = clocks.stop()
+    ms_max = ranks.max_over_ranks(dist, ms, local)
+    value = n * ws * args.steps / (ms_max / 1e3)
+    cfl = r.min_stable_dt(0.25)
+
+    rs = gb.GpuResidentLeapfrog.new_with_sph(1.0, eps, theta, device=local, stage_times=True)
+    rs.upload(st)
+    keys = ("ms_bbox_morton", "ms_sort", "ms_build", "ms_walk", "ms_sph", "ms_sph_density")
+    stage = dict.fromkeys(keys, 0.0)
+    k_st = max(1, min(args.steps, 5))
+    rs.step(dt)
+    for _ in range(k_st):
+        rs.step(dt)
+        sd = rs.stats()
+        for k in keys:
+            stage[k] += sd[k] / k_st
+    del rs
+
+    # e2e: GravitySph on host arrays driven by LeapfrogKdk (copies each step)
+    host = st.copy()
+    solver = gb.GpuGravitySph(1.0, eps, theta, device=local)
+    kdk = gb.LeapfrogKdk()
+    kdk.step(host, solver, dt)
+    k_e2e = max(1, min(args.steps, 5))
+    gb.device_synchronize(local)
+    ranks.barrier(dist, local)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        kdk.step(host, solver, dt)
+    t_e2e = ranks.max_over_ranks(dist, time.perf_counter() - t0, local)
+    e2e = {"value": n * ws * k_e2e / t_e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 57 * n,
+           "d2h_bytes_per_step": 24 * n, "steps": k_e2e,
+           "path": "LeapfrogKdk (numpy kicks) + GpuGravitySph.accelerations on host arrays "
+                   "(upload pos, vel, mass, kind, u; download acc)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle
+
+        threads = os.cpu_count() or 1
+        sample = workloads.gas_star_mix(65_536, 65_536, seed=7)
+        gs = oracle.GravitySph(1.0, eps, theta, threads=threads)
+        t0 = time.perf_counter()
+        gs.accelerations(sample.pos, sample.vel, sample.mass, sample.kind)
+        t = time.perf_counter() - t0
+        cpu = {"value": len(sample) / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"one GravitySph force evaluation (Lbvh gravity + adaptive-h density + hydro) of a "
+                         f"131072-particle mix (65536 gas), {threads} threads, per particle (oracle C++ "
+                         f"restatement)"}
+    if rank == 0:
+        gas_frac = stage["ms_sph"] / max(ms_max / args.steps, 1e-9)
+        line = {"metric": "particle-steps/s (resident KDK step with SPH on the gas subset)", "value": value,
+                "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 (SPH), f32 (gravity walk)", "data": "synthetic",
+                "config": {"workload": f"gas-star-mix-{ng}+{ng}", "particles_per_gpu": n, "gas": ng, "eps": eps,
+                           "theta": theta, "dt": dt, "sph": "isothermal c_s 1, n_ngb 48, h_tol 1e-3, alpha 1, "
+                                                        "beta 2, warm-started h",
+                           "parallelism": "replicas" if ws > 1 else "single system", "cuda_graph": True,
+                           "l2": f"working set ~{900 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)",
+                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}},
+                "gas_particle_steps_per_s": ng * ws * args.steps / (ms_max / 1e3),
+                "e2e": e2e, "gpu_launches": None, "cpu_baseline": cpu, "clocks": clk, "stage_ms": stage,
+                "sph_share_of_step": gas_frac, "min_stable_dt_c0.25": cfl,
+                "roofline": {"kernel": "k_sph_density (adaptive-h root-find)", "bound": "issue",
+                             "note": "FP64 per-pair arithmetic with warp reductions; see profiles/ "
+                                     "k_sph_density_uniform_262144.md for the instruction and pipe counters",
+                             "peak_source": peaks.get("sm_max_mhz") and "clocks.max.sm" or "nominal 1965 MHz"}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="collision", choices=["collision", "plummer", "batched", "serving", "precision"])
+    ap.add_argument("--config", default="collision",
+                    choices=["collision", "plummer", "batched", "serving", "precision", "sph"])
+    ap.add_argument("--gas", type=int, default=1 << 20, help="sph: gas particles (and as many stars)")
     ap.add_argument("--systems", type=int, default=256, help="batched: number of systems")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
     ap.add_argument("--horizon", type=float, default=60.0, help="serving: seconds to serve")
@@ -539,6 +642,8 @@ def main():
         run_serving(args)
     elif args.config == "precision":
         run_precision(args)
+    elif args.config == "sph":
+        run_sph(args)
     else:
         run_ours(args)
 

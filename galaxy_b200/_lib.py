@@ -65,7 +65,7 @@ class Stats(C.Structure):
         ("ms_walk", C.c_float),
         ("ms_total", C.c_float),
         ("ms_sph", C.c_float),
-        ("pad", C.c_float),
+        ("ms_sph_density", C.c_float),
     ]
 
 

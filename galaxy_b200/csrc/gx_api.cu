@@ -273,7 +273,7 @@ struct gx_handle {
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[7] = {};  // stage boundaries; [5] gx_step_many_timed, [6] end of SPH
+  cudaEvent_t ev[8] = {};  // stage boundaries; [5] gx_step_many_timed, [6] end of SPH, [7] end of its density
   cudaEvent_t chunk_ev[8] = {};  // gx_kdk_step_host: acceleration chunks copied back
   DevCtl* ctl_host = nullptr;     // pinned copy of the device error word
   std::string err;
@@ -417,7 +417,7 @@ void enqueue_force(gx_handle* h, const StepBufs& b, int kick, int pending, bool 
   if (timed) cudaEventRecord(h->ev[4], h->stream);
   if (h->resident && h->resident_gas) {
     NvtxRange g("gx.sph");
-    sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream);
+    sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream, timed ? h->ev[7] : nullptr);
     if (timed) cudaEventRecord(h->ev[6], h->stream);
   }
   h->launches += 1;
@@ -436,8 +436,11 @@ int finish(gx_handle* h, bool timed) {
     cudaEventElapsedTime(&h->stats.ms_build, h->ev[2], h->ev[3]);
     cudaEventElapsedTime(&h->stats.ms_walk, h->ev[3], h->ev[4]);
     cudaEventElapsedTime(&h->stats.ms_total, h->ev[0], h->ev[4]);
-    h->stats.ms_sph = 0.0f;
-    if (h->resident && h->resident_gas) cudaEventElapsedTime(&h->stats.ms_sph, h->ev[4], h->ev[6]);
+    h->stats.ms_sph = h->stats.ms_sph_density = 0.0f;
+    if (h->resident && h->resident_gas) {
+      cudaEventElapsedTime(&h->stats.ms_sph, h->ev[4], h->ev[6]);
+      cudaEventElapsedTime(&h->stats.ms_sph_density, h->ev[4], h->ev[7]);
+    }
   }
   h->stats.leaf_interactions = ctl.stats[0];
   h->stats.far_interactions = ctl.stats[1];
@@ -534,7 +537,7 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
   cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-  for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
   for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&h->chunk_ev[i], cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaHostAlloc(&h->ctl_host, sizeof(DevCtl), cudaHostAllocDefault);
   if (e != cudaSuccess) {

@@ -21,9 +21,12 @@
 // is the queried one, so each particle is seen once. Cell coordinates are clamped to the
 // int32 range (monotone, so a clamped query box still covers its ball). One warp serves
 // one target: its lanes walk the query box's buckets 32 at a time as one flattened list.
-// The density warp keeps the candidates of its bracket (radius, sorted slot) in shared
-// memory and evaluates every bisection step from there (streaming the box again only when
-// more than kCandCap candidates fall inside). Sums are lane-strided and reduced by a
+// The density warp keeps its candidates (radius, sorted slot) in shared memory and
+// evaluates every bisection step from there (streaming the box again only when more than
+// kCandCap candidates fall inside). It gathers a ball of 2.5 x the bracket seed instead
+// of the reference's 2 x hi = 4 x seed: a comparison whose count needs a wider ball is
+// settled by the lower bound of the gathered part when that clears n_ngb, else the
+// gather widens first, so every comparison is the reference's. Sums are lane-strided and reduced by a
 // fixed shuffle tree, so results are deterministic; against the reference's ascending
 // serial sum they differ by rounding only. The CFL bound is a max over pairs and a min
 // over targets, so it is exact given the same h.
@@ -41,7 +44,10 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr double kFourThirdsPi = 4.0 * kPi / 3.0;  // (4 pi / 3), rounded as the reference's
 constexpr int kSphThreads = 128;                  // one target per warp
 constexpr int kSphWarps = kSphThreads / 32;
-constexpr int kCandCap = 1024;                    // density candidates cached per warp
+constexpr int kDensThreads = 256;                 // density: one target per warp, 8 a block
+constexpr int kDensWarps = kDensThreads / 32;
+constexpr int kCandCap = 512;                     // density candidates cached per warp
+constexpr double kLowerBoundMargin = 1.0 + 1e-10; // a partial count this far above n_ngb decides
 constexpr uint32_t kBoxAxisMax = 1u << 10;        // a query box wider than this scans all
 constexpr uint32_t kBoxCellsMax = 1u << 15;       //   gas instead of its cells
 constexpr int kLoopCap = 512;                     // bound on every root-find loop
@@ -362,11 +368,11 @@ struct DensArgs {
   DevCtl* ctl;
 };
 
-__global__ void __launch_bounds__(kSphThreads) k_sph_density(DensArgs a) {
-  __shared__ double s_r[kSphWarps][kCandCap];
-  __shared__ uint32_t s_s[kSphWarps][kCandCap];
+__global__ void __launch_bounds__(kDensThreads) k_sph_density(DensArgs a) {
+  __shared__ double s_r[kDensWarps][kCandCap];
+  __shared__ uint32_t s_s[kDensWarps][kCandCap];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t w = blockIdx.x * kSphWarps + warp;
+  const uint32_t w = blockIdx.x * kDensWarps + warp;
   if (w >= a.g.n) return;  // warp-uniform
   double* cr = s_r[warp];
   uint32_t* cs = s_s[warp];
@@ -443,27 +449,43 @@ __global__ void __launch_bounds__(kSphThreads) k_sph_density(DensArgs a) {
     const double s = 2.0 * h;
     return kFourThirdsPi * (s * s * s) * wsum(h, false);
   };
+  // The candidates are every particle within Rc of the target. count(h) needs all within
+  // 2h; when 2h > Rc the candidates' sum is a lower bound of it (every term is >= 0),
+  // which settles "count >= n_ngb" whenever it clears n_ngb by more than any rounding
+  // could move it. Otherwise the gather widens to 2h first: the comparisons are the
+  // reference's, on a gather that is usually a quarter of its 2 * hi ball.
+  auto less = [&](double h) -> bool {  // count(h) < n_ngb
+    if (2.0 * h <= Rc) return count(h) < a.n_ngb;
+    if (count(h) >= a.n_ngb * kLowerBoundMargin) return false;
+    gather(2.0 * h);
+    return count(h) < a.n_ngb;
+  };
+  auto greater = [&](double h) -> bool {  // count(h) > n_ngb
+    if (2.0 * h <= Rc) return count(h) > a.n_ngb;
+    if (count(h) >= a.n_ngb * kLowerBoundMargin) return true;
+    gather(2.0 * h);
+    return count(h) > a.n_ngb;
+  };
 
   bool bad = false;
-  gather(2.0 * hi);
+  gather(fmin(2.0 * hi, 2.5 * seed));
   int it = 0;
-  while (count(hi) < a.n_ngb && hi < h_cap) {
+  while (less(hi) && hi < h_cap) {
     if (++it > kLoopCap) {
       bad = true;
       break;
     }
     hi = fmin(hi * 2.0, h_cap);
-    gather(2.0 * hi);
   }
   int shrinks = 0;
-  while (count(lo) > a.n_ngb && shrinks < 60) {
+  while (greater(lo) && shrinks < 60) {
     lo /= 2.0;
     shrinks += 1;
   }
   double h;
-  if (count(hi) < a.n_ngb) {
+  if (less(hi)) {
     h = hi;
-  } else if (count(lo) > a.n_ngb) {
+  } else if (greater(lo)) {
     h = lo;
   } else {
     it = 0;
@@ -473,13 +495,14 @@ __global__ void __launch_bounds__(kSphThreads) k_sph_density(DensArgs a) {
         break;
       }
       const double mid = 0.5 * (lo + hi);
-      if (count(mid) < a.n_ngb)
+      if (less(mid))
         lo = mid;
       else
         hi = mid;
     }
     h = 0.5 * (lo + hi);
   }
+  if (2.0 * h > Rc) gather(2.0 * h);
   const double rho = wsum(h, true);
   if (lane == 0) {
     a.rho[k] = rho;
@@ -846,7 +869,7 @@ void sph_free(SphState& s) {
 }
 
 void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const double* mass, double* acc,
-                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st) {
+                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density) {
   const uint32_t n = static_cast<uint32_t>(s.n_gas);
   if (n == 0) return;
   SphScalars* sc = s.sc;
@@ -871,8 +894,9 @@ void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const 
     da.tol = s.p.h_tol_rel;
     da.warm = s.p.warm_start;
     da.ctl = ctl;
-    k_sph_density<<<warp_grid(n), kSphThreads, 0, st>>>(da);
+    k_sph_density<<<static_cast<uint32_t>((n + kDensWarps - 1) / kDensWarps), kDensThreads, 0, st>>>(da);
   }
+  if (after_density) cudaEventRecord(after_density, st);
   if (!hydro) {
     k_sph_done<<<1, 1, 0, st>>>(sc);
     return;

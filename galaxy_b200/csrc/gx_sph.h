@@ -85,7 +85,7 @@ void sph_free(SphState& s);
 // density (when `density`; otherwise rho / hs hold the caller's values), the hydro force
 // (when `hydro`) and, when acc is non-null, its scatter-add into the gas rows of acc.
 void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const double* mass, double* acc,
-                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st);
+                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density = nullptr);
 // The CFL bound per gas particle (dtv) and its minimum (sc->min_dt_enc) at the current
 // velocities, on the hydro grid of the last force evaluation. With rebuild, the gas is
 // gathered and the hydro grid rebuilt from hs first (the caller supplied h).

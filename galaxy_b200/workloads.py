@@ -89,3 +89,30 @@ def request_stream(count: int, rate: float = 50.0, seed: int = 0, n_min: int = 1
     steps = rng.integers(steps_min, steps_max + 1, count)
     return [Request(i, float(t[i]), int(n[i]), float(q[i]), float(rp[i]), int(steps[i]), seed * 1_000_003 + i)
             for i in range(count)]
+
+
+def gas_star_mix(n_gas: int, n_star: int, seed: int = 0) -> State:
+    """A gas blob inside a wider star field, the resident SPH gates' setup scaled up
+    (gpu/tests/gpu_resident_sph.rs:38-96: gas in a cube of side 2 at every
+    (1 + n_star/n_gas)-th index, stars in a cube of side 6, velocities of 0.1 scale).
+    Seeded numpy draws; total mass 1 (gas masses U[0.5, 1), star masses U[0.1, 1), scaled)."""
+    rng = np.random.default_rng(seed)
+    n = n_gas + n_star
+    gpos = (rng.random((n_gas, 3)) - 0.5) * 2.0
+    gvel = (rng.random((n_gas, 3)) - 0.5) * 0.1
+    gm = 0.5 + 0.5 * rng.random(n_gas)
+    spos = (rng.random((n_star, 3)) - 0.5) * 6.0
+    svel = (rng.random((n_star, 3)) - 0.5) * 0.1
+    sm = 0.1 + 0.9 * rng.random(n_star)
+    take = max(n_star // max(n_gas, 1), 1)
+    gas_rows = np.arange(n_gas) * (1 + take)
+    gas_rows = gas_rows[gas_rows < n]
+    kind = np.zeros(n, np.uint8)
+    kind[gas_rows[:n_gas]] = 1
+    gi = np.flatnonzero(kind == 1)
+    si = np.flatnonzero(kind == 0)
+    pos, vel, mass = np.empty((n, 3)), np.empty((n, 3)), np.empty(n)
+    pos[gi], vel[gi], mass[gi] = gpos[:gi.size], gvel[:gi.size], gm[:gi.size]
+    pos[si], vel[si], mass[si] = spos[:si.size], svel[:si.size], sm[:si.size]
+    mass /= mass.sum()
+    return State(pos, vel, mass, kind=kind)

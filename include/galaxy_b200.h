@@ -81,7 +81,7 @@ typedef struct gx_stats {
   float ms_walk;
   float ms_total;
   float ms_sph;            /* gas density + hydro + scatter (gas mode), CUDA events */
-  float pad;
+  float ms_sph_density;    /* the density part of ms_sph (grids, seeds, root-find) */
 } gx_stats;
 
 /* ---- lifecycle ------------------------------------------------------------- */
