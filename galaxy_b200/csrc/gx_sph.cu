@@ -59,6 +59,7 @@ struct GridDev {
   uint32_t tmask, n;
   const uint32_t* start;
   const uint32_t* end;
+  const uint32_t* mixed;  // bit per bucket: it holds more than one cell
   const double4* sp;
   const int4* sc;
 };
@@ -71,6 +72,7 @@ GridDev view(const SphState& s, int g) {
   d.n = static_cast<uint32_t>(s.n_gas);
   d.start = s.grid[g].start;
   d.end = s.grid[g].end;
+  d.mixed = s.grid[g].mixed;
   d.sp = s.grid[g].sp;
   d.sc = s.grid[g].sc;
   return d;
@@ -148,8 +150,8 @@ __device__ __forceinline__ double warp_max(double v) {
 
 // Every gas particle whose cell lies in the query box of centre c and half-width R,
 // each exactly once: f(ok, slot) is called by all 32 lanes together (ok false for
-// padding lanes and for bucket entries of another cell). A box wider than the limits
-// visits every slot instead (ok for all of them).
+// padding lanes and for bucket entries of another cell; a bucket that holds one cell is
+// checked once, by its first entry). A box wider than the limits visits every slot instead.
 template <class F>
 __device__ __forceinline__ void visit_box(const GridDev& g, double cx, double cy, double cz, double R, F&& f) {
   const int lane = threadIdx.x & 31;
@@ -167,7 +169,7 @@ __device__ __forceinline__ void visit_box(const GridDev& g, double cx, double cy
   const uint32_t nxu = static_cast<uint32_t>(nx), nxy = static_cast<uint32_t>(nx * ny);
   for (uint32_t c0 = 0; c0 < nc; c0 += 32) {
     const uint32_t c = c0 + lane;
-    uint32_t st = 0, cnt = 0;
+    uint32_t st = 0, cnt = 0, mix = 0;
     int ox = 0, oy = 0, oz = 0;
     if (c < nc) {
       ox = lx + static_cast<int>(c % nxu);
@@ -176,6 +178,11 @@ __device__ __forceinline__ void visit_box(const GridDev& g, double cx, double cy
       const uint32_t b = cell_hash(ox, oy, oz) & g.tmask;
       st = g.start[b];
       cnt = g.end[b] - st;
+      mix = (g.mixed[b >> 5] >> (b & 31)) & 1u;
+      if (cnt && !mix) {  // a bucket of one cell: this cell's, or none of it
+        const int4 q = g.sc[st];
+        if (q.x != ox || q.y != oy || q.z != oz) cnt = 0;
+      }
     }
     uint32_t incl = cnt;
 #pragma unroll
@@ -196,13 +203,17 @@ __device__ __forceinline__ void visit_box(const GridDev& g, double cx, double cy
       }
       L = min(L, 31);
       const uint32_t exL = __shfl_sync(kFull, excl, L), stL = __shfl_sync(kFull, st, L);
+      const uint32_t mixL = __shfl_sync(kFull, mix, L);
       const int ax = __shfl_sync(kFull, ox, L), ay = __shfl_sync(kFull, oy, L), az = __shfl_sync(kFull, oz, L);
       bool ok = false;
       uint32_t s = 0;
       if (t < total) {
         s = stL + (t - exL);
-        const int4 q = g.sc[s];
-        ok = q.x == ax && q.y == ay && q.z == az;
+        ok = true;
+        if (mixL) {
+          const int4 q = g.sc[s];
+          ok = q.x == ax && q.y == ay && q.z == az;
+        }
       }
       f(ok, s);
     }
@@ -349,11 +360,11 @@ __global__ void __launch_bounds__(kFlat) k_sph_hmax(uint32_t n, const double* __
     atomicMax(&sc->h_max_bits, static_cast<unsigned long long>(__double_as_longlong(m)));
 }
 
-// forces.rs:286-293: the hydro grid's edge and the gather radius are SUPPORT * h_max.
+// forces.rs:286-293: the gather radius is SUPPORT * h_max; the grid's edge is h_max.
 __global__ void k_sph_hydro_cell(SphScalars* sc) {
   const double h_max = __longlong_as_double(static_cast<long long>(sc->h_max_bits));
   sc->h_max = h_max;
-  sc->hydro_cell = fmax(2.0 * h_max, 1e-300);
+  sc->hydro_cell = fmax(h_max, 1e-300);  // queries of radius 2 h_max span 3 to 5 cells an axis
 }
 
 // ---- density (density.rs:232-289) -----------------------------------------------------
@@ -562,8 +573,7 @@ __global__ void __launch_bounds__(kSphThreads) k_sph_hydro(HydroArgs a) {
   const double R2 = R * R;
   double ax = 0.0, ay = 0.0, az = 0.0, du = 0.0;
   visit_box(a.g, xi.x, xi.y, xi.z, R, [&](bool ok, uint32_t s) {
-    if (!ok) return;
-    if (static_cast<uint32_t>(a.g.sc[s].w) == k) return;
+    if (!ok || s == w) return;  // slot w is the target itself
     const double4 p = a.g.sp[s];
     const double rx = xi.x - p.x, ry = xi.y - p.y, rz = xi.z - p.z;
     const double r2 = rx * rx + ry * ry + rz * rz;
@@ -677,8 +687,7 @@ uint32_t warp_grid(size_t n) { return static_cast<uint32_t>((n + kSphWarps - 1) 
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Build grid g over the gathered gas: keys, stable sort by bucket, runs, (occupancy
-// grid) mixed buckets.
+// Build grid g over the gathered gas: keys, stable sort by bucket, runs, mixed buckets.
 void grid_build(SphState& s, int g, DevCtl* ctl, cudaStream_t st) {
   SphGrid& G = s.grid[g];
   const uint32_t n = static_cast<uint32_t>(s.n_gas);
@@ -702,10 +711,8 @@ void grid_build(SphState& s, int g, DevCtl* ctl, cudaStream_t st) {
   launch_sort_passes(G.key, G.skey, G.order, s.keys_tmp, s.vals_tmp, s.tiles, s.sys, s.hist, s.status, s.counters,
                      s.ntiles, ctl, st);
   k_grid_fill<<<flat_grid(n), kFlat, 0, st>>>(n, G.skey, G.order, s.gp, G.cc, G.sp, G.sc, G.start, G.end);
-  if (g == 0) {
-    cudaMemsetAsync(G.mixed, 0, (T / 32 + 1) * sizeof(uint32_t), st);
-    k_grid_mixed<<<flat_grid(n), kFlat, 0, st>>>(n, G.skey, G.sc, G.start, G.mixed);
-  }
+  cudaMemsetAsync(G.mixed, 0, (T / 32 + 1) * sizeof(uint32_t), st);
+  k_grid_mixed<<<flat_grid(n), kFlat, 0, st>>>(n, G.skey, G.sc, G.start, G.mixed);
 }
 
 std::mutex g_tab_mu;
