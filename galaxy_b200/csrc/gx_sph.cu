@@ -48,6 +48,7 @@ constexpr int kDensThreads = 256;                 // density: one target per war
 constexpr int kDensWarps = kDensThreads / 32;
 constexpr int kCandCap = 512;                     // density candidates cached per warp
 constexpr double kLowerBoundMargin = 1.0 + 1e-10; // a partial count this far above n_ngb decides
+constexpr int kPairCap = 128;                     // hydro: neighbour slots listed per warp
 constexpr uint32_t kBoxAxisMax = 1u << 10;        // a query box wider than this scans all
 constexpr uint32_t kBoxCellsMax = 1u << 15;       //   gas instead of its cells
 constexpr int kLoopCap = 512;                     // bound on every root-find loop
@@ -417,13 +418,17 @@ __global__ void __launch_bounds__(kDensThreads) k_sph_density(DensArgs a) {
       const unsigned m = __ballot_sync(kFull, in);
       const uint32_t at = ncand + __popc(m & ((1u << lane) - 1u));
       if (in && at < static_cast<uint32_t>(kCandCap)) {
-        cr[at] = sqrt(r2);
+        cr[at] = r2;
         cs[at] = s;
       }
       ncand += __popc(m);
     });
     over = ncand > static_cast<uint32_t>(kCandCap);
     __syncwarp();
+    if (!over) {  // the distances, one pass with every lane busy
+      for (uint32_t j = lane; j < ncand; j += 32) cr[j] = sqrt(cr[j]);
+      __syncwarp();
+    }
   };
   // sum over the candidates of W(r, h), mass-weighted or not
   // Candidates at r >= 2h add exact zeros (r >= 2h gives r / h >= 2 after rounding) and
@@ -560,9 +565,11 @@ struct HydroArgs {
 };
 
 __global__ void __launch_bounds__(kSphThreads) k_sph_hydro(HydroArgs a) {
+  __shared__ uint32_t s_pair[kSphWarps][kPairCap];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t w = blockIdx.x * kSphWarps + warp;
   if (w >= a.g.n) return;
+  uint32_t* pl = s_pair[warp];
   const double4 xi = a.g.sp[w];
   const uint32_t k = static_cast<uint32_t>(a.g.sc[w].w);
   const double4 vi = a.sv[w];
@@ -572,40 +579,65 @@ __global__ void __launch_bounds__(kSphThreads) k_sph_hydro(HydroArgs a) {
   const double R = 2.0 * a.sc->h_max;
   const double R2 = R * R;
   double ax = 0.0, ay = 0.0, az = 0.0, du = 0.0;
-  visit_box(a.g, xi.x, xi.y, xi.z, R, [&](bool ok, uint32_t s) {
-    if (!ok || s == w) return;  // slot w is the target itself
-    const double4 p = a.g.sp[s];
-    const double rx = xi.x - p.x, ry = xi.y - p.y, rz = xi.z - p.z;
-    const double r2 = rx * rx + ry * ry + rz * rz;
-    if (!(r2 <= R2)) return;
-    const double r = sqrt(r2);
-    const double4 vj = a.sv[s];
-    // beyond both supports both gradients are zero and the pair adds exact zeros
-    if (r >= 2.0 * fmax(h_i, vj.w)) return;
-    const double4 aj = a.sa[s];
-    double gix, giy, giz, gjx, gjy, gjz;
-    const bool nzi = sph_grad(rx, ry, rz, r, h_i, ai.z, gix, giy, giz);
-    const bool nzj = sph_grad(rx, ry, rz, r, vj.w, aj.z, gjx, gjy, gjz);
-    if (!nzi && !nzj) return;
-    const double gax = (gix + gjx) * 0.5, gay = (giy + gjy) * 0.5, gaz = (giz + gjz) * 0.5;
-    const double term_j = aj.y;
-    const double vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
-    const double vr = vx * rx + vy * ry + vz * rz;
-    double visc = 0.0;
-    if (vr < 0.0) {
-      const double h_bar = 0.5 * (h_i + vj.w);
-      const double rho_bar = 0.5 * (ai.x + aj.x);
-      const double mu = h_bar * vr / (r * r + a.visc_eps2 * h_bar * h_bar);
-      const double c_bar = a.adiabatic ? 0.5 * (ai.w + aj.w) : a.c_s;
-      visc = (-a.alpha * c_bar * mu + a.beta * mu * mu) / rho_bar;
+  uint32_t np = 0;
+  // The pairs of the list, 32 at a time (every lane busy).
+  auto flush = [&]() {
+    for (uint32_t j = lane; j < np; j += 32) {
+      const uint32_t s = pl[j];
+      const double4 p = a.g.sp[s];
+      const double rx = xi.x - p.x, ry = xi.y - p.y, rz = xi.z - p.z;
+      const double r = sqrt(rx * rx + ry * ry + rz * rz);
+      const double4 vj = a.sv[s];
+      // beyond both supports both gradients are zero and the pair adds exact zeros
+      if (r >= 2.0 * fmax(h_i, vj.w)) continue;
+      const double4 aj = a.sa[s];
+      double gix, giy, giz, gjx, gjy, gjz;
+      const bool nzi = sph_grad(rx, ry, rz, r, h_i, ai.z, gix, giy, giz);
+      const bool nzj = sph_grad(rx, ry, rz, r, vj.w, aj.z, gjx, gjy, gjz);
+      if (!nzi && !nzj) continue;
+      const double gax = (gix + gjx) * 0.5, gay = (giy + gjy) * 0.5, gaz = (giz + gjz) * 0.5;
+      const double term_j = aj.y;
+      const double vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+      const double vr = vx * rx + vy * ry + vz * rz;
+      double visc = 0.0;
+      if (vr < 0.0) {
+        const double h_bar = 0.5 * (h_i + vj.w);
+        const double rho_bar = 0.5 * (ai.x + aj.x);
+        const double mu = h_bar * vr / (r * r + a.visc_eps2 * h_bar * h_bar);
+        const double c_bar = a.adiabatic ? 0.5 * (ai.w + aj.w) : a.c_s;
+        visc = (-a.alpha * c_bar * mu + a.beta * mu * mu) / rho_bar;
+      }
+      const double coeff = term_i + term_j + visc;
+      const double sc_ = -p.w * coeff;
+      ax += gax * sc_;
+      ay += gay * sc_;
+      az += gaz * sc_;
+      du += p.w * (term_i + 0.5 * visc) * (vx * gax + vy * gay + vz * gaz);
     }
-    const double coeff = term_i + term_j + visc;
-    const double sc_ = -p.w * coeff;
-    ax += gax * sc_;
-    ay += gay * sc_;
-    az += gaz * sc_;
-    du += p.w * (term_i + 0.5 * visc) * (vx * gax + vy * gay + vz * gaz);
+    np = 0;
+    __syncwarp();
+  };
+  // Scan the box: a neighbour whose squared distance is below (2 max(h_i, h_j))^2, with
+  // a margin over its rounding, goes to the list (a superset of the coupled pairs; the
+  // exact test r >= 2 max(h_i, h_j) is made again in the flush).
+  visit_box(a.g, xi.x, xi.y, xi.z, R, [&](bool ok, uint32_t s) {
+    bool take = false;
+    if (ok && s != w) {  // slot w is the target itself
+      const double4 p = a.g.sp[s];
+      const double rx = xi.x - p.x, ry = xi.y - p.y, rz = xi.z - p.z;
+      const double r2 = rx * rx + ry * ry + rz * rz;
+      if (r2 <= R2) {
+        const double lim = 2.0 * fmax(h_i, a.sv[s].w);
+        take = r2 < lim * lim * (1.0 + 1e-12);
+      }
+    }
+    const unsigned m = __ballot_sync(kFull, take);
+    if (take) pl[np + __popc(m & ((1u << lane) - 1u))] = s;
+    np += __popc(m);
+    __syncwarp();
+    if (np > static_cast<uint32_t>(kPairCap - 32)) flush();
   });
+  flush();
   ax = warp_sum(ax);
   ay = warp_sum(ay);
   az = warp_sum(az);
