@@ -1,14 +1,16 @@
-//! `GpuLbvhB200`, `GpuStaleTreeB200` and `GpuResidentB200`: galaxy's gravity-solver
-//! interface over libgalaxy_b200 (a B200 LBVH Barnes-Hut). `GpuLbvhB200` implements
-//! `ForceSolver` (core/src/traits.rs) and drops in beside `Lbvh`, `BarnesHut` and
-//! `GpuLbvhFused`; `GpuStaleTreeB200` plays `TreeGravity`'s stale-tree role for individual
-//! time steps; `GpuResidentB200` mirrors `GpuResidentLeapfrog`'s upload / step_many /
-//! snapshot.
+//! `GpuLbvhB200`, `GpuStaleTreeB200`, `GpuGravitySphB200` and `GpuResidentB200`: galaxy's
+//! gravity-solver interface over libgalaxy_b200 (a B200 LBVH Barnes-Hut). `GpuLbvhB200`
+//! implements `ForceSolver` (core/src/traits.rs) and drops in beside `Lbvh`, `BarnesHut`
+//! and `GpuLbvhFused`; `GpuStaleTreeB200` plays `TreeGravity`'s stale-tree role for
+//! individual time steps; `GpuGravitySphB200` plays `GravitySph<Lbvh>`
+//! (solvers/src/sph/gravity_sph.rs); `GpuResidentB200` mirrors `GpuResidentLeapfrog`'s
+//! upload / step_many / snapshot and, from `new_with_sph`, its gas mode.
 //!
 //! Written against include/galaxy_b200.h; DVec3 is three f64 (`#[repr(C)]`-compatible
 //! in glam), so `&[DVec3]` is passed as `*const f64` with no copy.
 
 use galaxy_core::{DVec3, ForceSolver, State};
+use galaxy_solvers::sph::{DensityConfig, Eos, HydroParams};
 use std::ffi::CStr;
 use std::os::raw::{c_char, c_int};
 
@@ -27,6 +29,48 @@ pub struct GxOptions {
 #[repr(C)]
 pub struct GxHandle {
     _private: [u8; 0],
+}
+
+/// `gx_sph_params`: HydroParams + DensityConfig as the C ABI takes them.
+#[repr(C)]
+#[derive(Clone, Copy, Default)]
+pub struct GxSphParams {
+    pub n_ngb: f64,
+    pub h_tol_rel: f64,
+    pub eos: c_int,
+    pub warm_start: c_int,
+    pub c_s: f64,
+    pub gamma: f64,
+    pub alpha: f64,
+    pub beta: f64,
+    pub visc_eps2: f64,
+}
+
+impl GxSphParams {
+    /// The reference's parameters (forces.rs:64-87, density.rs:33-51); h warm-started
+    /// across evaluations as GravitySph does.
+    pub fn from_reference(hydro: &HydroParams, density: &DensityConfig) -> Self {
+        let (eos, c_s, gamma) = match hydro.eos {
+            Eos::Isothermal { c_s } => (0, c_s, 5.0 / 3.0),
+            Eos::Adiabatic { gamma } => (1, 0.0, gamma),
+        };
+        GxSphParams { n_ngb: density.n_ngb, h_tol_rel: density.h_tol_rel, eos, warm_start: 1, c_s, gamma,
+                      alpha: hydro.alpha, beta: hydro.beta, visc_eps2: hydro.visc_eps2 }
+    }
+}
+
+extern "C" {
+    fn gx_sph_enable(h: *mut GxHandle, p: *const GxSphParams) -> c_int;
+    fn gx_upload_species(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
+                         kind: *const u8, u: *const f64) -> c_int;
+    fn gx_gas_count(h: *const GxHandle, n_gas: *mut usize) -> c_int;
+    fn gx_snapshot_gas_density(h: *mut GxHandle, gas_idx: *mut u32, rho: *mut f64, hsml: *mut f64) -> c_int;
+    fn gx_snapshot_gas_accel(h: *mut GxHandle, acc: *mut f64, dudt: *mut f64) -> c_int;
+    fn gx_snapshot_accel(h: *mut GxHandle, acc: *mut f64) -> c_int;
+    fn gx_min_stable_dt(h: *mut GxHandle, c_cfl: f64, out: *mut f64) -> c_int;
+    fn gx_snapshot_gas_dt(h: *mut GxHandle, c_cfl: f64, dt: *mut f64) -> c_int;
+    fn gx_sph_accelerations(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
+                            kind: *const u8, u: *const f64, acc: *mut f64) -> c_int;
 }
 
 extern "C" {
@@ -212,10 +256,64 @@ impl Drop for GpuStaleTreeB200 {
     }
 }
 
+/// `GravitySph<Lbvh>` (solvers/src/sph/gravity_sph.rs:172-207): gravity on every
+/// particle, density, smoothing lengths and the hydro force on the gas rows, h
+/// warm-started across calls while the gas count holds.
+pub struct GpuGravitySphB200 {
+    h: *mut GxHandle,
+}
+
+impl GpuGravitySphB200 {
+    pub fn new(g: f64, softening: f64, theta: f64, hydro: HydroParams, density: DensityConfig)
+               -> Result<Self, GxError> {
+        let mut h = std::ptr::null_mut();
+        let rc = unsafe { gx_create(g, softening, theta, std::ptr::null(), &mut h) };
+        if rc != 0 {
+            return Err(err(std::ptr::null(), rc));
+        }
+        let p = GxSphParams::from_reference(&hydro, &density);
+        let rc = unsafe { gx_sph_enable(h, &p) };
+        if rc != 0 {
+            let e = err(h, rc);
+            unsafe { gx_destroy(h) };
+            return Err(e);
+        }
+        Ok(Self { h })
+    }
+}
+
+impl ForceSolver for GpuGravitySphB200 {
+    fn accelerations(&mut self, state: &State, acc: &mut [DVec3]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        // Species is #[repr(u8)] (Collisionless = 0, Gas = 1): the column crosses as bytes.
+        let rc = unsafe {
+            gx_sph_accelerations(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                 state.kind.as_ptr() as *const u8, state.u.as_ptr(), acc.as_mut_ptr() as *mut f64)
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    fn potential_energy(&self, state: &State) -> f64 {
+        let mut out = 0.0;
+        let rc = unsafe { gx_potential_energy(self.h, state.len(), as_f64(&state.pos), state.mass.as_ptr(), &mut out) };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+        out
+    }
+}
+
+impl Drop for GpuGravitySphB200 {
+    fn drop(&mut self) {
+        unsafe { gx_destroy(self.h) }
+    }
+}
+
 /// Device-resident KDK stepping (the role of `GpuResidentLeapfrog`).
 pub struct GpuResidentB200 {
     h: *mut GxHandle,
     mass: Vec<f64>,
+    kind: Vec<galaxy_core::Species>,
+    gas_mode: bool,
 }
 
 impl GpuResidentB200 {
@@ -225,15 +323,79 @@ impl GpuResidentB200 {
         if rc != 0 {
             return Err(err(std::ptr::null(), rc));
         }
-        Ok(Self { h, mass: Vec::new() })
+        Ok(Self { h, mass: Vec::new(), kind: Vec::new(), gas_mode: false })
+    }
+
+    /// `GpuResidentLeapfrog::new_with_sph` (gpu/src/gpu_resident.rs:1393): gas mode.
+    pub fn new_with_sph(g: f64, softening: f64, theta: f64, hydro: HydroParams, density: DensityConfig)
+                        -> Result<Self, GxError> {
+        let mut s = Self::new(g, softening, theta)?;
+        let p = GxSphParams::from_reference(&hydro, &density);
+        let rc = unsafe { gx_sph_enable(s.h, &p) };
+        if rc != 0 {
+            return Err(err(s.h, rc));
+        }
+        s.gas_mode = true;
+        Ok(s)
     }
 
     pub fn upload(&mut self, state: &State) -> Result<(), GxError> {
         self.mass = state.mass.clone();
+        self.kind = state.kind.clone();
         let rc = unsafe {
-            gx_upload(self.h, state.len(), as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr())
+            if self.gas_mode {
+                gx_upload_species(self.h, state.len(), as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                  state.kind.as_ptr() as *const u8, state.u.as_ptr())
+            } else {
+                gx_upload(self.h, state.len(), as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr())
+            }
         };
         if rc != 0 { Err(err(self.h, rc)) } else { Ok(()) }
+    }
+
+    fn gas_count(&self) -> usize {
+        let mut n = 0usize;
+        unsafe { gx_gas_count(self.h, &mut n) };
+        n
+    }
+
+    /// `snapshot_gas_density` (gpu_resident.rs:1566): (gas_idx, rho, h).
+    pub fn snapshot_gas_density(&mut self) -> Result<(Vec<u32>, Vec<f64>, Vec<f64>), GxError> {
+        let ng = self.gas_count();
+        let (mut idx, mut rho, mut h) = (vec![0u32; ng], vec![0.0; ng], vec![0.0; ng]);
+        let rc = unsafe { gx_snapshot_gas_density(self.h, idx.as_mut_ptr(), rho.as_mut_ptr(), h.as_mut_ptr()) };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok((idx, rho, h)) }
+    }
+
+    /// `snapshot_gas_accel` (gpu_resident.rs:1593): the hydro acceleration of the gas rows.
+    pub fn snapshot_gas_accel(&mut self) -> Result<Vec<DVec3>, GxError> {
+        let mut acc = vec![DVec3::ZERO; self.gas_count()];
+        let rc = unsafe { gx_snapshot_gas_accel(self.h, acc.as_mut_ptr() as *mut f64, std::ptr::null_mut()) };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok(acc) }
+    }
+
+    /// `snapshot_accel` (gpu_resident.rs:1655).
+    pub fn snapshot_accel(&mut self) -> Result<Vec<DVec3>, GxError> {
+        let mut acc = vec![DVec3::ZERO; self.mass.len()];
+        let rc = unsafe { gx_snapshot_accel(self.h, acc.as_mut_ptr() as *mut f64) };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok(acc) }
+    }
+
+    /// `min_stable_dt` (gpu_resident.rs:1614): reduced on the device; +inf without gas.
+    pub fn min_stable_dt(&mut self, c_cfl: f64) -> Result<f64, GxError> {
+        let mut out = f64::INFINITY;
+        let rc = unsafe { gx_min_stable_dt(self.h, c_cfl, &mut out) };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok(out) }
+    }
+
+    /// `snapshot_gas_dt` (gpu_resident.rs:1632): the per-gas CFL vector.
+    pub fn snapshot_gas_dt(&mut self, c_cfl: f64) -> Result<Vec<f64>, GxError> {
+        let mut dt = vec![0.0; self.gas_count()];
+        if dt.is_empty() {
+            return Ok(dt);
+        }
+        let rc = unsafe { gx_snapshot_gas_dt(self.h, c_cfl, dt.as_mut_ptr()) };
+        if rc != 0 { Err(err(self.h, rc)) } else { Ok(dt) }
     }
 
     pub fn step_many(&mut self, dt: f64, steps: u64) -> Result<(), GxError> {
@@ -250,6 +412,9 @@ impl GpuResidentB200 {
             return Err(err(self.h, rc));
         }
         let mut s = State::from_phase_space(pos, vel, self.mass.clone());
+        if self.kind.len() == n {
+            s.kind = self.kind.clone();
+        }
         unsafe { gx_time(self.h, &mut s.time) };
         Ok(s)
     }
