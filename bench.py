@@ -516,6 +516,40 @@ def run_precision(args):
         dist.destroy_process_group()
 
 
+# Kernels a gas-mode step adds to the 8 of the gravity step: gather, scalars, 3 grids
+# (keys, histogram, 4 sort passes, fill, mixed flags), seeds, density cell, density, h_max,
+# hydro cell, pack, hydro, scatter.
+SPH_LAUNCHES_PER_STEP = 2 + 3 * 8 + 9
+
+
+def sph_roofline(n_gas: int, stage: dict, peaks: dict) -> dict:
+    """Issue-rate roofline of the SPH root-find and hydro kernels: warp instructions per gas
+    particle (ncu summary in profiles/, scaled to this n_gas) over this run's stage times;
+    the peak is one warp instruction per scheduler per clock. FP64 work with L2-resident
+    data: neither HBM nor tensor cores bound it."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", "k_sph_kernels_gas_star_mix_262144.md")
+    try:
+        text = open(path).read()
+        per = {k: float(re.search(k + r":\s*([0-9.]+)", text).group(1))
+               for k in ("density_instructions_per_gas", "hydro_instructions_per_gas")}
+    except (OSError, AttributeError):
+        return {"kernel": "k_sph_density + k_sph_hydro", "bound": "issue", "achieved": None}
+    mhz = peaks.get("sm_max_mhz", 1965.0)
+    peak = 148 * 4 * mhz / 1e3  # G warp instructions / s
+    ms_d = stage["ms_sph_density"]
+    ms_h = stage["ms_sph"] - stage["ms_sph_density"]
+    inst = (per["density_instructions_per_gas"] + per["hydro_instructions_per_gas"]) * n_gas
+    ach = inst / ((ms_d + ms_h) * 1e-3) / 1e9
+    return {"kernel": "k_sph_density + k_sph_hydro (FP64, one warp per gas particle)", "bound": "issue",
+            "achieved": ach, "peak": peak, "unit": "G warp instructions/s", "frac": ach / peak,
+            "traffic": None, "instructions_per_gas": per,
+            "source": "instructions per gas particle from profiles/k_sph_kernels_gas_star_mix_262144.md; "
+                      "time = this run's SPH stage events (grids, pack and scatter included)",
+            "peak_source": "148 SMs x 4 schedulers x clocks.max.sm"}
+
+
 def run_sph(args):
     """Resident gas mode (GpuResidentLeapfrog::new_with_sph, gpu_resident.rs:1393-1565):
     a gas blob of --gas particles inside a field of as many stars. Each step: KDK with
@@ -606,12 +640,9 @@ def run_sph(args):
                            "l2": f"working set ~{900 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)",
                            "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}},
                 "gas_particle_steps_per_s": ng * ws * args.steps / (ms_max / 1e3),
-                "e2e": e2e, "gpu_launches": None, "cpu_baseline": cpu, "clocks": clk, "stage_ms": stage,
-                "sph_share_of_step": gas_frac, "min_stable_dt_c0.25": cfl,
-                "roofline": {"kernel": "k_sph_density (adaptive-h root-find)", "bound": "issue",
-                             "note": "FP64 per-pair arithmetic with warp reductions; see profiles/ "
-                                     "k_sph_density_uniform_262144.md for the instruction and pipe counters",
-                             "peak_source": peaks.get("sm_max_mhz") and "clocks.max.sm" or "nominal 1965 MHz"}}
+                "e2e": e2e, "gpu_launches": (8 + SPH_LAUNCHES_PER_STEP) * args.steps, "cpu_baseline": cpu,
+                "clocks": clk, "stage_ms": stage, "sph_share_of_step": gas_frac, "min_stable_dt_c0.25": cfl,
+                "roofline": sph_roofline(ng, stage, peaks)}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
