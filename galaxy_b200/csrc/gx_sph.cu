@@ -564,7 +564,9 @@ struct HydroArgs {
   double c_s, gamma, alpha, beta, visc_eps2;
 };
 
-__global__ void __launch_bounds__(kSphThreads) k_sph_hydro(HydroArgs a) {
+// Six blocks an SM (80 registers, a few spilled): the kernel is latency-bound on its
+// neighbour loads, and 24 resident warps beat 16 at 112 registers (measured).
+__global__ void __launch_bounds__(kSphThreads, 6) k_sph_hydro(HydroArgs a) {
   __shared__ uint32_t s_pair[kSphWarps][kPairCap];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t w = blockIdx.x * kSphWarps + warp;
