@@ -302,6 +302,16 @@ class GpuGravitySph(GpuLbvh):
                                             _ptr(state.kind), _ptr(state.u), _ptr(acc)))
         return acc
 
+    def accel_and_dudt(self, state, acc=None, dudt=None):
+        """ForceSolver::accel_and_dudt of GravitySph (gravity_sph.rs:209-245): (acc [n,3],
+        dudt [n], zero on collisionless rows)."""
+        n = len(state)
+        acc = np.empty((n, 3)) if acc is None else acc
+        dudt = np.empty(n) if dudt is None else dudt
+        self._ck(lib().gx_sph_accel_and_dudt(self._h, n, _ptr(state.pos), _ptr(state.vel), _ptr(state.mass),
+                                             _ptr(state.kind), _ptr(state.u), _ptr(acc), _ptr(dudt)))
+        return acc, dudt
+
     def density(self, pos, mass, h_init=None):
         """density_adaptive (density.rs:86-96) over gas positions: (rho, h)."""
         pos, mass = _f64(pos).reshape(-1, 3), _f64(mass).reshape(-1)

@@ -1504,6 +1504,11 @@ int gx_snapshot_gas_dt(gx_handle* h, double c_cfl, double* dt_out) {
 
 int gx_sph_accelerations(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                          const uint8_t* kind, const double* u, double* acc_out) {
+  return gx_sph_accel_and_dudt(h, n, pos, vel, mass, kind, u, acc_out, nullptr);
+}
+
+int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                          const uint8_t* kind, const double* u, double* acc_out, double* dudt_out) {
   if (!h) return GX_ERR_INVALID_ARG;
   if (int rc = need_sph(h)) return rc;
   if (n == 0) return GX_OK;
@@ -1530,10 +1535,21 @@ int gx_sph_accelerations(gx_handle* h, size_t n, const double* pos, const double
     sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream);
   }
   GX_CK(h, cudaMemcpyAsync(acc_out, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> gdudt;
+  if (dudt_out && !gas.empty()) {
+    gdudt.resize(gas.size());
+    GX_CK(h, cudaMemcpyAsync(gdudt.data(), h->sph.dudt, gas.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                             h->stream));
+  }
   h->stats.n = n;
   rc = finish(h, stats_on(h));
-  if (rc == GX_OK) h->sph_host_hint_ngas = gas.size();
-  return rc;
+  if (rc != GX_OK) return rc;
+  h->sph_host_hint_ngas = gas.size();
+  if (dudt_out) {
+    std::fill(dudt_out, dudt_out + n, 0.0);
+    for (size_t k = 0; k < gas.size(); ++k) dudt_out[gas[k]] = gdudt[k];
+  }
+  return GX_OK;
 }
 
 int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,

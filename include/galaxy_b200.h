@@ -221,6 +221,11 @@ int gx_snapshot_gas_dt(gx_handle* h, double c_cfl, double* dt_out);
  * warm-started across calls while the gas count is unchanged (params.warm_start). */
 int gx_sph_accelerations(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                          const uint8_t* kind, const double* u, double* acc_out);
+/* GravitySph::accel_and_dudt (gravity_sph.rs:209-245; core/src/traits.rs:37-40): the same
+ * accelerations and, in dudt_out[n], the gas rows' du/dt (PdV work + viscous heating,
+ * forces.rs:160-172); 0 on collisionless rows. */
+int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                          const uint8_t* kind, const double* u, double* acc_out, double* dudt_out);
 /* density_adaptive (density.rs:86-96) over n gas particles: rho_out[n], h_out[n];
  * h_init[n] (nullable) seeds the brackets. */
 int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,

@@ -294,3 +294,17 @@ def test_resident_gas_mode_large_properties(oracle):
     m = st.mass[gas]
     scale = np.sum(m[:, None] * np.abs(acc))
     assert np.linalg.norm((m[:, None] * acc).sum(axis=0)) < 1e-10 * scale
+
+
+def test_accel_and_dudt_matches_oracle_hydro(oracle):
+    # gravity_sph.rs:209-245: gas rows get the fused hydro du/dt, collisionless rows 0
+    st = mix_state(oracle, 0xD0D7, 800, 1600)
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    acc, dudt = s.accel_and_dudt(st)
+    acc2 = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64").accelerations(st)
+    assert np.array_equal(acc, acc2)
+    gas = st.gas()
+    rho, h = oracle.sph_density_adaptive(st.pos[gas], st.mass[gas])
+    _, dref = oracle.sph_hydro(st.pos[gas], st.vel[gas], st.mass[gas], rho, h)
+    assert not dudt[st.kind == 0].any()
+    assert np.max(np.abs(dudt[gas] - dref)) <= 1e-10 * np.sqrt(np.mean(dref * dref))
