@@ -858,7 +858,7 @@ namespace {
 int upload_impl(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                 const std::vector<uint32_t>* gas, const double* u) {
   cudaSetDevice(h->device);
-  if (h->resident_gas && h->step_graph) {  // captured with the SPH stages
+  if (h->step_graph) {  // captured for the previous state (its gas map and SPH buffers)
     cudaGraphExecDestroy(h->step_graph);
     h->step_graph = nullptr;
   }
