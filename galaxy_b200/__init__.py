@@ -302,6 +302,18 @@ class GpuGravitySph(GpuLbvh):
                                             _ptr(state.kind), _ptr(state.u), _ptr(acc)))
         return acc
 
+    def accelerations_active(self, state, active, acc=None):
+        """GravitySph::accelerations_active (gravity_sph.rs:247-286): gravity of every
+        particle, then density and hydro for the active gas particles only, from the
+        persistent (rho, h) scratch (inactive neighbours read stale, as the reference)."""
+        n = len(state)
+        acc = np.empty((n, 3)) if acc is None else acc
+        act = np.ascontiguousarray(active, dtype=np.uint32)
+        self._ck(lib().gx_sph_accelerations_active(self._h, n, _ptr(state.pos), _ptr(state.vel), _ptr(state.mass),
+                                                   _ptr(state.kind), _ptr(state.u), act.shape[0], _ptr(act),
+                                                   _ptr(acc)))
+        return acc
+
     def accel_and_dudt(self, state, acc=None, dudt=None):
         """ForceSolver::accel_and_dudt of GravitySph (gravity_sph.rs:209-245): (acc [n,3],
         dudt [n], zero on collisionless rows)."""

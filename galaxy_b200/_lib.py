@@ -220,6 +220,7 @@ SIGNATURES = {
     "gx_snapshot_gas_dt": (_i, [_vp, _d, _vp]),
     "gx_sph_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gx_sph_accel_and_dudt": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gx_sph_accelerations_active": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp]),
     "gx_sph_density": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp]),
     "gx_sph_hydro": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gx_sph_cfl": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _d, _vp, C.POINTER(_d)]),

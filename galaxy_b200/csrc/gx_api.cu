@@ -306,6 +306,8 @@ struct gx_handle {
   SphState sph;
   bool resident_gas = false;     // the resident state has gas and runs SPH in each force
   size_t sph_host_hint_ngas = 0;  // gx_sph_accelerations: gas count of the last call
+  size_t sph_rho_scratch_ngas = 0;  // gx_sph_accelerations_active: its rho scratch is set
+  uint64_t sph_rho_gen = 0;         // ... in this allocation of the SPH buffers
   // graph of one resident step (pending closing kick + opening kick, drift, force)
   cudaGraphExec_t step_graph = nullptr;
   size_t graph_n = 0;
@@ -1549,6 +1551,77 @@ int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const doubl
     std::fill(dudt_out, dudt_out + n, 0.0);
     for (size_t k = 0; k < gas.size(); ++k) dudt_out[gas[k]] = gdudt[k];
   }
+  return GX_OK;
+}
+
+int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                                const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
+                                double* acc_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (n == 0) return GX_OK;
+  if (!pos || !vel || !mass || !acc_out || (n_active && !active)) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  for (size_t i = 0; i < n_active; ++i)
+    if (active[i] >= n) return fail(h, GX_ERR_INVALID_ARG, "active index out of range");
+  std::vector<uint32_t> gas;
+  int rc = gas_map(h, n, kind, gas);
+  if (rc) return rc;
+  cudaSetDevice(h->device);
+  const size_t ng = gas.size();
+  // gravity_sph.rs:88-150 (active_gas): a scratch that is unset for this gas count forces a
+  // refresh of every gas particle, warm-started from h when h is set
+  const bool h_set0 = ng && h->sph_host_hint_ngas == ng;
+  const bool rho_set0 = ng && h->sph_rho_scratch_ngas == ng;
+  const uint64_t gen0 = h->sph.alloc_gen;
+  h->sph_host_hint_ngas = 0;
+  h->sph_rho_scratch_ngas = 0;
+  rc = host_sph_setup(h, n, pos, vel, mass, &gas, h_set0 && h->sph.p.warm_start, true);
+  if (rc) return rc;
+  const bool same_alloc = h->sph.alloc_gen == gen0;  // a reallocation loses both scratches
+  const bool h_set = h_set0 && same_alloc;
+  const bool rho_set = rho_set0 && same_alloc && h->sph_rho_gen == gen0;
+  StepBufs& b = h->ar.b;
+  if (n == 1)
+    GX_CK(h, cudaMemsetAsync(b.acc, 0, 3 * sizeof(double), h->stream));
+  else
+    enqueue_force(h, b, 0, 0, stats_on(h));
+  std::vector<uint32_t> local;
+  const bool all = !(h_set && rho_set);
+  if (ng && !all) {
+    std::vector<uint8_t> mark(ng, 0);
+    std::vector<uint32_t> g2l(n, 0xFFFFFFFFu);
+    for (size_t k = 0; k < ng; ++k) g2l[gas[k]] = static_cast<uint32_t>(k);
+    for (size_t i = 0; i < n_active; ++i)
+      if (g2l[active[i]] != 0xFFFFFFFFu) mark[g2l[active[i]]] = 1;
+    for (size_t k = 0; k < ng; ++k)
+      if (mark[k]) local.push_back(static_cast<uint32_t>(k));
+  }
+  if (ng) {
+    if (u) {
+      std::vector<double> gu(ng);
+      for (size_t k = 0; k < ng; ++k) gu[k] = u[gas[k]];
+      GX_CK(h, cudaMemcpy(h->sph.gu, gu.data(), ng * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // the density pass writes the refreshed rows over the active path's rho scratch
+    if (rho_set)
+      GX_CK(h, cudaMemcpyAsync(h->sph.rho, h->sph.rho_act, ng * sizeof(double), cudaMemcpyDeviceToDevice,
+                               h->stream));
+    if (!all && !local.empty())
+      GX_CK(h, cudaMemcpyAsync(h->sph.targets, local.data(), local.size() * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, h->stream));
+    if (all || !local.empty())
+      sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream, nullptr,
+                        all ? nullptr : h->sph.targets, static_cast<uint32_t>(local.size()));
+    GX_CK(h, cudaMemcpyAsync(h->sph.rho_act, h->sph.rho, ng * sizeof(double), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  }
+  GX_CK(h, cudaMemcpyAsync(acc_out, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  h->stats.n = n;
+  rc = finish(h, stats_on(h));  // also keeps `local` alive until its copy has run
+  if (rc != GX_OK) return rc;
+  h->sph_host_hint_ngas = ng;
+  h->sph_rho_scratch_ngas = ng;
+  h->sph_rho_gen = h->sph.alloc_gen;
   return GX_OK;
 }
 

@@ -289,12 +289,13 @@ __global__ void __launch_bounds__(kFlat) k_grid_fill(uint32_t n, const uint32_t*
                                                      const uint32_t* __restrict__ order, const double4* __restrict__ gp,
                                                      const int4* __restrict__ cc, double4* __restrict__ sp,
                                                      int4* __restrict__ sc, uint32_t* __restrict__ start,
-                                                     uint32_t* __restrict__ end) {
+                                                     uint32_t* __restrict__ end, uint32_t* __restrict__ inv) {
   for (uint32_t s = blockIdx.x * kFlat + threadIdx.x; s < n; s += gridDim.x * kFlat) {
     const uint32_t k = order[s];
     if (k >= n) continue;
     sp[s] = gp[k];
     sc[s] = cc[k];
+    inv[k] = s;
     const uint32_t b = skey[s];
     if (s == 0 || skey[s - 1] != b) start[b] = s;
     if (s == n - 1 || skey[s + 1] != b) end[b] = s + 1;
@@ -378,6 +379,9 @@ struct DensArgs {
   double n_ngb, tol;
   int warm;
   DevCtl* ctl;
+  const uint32_t* targets;  // gas-local targets (nullptr: every gas particle, in grid order)
+  uint32_t n_targets;
+  const uint32_t* inv;      // gas-local index -> slot of this grid
 };
 
 __global__ void __launch_bounds__(kDensThreads) k_sph_density(DensArgs a) {
@@ -385,11 +389,12 @@ __global__ void __launch_bounds__(kDensThreads) k_sph_density(DensArgs a) {
   __shared__ uint32_t s_s[kDensWarps][kCandCap];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t w = blockIdx.x * kDensWarps + warp;
-  if (w >= a.g.n) return;  // warp-uniform
+  if (w >= (a.targets ? a.n_targets : a.g.n)) return;  // warp-uniform
   double* cr = s_r[warp];
   uint32_t* cs = s_s[warp];
-  const double4 xi = a.g.sp[w];
-  const uint32_t k = static_cast<uint32_t>(a.g.sc[w].w);
+  const uint32_t slot = a.targets ? a.inv[a.targets[w]] : w;
+  const double4 xi = a.g.sp[slot];
+  const uint32_t k = static_cast<uint32_t>(a.g.sc[slot].w);
   const double h_cap = a.sc->h_cap;
   double seed = a.seeds[k];
   if (a.warm && a.sc->hint_valid) {
@@ -562,6 +567,9 @@ struct HydroArgs {
   double* dudt;
   int adiabatic;
   double c_s, gamma, alpha, beta, visc_eps2;
+  const uint32_t* targets;  // gas-local targets (nullptr: every gas particle, in grid order)
+  uint32_t n_targets;
+  const uint32_t* inv;      // gas-local index -> slot of this grid
 };
 
 // Six blocks an SM (80 registers, a few spilled): the kernel is latency-bound on its
@@ -569,9 +577,10 @@ struct HydroArgs {
 __global__ void __launch_bounds__(kSphThreads, 6) k_sph_hydro(HydroArgs a) {
   __shared__ uint32_t s_pair[kSphWarps][kPairCap];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t w = blockIdx.x * kSphWarps + warp;
-  if (w >= a.g.n) return;
+  const uint32_t wi = blockIdx.x * kSphWarps + warp;
+  if (wi >= (a.targets ? a.n_targets : a.g.n)) return;  // warp-uniform
   uint32_t* pl = s_pair[warp];
+  const uint32_t w = a.targets ? a.inv[a.targets[wi]] : wi;  // the target's slot
   const double4 xi = a.g.sp[w];
   const uint32_t k = static_cast<uint32_t>(a.g.sc[w].w);
   const double4 vi = a.sv[w];
@@ -652,10 +661,12 @@ __global__ void __launch_bounds__(kSphThreads, 6) k_sph_hydro(HydroArgs a) {
   }
 }
 
-// acc[gas row] += hydro (gravity_sph.rs:203-205).
+// acc[gas row] += hydro (gravity_sph.rs:203-205), for every gas particle or the listed ones.
 __global__ void __launch_bounds__(kFlat) k_sph_scatter(uint32_t n_gas, const uint32_t* __restrict__ gas_idx,
+                                                       const uint32_t* __restrict__ targets,
                                                        const double* __restrict__ gacc, double* __restrict__ acc) {
-  for (uint32_t k = blockIdx.x * kFlat + threadIdx.x; k < n_gas; k += gridDim.x * kFlat) {
+  for (uint32_t t = blockIdx.x * kFlat + threadIdx.x; t < n_gas; t += gridDim.x * kFlat) {
+    const uint32_t k = targets ? targets[t] : t;
     const size_t i = gas_idx[k];
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[3 * i + c] = acc[3 * i + c] + gacc[3 * (size_t)k + c];
@@ -744,7 +755,7 @@ void grid_build(SphState& s, int g, DevCtl* ctl, cudaStream_t st) {
   launch_code_hist(b, st);
   launch_sort_passes(G.key, G.skey, G.order, s.keys_tmp, s.vals_tmp, s.tiles, s.sys, s.hist, s.status, s.counters,
                      s.ntiles, ctl, st);
-  k_grid_fill<<<flat_grid(n), kFlat, 0, st>>>(n, G.skey, G.order, s.gp, G.cc, G.sp, G.sc, G.start, G.end);
+  k_grid_fill<<<flat_grid(n), kFlat, 0, st>>>(n, G.skey, G.order, s.gp, G.cc, G.sp, G.sc, G.start, G.end, G.inv);
   cudaMemsetAsync(G.mixed, 0, (T / 32 + 1) * sizeof(uint32_t), st);
   k_grid_mixed<<<flat_grid(n), kFlat, 0, st>>>(n, G.skey, G.sc, G.start, G.mixed);
 }
@@ -796,7 +807,7 @@ cudaError_t sph_reserve(SphState& s, size_t n_gas, bool keep_hint, double s_est_
                  o_rho = take(cap * 8), o_hs = take(cap * 8), o_seeds = take(cap * 8), o_gacc = take(cap * 24),
                  o_dudt = take(cap * 8), o_dtv = take(cap * 8), o_sv = take(cap * 32), o_sa = take(cap * 32),
                  o_sc = take(sizeof(SphScalars));
-    size_t o_g[3][9];
+    size_t o_g[3][10];
     for (int g = 0; g < 3; ++g) {
       o_g[g][0] = take(cap * 4);
       o_g[g][1] = take(cap * 4);
@@ -807,7 +818,9 @@ cudaError_t sph_reserve(SphState& s, size_t n_gas, bool keep_hint, double s_est_
       o_g[g][6] = take(T * 4);
       o_g[g][7] = take(T * 4);
       o_g[g][8] = take((T / 32 + 1) * 4);
+      o_g[g][9] = take(cap * 4);
     }
+    const size_t o_tg = take(cap * 4), o_rho_act = take(cap * 8);
     const size_t o_kt = take(cap * 4), o_vt = take(cap * 4), o_hist = take(kMaxRadixPasses * kRadixBins * 4),
                  o_status = take(size_t(kRadixPasses) * ct * kRadixBins * 4), o_cnt = take(kCounterWords * 4),
                  o_tiles = take(ct * sizeof(TileDesc)), o_sys = take(sizeof(SysDesc)),
@@ -816,6 +829,7 @@ cudaError_t sph_reserve(SphState& s, size_t n_gas, bool keep_hint, double s_est_
     cudaError_t e = cudaMalloc(&blk, off);
     if (e != cudaSuccess) return e;
     s.block = blk;
+    ++s.alloc_gen;
     char* B = static_cast<char*>(blk);
     s.cap = cap;
     s.tbits = cb;
@@ -843,7 +857,10 @@ cudaError_t sph_reserve(SphState& s, size_t n_gas, bool keep_hint, double s_est_
       G.start = reinterpret_cast<uint32_t*>(B + o_g[g][6]);
       G.end = reinterpret_cast<uint32_t*>(B + o_g[g][7]);
       G.mixed = reinterpret_cast<uint32_t*>(B + o_g[g][8]);
+      G.inv = reinterpret_cast<uint32_t*>(B + o_g[g][9]);
     }
+    s.targets = reinterpret_cast<uint32_t*>(B + o_tg);
+    s.rho_act = reinterpret_cast<double*>(B + o_rho_act);
     s.keys_tmp = reinterpret_cast<uint32_t*>(B + o_kt);
     s.vals_tmp = reinterpret_cast<uint32_t*>(B + o_vt);
     s.hist = reinterpret_cast<uint32_t*>(B + o_hist);
@@ -910,7 +927,8 @@ void sph_free(SphState& s) {
 }
 
 void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const double* mass, double* acc,
-                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density) {
+                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density,
+                       const uint32_t* targets, uint32_t n_targets) {
   const uint32_t n = static_cast<uint32_t>(s.n_gas);
   if (n == 0) return;
   SphScalars* sc = s.sc;
@@ -935,7 +953,11 @@ void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const 
     da.tol = s.p.h_tol_rel;
     da.warm = s.p.warm_start;
     da.ctl = ctl;
-    k_sph_density<<<static_cast<uint32_t>((n + kDensWarps - 1) / kDensWarps), kDensThreads, 0, st>>>(da);
+    da.targets = targets;
+    da.n_targets = n_targets;
+    da.inv = s.grid[1].inv;
+    const uint32_t nd = targets ? n_targets : n;
+    if (nd) k_sph_density<<<(nd + kDensWarps - 1) / kDensWarps, kDensThreads, 0, st>>>(da);
   }
   if (after_density) cudaEventRecord(after_density, st);
   if (!hydro) {
@@ -960,8 +982,13 @@ void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const 
   ha.alpha = s.p.alpha;
   ha.beta = s.p.beta;
   ha.visc_eps2 = s.p.visc_eps2;
-  k_sph_hydro<<<warp_grid(n), kSphThreads, 0, st>>>(ha);
-  if (acc) k_sph_scatter<<<flat_grid(n), kFlat, 0, st>>>(n, s.gas_idx, s.gacc, acc);
+  ha.targets = targets;
+  ha.n_targets = n_targets;
+  ha.inv = s.grid[2].inv;
+  const uint32_t nh = targets ? n_targets : n;
+  if (!nh) return;
+  k_sph_hydro<<<warp_grid(nh), kSphThreads, 0, st>>>(ha);
+  if (acc) k_sph_scatter<<<flat_grid(nh), kFlat, 0, st>>>(nh, s.gas_idx, targets, s.gacc, acc);
 }
 
 void sph_enqueue_cfl(SphState& s, const double* pos, const double* vel, double c_cfl, bool rebuild, DevCtl* ctl,

@@ -42,6 +42,7 @@ struct SphGrid {
   uint32_t* start = nullptr;  // T
   uint32_t* end = nullptr;    // T
   uint32_t* mixed = nullptr;  // T / 32 bits: bucket holds more than one cell
+  uint32_t* inv = nullptr;    // gas-local index -> sorted slot
 };
 
 struct SphState {
@@ -60,6 +61,8 @@ struct SphState {
   double* gacc = nullptr;  // hydro acceleration, 3 per gas particle
   double* dudt = nullptr;
   double* dtv = nullptr;   // CFL bound per gas particle
+  uint32_t* targets = nullptr;  // gas-local targets of an active-subset pass
+  double* rho_act = nullptr;    // the active path's persistent density scratch
   double4* sv = nullptr;   // hydro grid order: vx, vy, vz, h
   double4* sa = nullptr;   // hydro grid order: rho, P/rho^2 term, 1/(pi h^3), c_s
   SphScalars* sc = nullptr;
@@ -71,6 +74,7 @@ struct SphState {
   uint32_t ntiles = 0;
   double* cbrt_tab = nullptr;  // cbrt(c) for integer c < kSphCbrtTable, from the host's libm
   void* block = nullptr;       // the single allocation behind every buffer above
+  uint64_t alloc_gen = 0;      // bumped at every (re)allocation: device scratch is lost
 };
 
 constexpr int kSphCbrtTable = 65536;
@@ -84,8 +88,12 @@ void sph_free(SphState& s);
 // Gas gather + bbox (pos, vel, mass of the system; vel nullable; u from gu), then the
 // density (when `density`; otherwise rho / hs hold the caller's values), the hydro force
 // (when `hydro`) and, when acc is non-null, its scatter-add into the gas rows of acc.
+// targets (device, gas-local, n_targets of them; nullptr: every gas particle) restricts
+// the density and hydro passes and the scatter to those particles; the grids, seeds and
+// h_max cover all gas, the others' rho / h are read as they are (the active path).
 void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const double* mass, double* acc,
-                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density = nullptr);
+                       bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density = nullptr,
+                       const uint32_t* targets = nullptr, uint32_t n_targets = 0);
 // The CFL bound per gas particle (dtv) and its minimum (sc->min_dt_enc) at the current
 // velocities, on the hydro grid of the last force evaluation. With rebuild, the gas is
 // gathered and the hydro grid rebuilt from hs first (the caller supplied h).

@@ -226,6 +226,16 @@ int gx_sph_accelerations(gx_handle* h, size_t n, const double* pos, const double
  * forces.rs:160-172); 0 on collisionless rows. */
 int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                           const uint8_t* kind, const double* u, double* acc_out, double* dudt_out);
+/* GravitySph::accelerations_active (gravity_sph.rs:247-286, the fresh-gravity path): gravity
+ * of all n into acc_out (as gx_sph_accelerations), then density and hydro for the active
+ * gas particles only (active[n_active], global indices; non-gas entries are ignored),
+ * their hydro added to their rows. The handle keeps the reference's persistent (rho, h)
+ * scratch of the gas: h shared with gx_sph_accelerations (its warm start), rho the active
+ * path's own; inactive neighbours are read from it (the reference's bounded staleness).
+ * While either scratch is unset for this gas count, every gas particle is refreshed. */
+int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                                const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
+                                double* acc_out);
 /* density_adaptive (density.rs:86-96) over n gas particles: rho_out[n], h_out[n];
  * h_init[n] (nullable) seeds the brackets. */
 int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,

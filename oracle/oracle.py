@@ -87,6 +87,9 @@ def lib():
                                                  d, C.c_void_p, C.c_void_p, C.c_void_p, _f64p, i]),
             "or_kdk_gravity_sph": (i, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, d, d, d, i, d, d, d, d, d, d,
                                        C.c_void_p, C.c_void_p, C.c_void_p, _f64p, C.POINTER(C.c_int), d, u64, i]),
+            "or_gravity_sph_accelerations_active": (i, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, d, d, d, i, d, d, d,
+                                                        d, d, d, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                        sz, _u32p, _f64p, i]),
             "or_fixture_gas_star_mix": (None, [u64, sz, sz, _f64p, _f64p, _f64p, _u8p]),
             "or_fixture_sph_points": (None, [u64, sz, d, d, _f64p]),
         }
@@ -509,6 +512,27 @@ class GravitySph:
                                            kind, uu, *self._args(), self.h_hint.ctypes.data,
                                            C.addressof(self.h_valid), self.rho.ctypes.data, acc.reshape(-1),
                                            self.threads)
+        return acc
+
+    def accelerations_active(self, pos, vel, mass, kind, active, u=None) -> np.ndarray:
+        """GravitySph::accelerations_active (gravity_sph.rs:247-286): fresh gravity on all,
+        hydro on the active gas targets from the persistent (rho, h) scratch."""
+        pos, vel = _pos(pos), _pos(vel)
+        n = pos.shape[0]
+        kind = np.ascontiguousarray(kind, np.uint8)
+        ng = int((kind == 1).sum())
+        self._hint(ng)
+        if getattr(self, "rho_scratch", None) is None or self.rho_scratch.shape[0] != max(ng, 1):
+            self.rho_scratch = np.zeros(max(ng, 1))
+            self.rho_valid = C.c_int(0)
+        acc = np.zeros((n, 3))
+        uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        act = np.ascontiguousarray(active, dtype=np.uint32)
+        lib().or_gravity_sph_accelerations_active(n, pos.reshape(-1), vel.reshape(-1),
+                                                  np.ascontiguousarray(mass, np.float64), kind, uu, *self._args(),
+                                                  self.h_hint.ctypes.data, C.addressof(self.h_valid),
+                                                  self.rho_scratch.ctypes.data, C.addressof(self.rho_valid),
+                                                  act.shape[0], act, acc.reshape(-1), self.threads)
         return acc
 
     def step_many(self, pos, vel, mass, kind, dt, steps, u=None):

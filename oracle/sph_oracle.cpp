@@ -519,6 +519,91 @@ int or_gravity_sph_accelerations(size_t n, const double* pos, const double* vel,
   return 0;
 }
 
+// gravity_sph.rs:247-286 GravitySph::accelerations_active (fresh gravity on all n), with
+// :101-150 active_gas: h_scratch (shared with or_gravity_sph_accelerations' h_hint) and
+// rho_scratch hold the persistent gas-subset scratch; a scratch that is not set forces a
+// refresh of every gas particle (warm-started from h when h is set). Density
+// (density.rs:118-140, density_adaptive_active) and hydro (forces.rs:188-217,
+// hydro_accel_and_dudt_active) run for the active gas targets only, reading the inactive
+// neighbours' rho / h from the scratch.
+int or_gravity_sph_accelerations_active(size_t n, const double* pos, const double* vel, const double* mass,
+                                        const uint8_t* kind, const double* u, double g, double softening,
+                                        double theta, int eos, double eos_param, double alpha, double beta,
+                                        double visc_eps2, double n_ngb, double h_tol_rel, double* h_scratch,
+                                        int* h_valid, double* rho_scratch, int* rho_valid, size_t n_active,
+                                        const uint32_t* active, double* acc_out, int threads) {
+  if (n == 0) return 0;
+  if (g > 0.0)
+    or_lbvh_accelerations(n, pos, mass, g, softening, theta, acc_out, threads, nullptr);
+  else
+    for (size_t i = 0; i < 3 * n; ++i) acc_out[i] = 0.0;
+  std::vector<size_t> gas;
+  gather_gas(n, kind, gas);
+  if (gas.empty()) {
+    *h_valid = 0;
+    *rho_valid = 0;
+    return 0;
+  }
+  const size_t ng = gas.size();
+  std::vector<double> gpos, gvel, gmass, gu;
+  subset3(pos, gas, gpos);
+  subset3(vel, gas, gvel);
+  subset1(mass, gas, gmass);
+  subset1(u, gas, gu);
+  const bool h_init = !*h_valid, rho_init = !*rho_valid;
+  if (h_init)
+    for (size_t k = 0; k < ng; ++k) h_scratch[k] = 0.0;
+  if (rho_init)
+    for (size_t k = 0; k < ng; ++k) rho_scratch[k] = 0.0;
+  std::vector<size_t> local;
+  if (h_init || rho_init) {
+    for (size_t k = 0; k < ng; ++k) local.push_back(k);
+  } else {
+    std::vector<size_t> g2l(n, SIZE_MAX);
+    for (size_t k = 0; k < ng; ++k) g2l[gas[k]] = k;
+    for (size_t a = 0; a < n_active; ++a)
+      if (g2l[active[a]] != SIZE_MAX) local.push_back(g2l[active[a]]);
+  }
+  DensitySetup setup(gpos.data(), gmass.data(), ng, n_ngb, h_tol_rel);
+  std::vector<double> nr(local.size()), nh(local.size());
+#pragma omp parallel for num_threads(threads > 1 ? threads : 1) schedule(dynamic, 64)
+  for (size_t t = 0; t < local.size(); ++t) setup.solve_one(local[t], h_scratch + local[t], &nr[t], &nh[t]);
+  for (size_t t = 0; t < local.size(); ++t) {
+    rho_scratch[local[t]] = nr[t];
+    h_scratch[local[t]] = nh[t];
+  }
+  Hydro H;
+  H.pos = gpos.data();
+  H.vel = gvel.data();
+  H.mass = gmass.data();
+  H.rho = rho_scratch;
+  H.h = h_scratch;
+  H.u = gu.data();
+  H.n = ng;
+  H.adiabatic = eos;
+  H.c_s = eos == 0 ? eos_param : 0.0;
+  H.gamma = eos == 1 ? eos_param : 0.0;
+  H.alpha = alpha;
+  H.beta = beta;
+  H.visc_eps2 = visc_eps2;
+  H.setup();
+  std::vector<D3> ca(local.size());
+#pragma omp parallel for num_threads(threads > 1 ? threads : 1) schedule(dynamic, 64)
+  for (size_t t = 0; t < local.size(); ++t) {
+    double d;
+    H.force_one(local[t], &ca[t], &d);
+  }
+  for (size_t t = 0; t < local.size(); ++t) {
+    const size_t i = gas[local[t]];
+    acc_out[3 * i] = acc_out[3 * i] + ca[t].x;
+    acc_out[3 * i + 1] = acc_out[3 * i + 1] + ca[t].y;
+    acc_out[3 * i + 2] = acc_out[3 * i + 2] + ca[t].z;
+  }
+  *h_valid = 1;
+  *rho_valid = 1;
+  return 0;
+}
+
 // integrator.rs:38-78 driving GravitySph: `steps` KDK steps in place; acc_io and
 // primed_io carry the integrator's cached force, h_hint / h_hint_valid the composite's
 // warm start (n_gas entries); rho_out (nullable) the last evaluation's gas densities.

@@ -308,3 +308,32 @@ def test_accel_and_dudt_matches_oracle_hydro(oracle):
     _, dref = oracle.sph_hydro(st.pos[gas], st.vel[gas], st.mass[gas], rho, h)
     assert not dudt[st.kind == 0].any()
     assert np.max(np.abs(dudt[gas] - dref)) <= 1e-10 * np.sqrt(np.mean(dref * dref))
+
+
+def test_sph_accelerations_active_matches_oracle(oracle):
+    # gravity_sph.rs:247-286: the first call refreshes every gas particle (it is the full
+    # pass); later calls refresh the active gas only and read inactive neighbours' rho / h
+    # from the persistent scratch, as the reference's individual-timestep path does.
+    st = mix_state(oracle, 0xACE, 1500, 3000)
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    og = oracle.GravitySph(1.0, 0.05, 0.5)
+    every = np.arange(len(st), dtype=np.uint32)
+    a0 = s.accelerations_active(st, every)
+    r0 = og.accelerations_active(st.pos, st.vel, st.mass, st.kind, every)
+    full = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64").accelerations(st)
+    assert np.array_equal(a0, full)
+    assert (np.linalg.norm(a0 - r0, axis=1) / np.linalg.norm(r0, axis=1)).max() < 1e-10
+    rng = np.random.default_rng(4)
+    gas = st.gas()
+    for _ in range(3):
+        st.pos += 1e-3 * st.vel
+        act = np.sort(rng.choice(len(st), len(st) // 3, replace=False)).astype(np.uint32)
+        a = s.accelerations_active(st, act)
+        r = og.accelerations_active(st.pos, st.vel, st.mass, st.kind, act)
+        err = np.linalg.norm(a - r, axis=1) / np.linalg.norm(r, axis=1)
+        assert (err > 1e-10).sum() <= 1 and err.max() < 1e-2
+        grav = oracle.lbvh_accelerations(st.pos, st.mass, 1.0, 0.05, 0.5)
+        stale = np.setdiff1d(gas, act)
+        assert np.array_equal(a[stale], grav[stale])  # inactive gas rows: gravity only
+    with pytest.raises(gb.GxError):
+        s.accelerations_active(st, np.array([len(st)], np.uint32))
