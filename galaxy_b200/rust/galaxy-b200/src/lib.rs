@@ -71,6 +71,9 @@ extern "C" {
     fn gx_snapshot_gas_dt(h: *mut GxHandle, c_cfl: f64, dt: *mut f64) -> c_int;
     fn gx_sph_accelerations(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
                             kind: *const u8, u: *const f64, acc: *mut f64) -> c_int;
+    fn gx_sph_accelerations_active(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64,
+                                   mass: *const f64, kind: *const u8, u: *const f64, n_active: usize,
+                                   active: *const u32, acc: *mut f64) -> c_int;
 }
 
 extern "C" {
@@ -290,6 +293,18 @@ impl ForceSolver for GpuGravitySphB200 {
         let rc = unsafe {
             gx_sph_accelerations(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
                                  state.kind.as_ptr() as *const u8, state.u.as_ptr(), acc.as_mut_ptr() as *mut f64)
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    fn accelerations_active(&mut self, state: &State, active: &[usize], acc: &mut [DVec3]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        let idx: Vec<u32> = active.iter().map(|&i| i as u32).collect();
+        let rc = unsafe {
+            gx_sph_accelerations_active(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                        state.kind.as_ptr() as *const u8, state.u.as_ptr(), idx.len(), idx.as_ptr(),
+                                        acc.as_mut_ptr() as *mut f64)
         };
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
     }
