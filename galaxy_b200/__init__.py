@@ -314,6 +314,28 @@ class GpuGravitySph(GpuLbvh):
                                                    _ptr(acc)))
         return acc
 
+    def sf_fields(self, state):
+        """GravitySph::sf_fields (gravity_sph.rs:353-382): state-indexed (rho, div_v) from a
+        cold-start density solve; zero on collisionless rows."""
+        n = len(state)
+        rho, dv = np.zeros(n), np.zeros(n)
+        self._ck(lib().gx_sph_sf_fields(self._h, n, _ptr(state.pos), _ptr(state.vel), _ptr(state.mass),
+                                        _ptr(state.kind), _ptr(rho), _ptr(dv)))
+        return rho, dv
+
+    def coupled_pairs(self, state) -> np.ndarray:
+        """GravitySph::coupled_pairs (cfl.rs:195-228): [P, 2] global index pairs, ascending."""
+        n = len(state)
+        cap = 64 * max(n, 1)
+        out = np.zeros(2 * cap, dtype=np.uint64)
+        k = C.c_size_t()
+        args = (self._h, n, _ptr(state.pos), _ptr(state.mass), _ptr(state.kind))
+        self._ck(lib().gx_sph_coupled_pairs(*args, _ptr(out), cap, C.byref(k)))
+        if k.value > cap:
+            out = np.zeros(2 * k.value, dtype=np.uint64)
+            self._ck(lib().gx_sph_coupled_pairs(*args, _ptr(out), k.value, C.byref(k)))
+        return out[:2 * k.value].reshape(-1, 2).copy()
+
     def accel_and_dudt(self, state, acc=None, dudt=None):
         """ForceSolver::accel_and_dudt of GravitySph (gravity_sph.rs:209-245): (acc [n,3],
         dudt [n], zero on collisionless rows)."""

@@ -1625,6 +1625,102 @@ int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const
   return GX_OK;
 }
 
+int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                     const uint8_t* kind, double* rho_out, double* div_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  if (n == 0) return GX_OK;
+  if (!pos || !vel || !mass || !rho_out || !div_out) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  std::vector<uint32_t> gas;
+  int rc = gas_map(h, n, kind, gas);
+  if (rc) return rc;
+  std::fill(rho_out, rho_out + n, 0.0);
+  std::fill(div_out, div_out + n, 0.0);
+  if (gas.empty()) return GX_OK;
+  cudaSetDevice(h->device);
+  h->sph_host_hint_ngas = 0;
+  rc = host_sph_setup(h, n, pos, vel, mass, &gas, false, true);  // a cold-start solve
+  if (rc) return rc;
+  const StepBufs& b = h->ar.b;
+  const size_t ng = gas.size();
+  sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, nullptr, true, false, b.ctl, h->stream);
+  sph_enqueue_divergence(h->sph, h->sph.dudt, h->stream);  // dudt is free scratch here
+  std::vector<double> rho(ng), dv(ng);
+  GX_CK(h, cudaMemcpyAsync(rho.data(), h->sph.rho, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaMemcpyAsync(dv.data(), h->sph.dudt, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  rc = finish(h, false);
+  if (rc) return rc;
+  for (size_t k = 0; k < ng; ++k) {
+    rho_out[gas[k]] = rho[k];
+    div_out[gas[k]] = dv[k];
+  }
+  return GX_OK;
+}
+
+int gx_sph_coupled_pairs(gx_handle* h, size_t n, const double* pos, const double* mass, const uint8_t* kind,
+                         uint64_t* pairs_out, size_t cap, size_t* count_out) {
+  if (!h || !count_out) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  *count_out = 0;
+  if (n == 0) return GX_OK;
+  if (!pos || !mass || (cap && !pairs_out)) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  std::vector<uint32_t> gas;
+  int rc = gas_map(h, n, kind, gas);
+  if (rc || gas.empty()) return rc;
+  cudaSetDevice(h->device);
+  h->sph_host_hint_ngas = 0;
+  rc = host_sph_setup(h, n, pos, nullptr, mass, &gas, false, true);
+  if (rc) return rc;
+  const StepBufs& b = h->ar.b;
+  const size_t ng = gas.size();
+  sph_enqueue_force(h->sph, b.pos, nullptr, b.mass, nullptr, true, false, b.ctl, h->stream);
+  // pass 1: pairs per a; the host turns them into offsets; pass 2 writes the b's
+  uint32_t* d_counts = nullptr;
+  uint64_t* d_off = nullptr;
+  uint32_t* d_list = nullptr;
+  auto release = [&]() {
+    if (d_counts) cudaFree(d_counts);
+    if (d_off) cudaFree(d_off);
+    if (d_list) cudaFree(d_list);
+  };
+  cudaError_t e = cudaMalloc(&d_counts, ng * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&d_off, ng * sizeof(uint64_t));
+  if (e != cudaSuccess) {
+    release();
+    return fail(h, GX_ERR_CUDA, std::string("coupled pairs scratch: ") + cudaGetErrorString(e));
+  }
+  sph_enqueue_pairs(h->sph, d_counts, nullptr, nullptr, b.ctl, h->stream, true);
+  std::vector<uint32_t> counts(ng);
+  e = cudaMemcpyAsync(counts.data(), d_counts, ng * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  std::vector<uint64_t> off(ng + 1, 0);
+  for (size_t k = 0; k < ng; ++k) off[k + 1] = off[k] + counts[k];
+  const size_t total = off[ng];
+  std::vector<uint32_t> list(total);
+  if (e == cudaSuccess && total) {
+    e = cudaMalloc(&d_list, total * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_off, off.data(), ng * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) sph_enqueue_pairs(h->sph, nullptr, d_off, d_list, b.ctl, h->stream, false);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(list.data(), d_list, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream);
+  }
+  rc = e == cudaSuccess ? finish(h, false) : fail(h, GX_ERR_CUDA, std::string("coupled pairs: ") + cudaGetErrorString(e));
+  release();
+  if (rc) return rc;
+  // ascending (a, b): a runs in order, each run's b's sorted (cfl.rs:216-225)
+  size_t w = 0;
+  for (size_t a = 0; a < ng; ++a) {
+    std::sort(list.begin() + off[a], list.begin() + off[a + 1]);
+    for (uint64_t t = off[a]; t < off[a + 1]; ++t, ++w)
+      if (w < cap) {
+        pairs_out[2 * w] = gas[a];
+        pairs_out[2 * w + 1] = gas[list[t]];
+      }
+  }
+  *count_out = total;
+  return GX_OK;
+}
+
 int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,
                    double* rho_out, double* h_out) {
   if (!h) return GX_ERR_INVALID_ARG;

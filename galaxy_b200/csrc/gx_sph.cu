@@ -673,6 +673,74 @@ __global__ void __launch_bounds__(kFlat) k_sph_scatter(uint32_t n_gas, const uin
   }
 }
 
+// ---- velocity divergence (divergence.rs:34-72) and coupled pairs (cfl.rs:195-228) ----------
+// On the density grid of the same call: per target the gather of radius 2 h_i,
+// div v_i = sum_{j != i} m_j (v_j - v_i) . grad_i W(r_ij, h_i) / rho_i.
+__global__ void __launch_bounds__(kSphThreads) k_sph_divergence(GridDev g, const double4* __restrict__ gv,
+                                                                const double* __restrict__ hs,
+                                                                const double* __restrict__ rho,
+                                                                double* __restrict__ div) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t w = blockIdx.x * kSphWarps + warp;
+  if (w >= g.n) return;
+  const double4 xi = g.sp[w];
+  const uint32_t k = static_cast<uint32_t>(g.sc[w].w);
+  const double4 vi = gv[k];
+  const double h_i = hs[k], norm_i = sph_norm(h_i);
+  const double R = 2.0 * h_i, R2 = R * R;
+  double sum = 0.0;
+  visit_box(g, xi.x, xi.y, xi.z, R, [&](bool ok, uint32_t s) {
+    if (!ok || s == w) return;  // slot w is the target itself
+    const double4 p = g.sp[s];
+    const double rx = xi.x - p.x, ry = xi.y - p.y, rz = xi.z - p.z;
+    const double r2 = rx * rx + ry * ry + rz * rz;
+    if (!(r2 <= R2)) return;
+    double gx, gy, gz;
+    if (!sph_grad(rx, ry, rz, sqrt(r2), h_i, norm_i, gx, gy, gz)) return;
+    const double4 vj = gv[static_cast<uint32_t>(g.sc[s].w)];
+    sum += p.w * ((vj.x - vi.x) * gx + (vj.y - vi.y) * gy + (vj.z - vi.z) * gz);
+  });
+  sum = warp_sum(sum);
+  if (lane == 0) div[k] = sum / rho[k];
+}
+
+// Coupled pairs (a, b), a < b gas-local, 0 < r < 2 max(h_a, h_b), on the hydro grid (radius
+// 2 h_max as the reference's gather): counts[a] when list is null, else the b of each pair
+// written from list[offsets[a]] on (in the grid's visit order; the host sorts each run).
+__global__ void __launch_bounds__(kSphThreads) k_sph_pairs(GridDev g, const SphScalars* sc, const double* __restrict__ hs,
+                                                           uint32_t* __restrict__ counts,
+                                                           const uint64_t* __restrict__ offsets,
+                                                           uint32_t* __restrict__ list) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t w = blockIdx.x * kSphWarps + warp;
+  if (w >= g.n) return;
+  const double4 xi = g.sp[w];
+  const uint32_t a = static_cast<uint32_t>(g.sc[w].w);
+  const double h_a = hs[a];
+  const double R = 2.0 * sc->h_max, R2 = R * R;
+  uint32_t cnt = 0;
+  visit_box(g, xi.x, xi.y, xi.z, R, [&](bool ok, uint32_t s) {
+    bool take = false;
+    uint32_t b = 0;
+    if (ok) {
+      b = static_cast<uint32_t>(g.sc[s].w);
+      if (b > a) {
+        const double4 p = g.sp[s];
+        const double rx = xi.x - p.x, ry = xi.y - p.y, rz = xi.z - p.z;
+        const double r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 <= R2) {
+          const double r = sqrt(r2);
+          take = r > 0.0 && r < 2.0 * fmax(h_a, hs[b]);
+        }
+      }
+    }
+    const unsigned m = __ballot_sync(kFull, take);
+    if (list && take) list[offsets[a] + cnt + __popc(m & ((1u << lane) - 1u))] = b;
+    cnt += __popc(m);
+  });
+  if (!list && lane == 0) counts[a] = cnt;
+}
+
 // ---- CFL (cfl.rs:67-121) ----------------------------------------------------------------
 struct CflArgs {
   GridDev g;
@@ -989,6 +1057,24 @@ void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const 
   if (!nh) return;
   k_sph_hydro<<<warp_grid(nh), kSphThreads, 0, st>>>(ha);
   if (acc) k_sph_scatter<<<flat_grid(nh), kFlat, 0, st>>>(nh, s.gas_idx, targets, s.gacc, acc);
+}
+
+void sph_enqueue_divergence(SphState& s, double* div, cudaStream_t st) {
+  const uint32_t n = static_cast<uint32_t>(s.n_gas);
+  if (n) k_sph_divergence<<<warp_grid(n), kSphThreads, 0, st>>>(view(s, 1), s.gv, s.hs, s.rho, div);
+}
+
+void sph_enqueue_pairs(SphState& s, uint32_t* counts, const uint64_t* offsets, uint32_t* list, DevCtl* ctl,
+                       cudaStream_t st, bool build_grid) {
+  const uint32_t n = static_cast<uint32_t>(s.n_gas);
+  if (!n) return;
+  if (build_grid) {
+    cudaMemsetAsync(&s.sc->h_max_bits, 0, sizeof(unsigned long long), st);
+    k_sph_hmax<<<flat_grid(n), kFlat, 0, st>>>(n, s.hs, s.sc);
+    k_sph_hydro_cell<<<1, 1, 0, st>>>(s.sc);
+    grid_build(s, 2, ctl, st);
+  }
+  k_sph_pairs<<<warp_grid(n), kSphThreads, 0, st>>>(view(s, 2), s.sc, s.hs, counts, offsets, list);
 }
 
 void sph_enqueue_cfl(SphState& s, const double* pos, const double* vel, double c_cfl, bool rebuild, DevCtl* ctl,

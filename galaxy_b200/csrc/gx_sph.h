@@ -99,6 +99,13 @@ void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const 
 // gathered and the hydro grid rebuilt from hs first (the caller supplied h).
 void sph_enqueue_cfl(SphState& s, const double* pos, const double* vel, double c_cfl, bool rebuild, DevCtl* ctl,
                      cudaStream_t st);
+// div v of every gas particle (divergence.rs:34-72) into div (gas-local), on the density
+// grid, h and rho of the density pass just enqueued and the velocities it gathered.
+void sph_enqueue_divergence(SphState& s, double* div, cudaStream_t st);
+// Coupled gas pairs (cfl.rs:195-228) on the hydro grid (built first when build_grid): with
+// list null, counts[a] = pairs (a, b > a); else the b's from list[offsets[a]] on.
+void sph_enqueue_pairs(SphState& s, uint32_t* counts, const uint64_t* offsets, uint32_t* list, DevCtl* ctl,
+                       cudaStream_t st, bool build_grid);
 // Host-side s_est of DensitySetup::new (density.rs:166-181) from host positions: the
 // gas rows gas_idx[0 .. n_gas) of pos (gas_idx NULL: rows 0 .. n_gas).
 double sph_host_s_est(size_t n_gas, const double* pos, const uint32_t* gas_idx);

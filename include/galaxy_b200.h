@@ -236,6 +236,16 @@ int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const doubl
 int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                                 const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
                                 double* acc_out);
+/* GravitySph::sf_fields (gravity_sph.rs:353-382): rho_out[n] and div_out[n] (velocity
+ * divergence, divergence.rs:34-72) of the gas rows from a cold-start density solve;
+ * collisionless rows 0. */
+int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                     const uint8_t* kind, double* rho_out, double* div_out);
+/* GravitySph::coupled_pairs (cfl.rs:195-228): the gas pairs the force couples, 0 < r <
+ * 2 max(h_a, h_b) after a cold-start density solve, as (global a, global b), a < b, in
+ * ascending order; up to cap pairs are written to pairs_out[2 cap], *count_out = all. */
+int gx_sph_coupled_pairs(gx_handle* h, size_t n, const double* pos, const double* mass, const uint8_t* kind,
+                         uint64_t* pairs_out, size_t cap, size_t* count_out);
 /* density_adaptive (density.rs:86-96) over n gas particles: rho_out[n], h_out[n];
  * h_init[n] (nullable) seeds the brackets. */
 int gx_sph_density(gx_handle* h, size_t n, const double* pos, const double* mass, const double* h_init,

@@ -90,6 +90,9 @@ def lib():
             "or_gravity_sph_accelerations_active": (i, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, d, d, d, i, d, d, d,
                                                         d, d, d, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                         sz, _u32p, _f64p, i]),
+            "or_sph_velocity_divergence": (None, [sz, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, i]),
+            "or_sph_sf_fields": (None, [sz, _f64p, _f64p, _f64p, _u8p, d, d, _f64p, _f64p, i]),
+            "or_sph_coupled_pairs": (sz, [sz, _f64p, _f64p, _u8p, d, d, _u64p, sz, i]),
             "or_fixture_gas_star_mix": (None, [u64, sz, sz, _f64p, _f64p, _f64p, _u8p]),
             "or_fixture_sph_points": (None, [u64, sz, d, d, _f64p]),
         }
@@ -473,6 +476,42 @@ def sph_max_stable_dt(pos, vel, mass, kind, c_cfl, u=None, per_particle: bool = 
                                    float(p["n_ngb"]), float(p["h_tol_rel"]), float(c_cfl),
                                    None if vec is None else vec.ctypes.data, threads or max_threads())
     return (m, vec) if per_particle else m
+
+
+def sph_velocity_divergence(pos, vel, mass, rho, h, threads: int = 0) -> np.ndarray:
+    """divergence.rs:34-72 over a gas subset with given rho / h."""
+    pos, vel = _pos(pos), _pos(vel)
+    out = np.zeros(pos.shape[0])
+    lib().or_sph_velocity_divergence(pos.shape[0], pos.reshape(-1), vel.reshape(-1),
+                                     np.ascontiguousarray(mass, np.float64), np.ascontiguousarray(rho, np.float64),
+                                     np.ascontiguousarray(h, np.float64), out, threads or max_threads())
+    return out
+
+
+def sph_sf_fields(pos, vel, mass, kind, n_ngb=48.0, h_tol_rel=1e-3, threads: int = 0):
+    """GravitySph::sf_fields (gravity_sph.rs:353-382): state-indexed (rho, div_v)."""
+    pos, vel = _pos(pos), _pos(vel)
+    n = pos.shape[0]
+    rho, dv = np.zeros(n), np.zeros(n)
+    lib().or_sph_sf_fields(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64),
+                           np.ascontiguousarray(kind, np.uint8), float(n_ngb), float(h_tol_rel), rho, dv,
+                           threads or max_threads())
+    return rho, dv
+
+
+def sph_coupled_pairs(pos, mass, kind, n_ngb=48.0, h_tol_rel=1e-3, threads: int = 0) -> np.ndarray:
+    """cfl.rs:195-228 coupled_pairs: [P, 2] global index pairs, ascending."""
+    pos = _pos(pos)
+    n = pos.shape[0]
+    args = (n, pos.reshape(-1), np.ascontiguousarray(mass, np.float64), np.ascontiguousarray(kind, np.uint8),
+            float(n_ngb), float(h_tol_rel))
+    cap = 64 * max(n, 1)
+    out = np.zeros(2 * cap, dtype=np.uint64)
+    k = lib().or_sph_coupled_pairs(*args, out, cap, threads or max_threads())
+    if k > cap:
+        out = np.zeros(2 * k, dtype=np.uint64)
+        k = lib().or_sph_coupled_pairs(*args, out, k, threads or max_threads())
+    return out[:2 * k].reshape(-1, 2).copy()
 
 
 class GravitySph:

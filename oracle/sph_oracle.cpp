@@ -519,6 +519,85 @@ int or_gravity_sph_accelerations(size_t n, const double* pos, const double* vel,
   return 0;
 }
 
+// divergence.rs:34-72 velocity_divergence over a gas subset with given rho / h.
+void or_sph_velocity_divergence(size_t n, const double* pos, const double* vel, const double* mass, const double* rho,
+                                const double* h, double* div_out, int threads) {
+  if (n == 0) return;
+  double h_max = 0.0;
+  for (size_t i = 0; i < n; ++i) h_max = fmax_(h_max, h[i]);
+  HashGrid grid(pos, n, kSupport * h_max);
+#pragma omp parallel for num_threads(threads > 1 ? threads : 1) schedule(dynamic, 64)
+  for (size_t i = 0; i < n; ++i) {
+    std::vector<uint32_t> ngb;
+    grid.within(pos, ld(pos, i), kSupport * h[i], ngb);
+    double sum = 0.0;
+    for (uint32_t j : ngb) {
+      if (j == i) continue;
+      const D3 gw = grad_w(sub(ld(pos, i), ld(pos, j)), h[i]);
+      sum += mass[j] * dot(sub(ld(vel, j), ld(vel, i)), gw);
+    }
+    div_out[i] = sum / rho[i];
+  }
+}
+
+// gravity_sph.rs:353-382 GravitySph::sf_fields: cold-start density over the gas and the
+// divergence gather, scattered to the state's rows (collisionless rows 0, 0).
+void or_sph_sf_fields(size_t n, const double* pos, const double* vel, const double* mass, const uint8_t* kind,
+                      double n_ngb, double h_tol_rel, double* rho_out, double* div_out, int threads) {
+  for (size_t i = 0; i < n; ++i) rho_out[i] = div_out[i] = 0.0;
+  std::vector<size_t> gas;
+  gather_gas(n, kind, gas);
+  if (gas.empty()) return;
+  std::vector<double> gpos, gvel, gmass;
+  subset3(pos, gas, gpos);
+  subset3(vel, gas, gvel);
+  subset1(mass, gas, gmass);
+  const size_t ng = gas.size();
+  std::vector<double> rho(ng), h(ng), dv(ng);
+  or_sph_density_adaptive(ng, gpos.data(), gmass.data(), n_ngb, h_tol_rel, nullptr, rho.data(), h.data(), threads);
+  or_sph_velocity_divergence(ng, gpos.data(), gvel.data(), gmass.data(), rho.data(), h.data(), dv.data(), threads);
+  for (size_t k = 0; k < ng; ++k) {
+    rho_out[gas[k]] = rho[k];
+    div_out[gas[k]] = dv[k];
+  }
+}
+
+// cfl.rs:195-228 coupled_pairs: gas pairs (gas[a], gas[b]), a < b, with 0 < r <
+// 2 max(h_a, h_b) after a cold density solve, in ascending (a, b). Writes up to cap pairs
+// (2 per pair) and returns the count.
+size_t or_sph_coupled_pairs(size_t n, const double* pos, const double* mass, const uint8_t* kind, double n_ngb,
+                            double h_tol_rel, uint64_t* pairs_out, size_t cap, int threads) {
+  std::vector<size_t> gas;
+  gather_gas(n, kind, gas);
+  if (gas.empty()) return 0;
+  std::vector<double> gpos, gmass;
+  subset3(pos, gas, gpos);
+  subset1(mass, gas, gmass);
+  const size_t ng = gas.size();
+  std::vector<double> rho(ng), h(ng);
+  or_sph_density_adaptive(ng, gpos.data(), gmass.data(), n_ngb, h_tol_rel, nullptr, rho.data(), h.data(), threads);
+  double h_max = 0.0;
+  for (size_t k = 0; k < ng; ++k) h_max = fmax_(h_max, h[k]);
+  HashGrid grid(gpos.data(), ng, kSupport * h_max);
+  size_t count = 0;
+  std::vector<uint32_t> ngb;
+  for (size_t a = 0; a < ng; ++a) {
+    grid.within(gpos.data(), ld(gpos.data(), a), kSupport * h_max, ngb);
+    for (uint32_t b : ngb) {
+      if (b <= a) continue;
+      const double r = length(sub(ld(gpos.data(), a), ld(gpos.data(), b)));
+      if (r > 0.0 && r < kSupport * fmax_(h[a], h[b])) {
+        if (count < cap) {
+          pairs_out[2 * count] = gas[a];
+          pairs_out[2 * count + 1] = gas[b];
+        }
+        ++count;
+      }
+    }
+  }
+  return count;
+}
+
 // gravity_sph.rs:247-286 GravitySph::accelerations_active (fresh gravity on all n), with
 // :101-150 active_gas: h_scratch (shared with or_gravity_sph_accelerations' h_hint) and
 // rho_scratch hold the persistent gas-subset scratch; a scratch that is not set forces a

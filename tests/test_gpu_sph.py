@@ -337,3 +337,22 @@ def test_sph_accelerations_active_matches_oracle(oracle):
         assert np.array_equal(a[stale], grav[stale])  # inactive gas rows: gravity only
     with pytest.raises(gb.GxError):
         s.accelerations_active(st, np.array([len(st)], np.uint32))
+
+
+def test_sf_fields_and_coupled_pairs_match_oracle(oracle):
+    # gravity_sph.rs:353-382 (rho, div v) and cfl.rs:195-228 (coupled pairs), cold start
+    st = mix_state(oracle, 0x5F5F, 1200, 2400)
+    st.vel[st.kind == 1] += -0.3 * st.pos[st.kind == 1]  # a converging gas flow
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5)
+    rho, dv = s.sf_fields(st)
+    rr, dr = oracle.sph_sf_fields(st.pos, st.vel, st.mass, st.kind)
+    gas = st.kind == 1
+    assert not rho[~gas].any() and not dv[~gas].any()
+    assert np.max(rel(rho[gas], rr[gas])) <= 1e-12
+    assert np.max(np.abs(dv[gas] - dr[gas])) <= 1e-10 * np.sqrt(np.mean(dr[gas] ** 2))
+    assert np.mean(dv[gas] < 0) > 0.9  # converging flow
+    pairs = s.coupled_pairs(st)
+    ref = oracle.sph_coupled_pairs(st.pos, st.mass, st.kind)
+    assert np.array_equal(pairs, ref)
+    empty = gb.State(st.pos, st.vel, st.mass)  # no gas
+    assert s.coupled_pairs(empty).shape == (0, 2) and not s.sf_fields(empty)[0].any()
