@@ -9,7 +9,7 @@
 //! Written against include/galaxy_b200.h; DVec3 is three f64 (`#[repr(C)]`-compatible
 //! in glam), so `&[DVec3]` is passed as `*const f64` with no copy.
 
-use galaxy_core::{DVec3, ForceSolver, State};
+use galaxy_core::{DVec3, ForceSolver, SfFields, State};
 use galaxy_solvers::sph::{DensityConfig, Eos, HydroParams};
 use std::ffi::CStr;
 use std::os::raw::{c_char, c_int};
@@ -74,6 +74,10 @@ extern "C" {
     fn gx_sph_accelerations_active(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64,
                                    mass: *const f64, kind: *const u8, u: *const f64, n_active: usize,
                                    active: *const u32, acc: *mut f64) -> c_int;
+    fn gx_sph_sf_fields(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
+                        kind: *const u8, rho: *mut f64, div: *mut f64) -> c_int;
+    fn gx_sph_coupled_pairs(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, kind: *const u8,
+                            pairs: *mut u64, cap: usize, count: *mut usize) -> c_int;
 }
 
 extern "C" {
@@ -314,6 +318,34 @@ impl ForceSolver for GpuGravitySphB200 {
         let rc = unsafe { gx_potential_energy(self.h, state.len(), as_f64(&state.pos), state.mass.as_ptr(), &mut out) };
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
         out
+    }
+
+    fn sf_fields(&self, state: &State) -> SfFields {
+        let n = state.len();
+        let (mut rho, mut div_v) = (vec![0.0; n], vec![0.0; n]);
+        let rc = unsafe {
+            gx_sph_sf_fields(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                             state.kind.as_ptr() as *const u8, rho.as_mut_ptr(), div_v.as_mut_ptr())
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+        SfFields { rho, div_v }
+    }
+
+    fn coupled_pairs(&self, state: &State) -> Vec<(usize, usize)> {
+        let n = state.len();
+        let mut count = 0usize;
+        let mut buf = vec![0u64; 2 * 64 * n.max(1)];
+        let mut call = |buf: &mut Vec<u64>, count: &mut usize| unsafe {
+            gx_sph_coupled_pairs(self.h, n, as_f64(&state.pos), state.mass.as_ptr(), state.kind.as_ptr() as *const u8,
+                                 buf.as_mut_ptr(), buf.len() / 2, count)
+        };
+        let mut rc = call(&mut buf, &mut count);
+        if rc == 0 && 2 * count > buf.len() {
+            buf = vec![0u64; 2 * count];
+            rc = call(&mut buf, &mut count);
+        }
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+        (0..count).map(|k| (buf[2 * k] as usize, buf[2 * k + 1] as usize)).collect()
     }
 }
 
