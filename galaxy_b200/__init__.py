@@ -378,18 +378,21 @@ class GpuGravitySph(GpuLbvh):
     def max_stable_dt_per_particle(self, state, c_cfl: float = 1.0) -> np.ndarray:
         """cfl.rs:134-185 (gravity_sph.rs:380-386 at Courant number 1): state-indexed,
         +inf on collisionless rows; h from a cold-start density solve."""
-        out = np.full(len(state), np.inf)
-        gas = state.gas()
-        if gas.size:
-            gpos, gvel = state.pos[gas], state.vel[gas]
-            _, h = self.density(gpos, state.mass[gas])
-            dt, _ = self.cfl(gpos, gvel, h, c_cfl, state.u[gas])
-            out[gas] = dt
+        out = np.empty(len(state))
+        m = C.c_double()
+        self._ck(lib().gx_sph_max_stable_dt(self._h, len(state), _ptr(state.pos), _ptr(state.vel),
+                                            _ptr(state.mass), _ptr(state.kind), _ptr(state.u), float(c_cfl),
+                                            _ptr(out), C.byref(m)))
         return out
 
     def max_stable_dt(self, state, c_cfl: float = 1.0) -> float:
-        """ForceSolver::max_stable_dt of GravitySph (gravity_sph.rs:371-378; cfl.rs:49-125)."""
-        return float(self.max_stable_dt_per_particle(state, c_cfl).min()) if len(state) else float("inf")
+        """ForceSolver::max_stable_dt of GravitySph (gravity_sph.rs:371-378; cfl.rs:49-125),
+        reduced on the device."""
+        m = C.c_double()
+        self._ck(lib().gx_sph_max_stable_dt(self._h, len(state), _ptr(state.pos), _ptr(state.vel),
+                                            _ptr(state.mass), _ptr(state.kind), _ptr(state.u), float(c_cfl),
+                                            None, C.byref(m)))
+        return m.value
 
 
 class LeapfrogKdk:

@@ -1657,6 +1657,43 @@ int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* ve
   return GX_OK;
 }
 
+int gx_sph_max_stable_dt(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                         const uint8_t* kind, const double* u, double c_cfl, double* dt_out, double* min_out) {
+  if (!h) return GX_ERR_INVALID_ARG;
+  if (int rc = need_sph(h)) return rc;
+  const double inf = std::numeric_limits<double>::infinity();
+  if (dt_out) std::fill(dt_out, dt_out + n, inf);
+  if (min_out) *min_out = inf;
+  if (n == 0) return GX_OK;
+  if (!pos || !vel || !mass) return fail(h, GX_ERR_INVALID_ARG, "null array");
+  std::vector<uint32_t> gas;
+  int rc = gas_map(h, n, kind, gas);
+  if (rc || gas.empty()) return rc;
+  cudaSetDevice(h->device);
+  h->sph_host_hint_ngas = 0;
+  rc = host_sph_setup(h, n, pos, vel, mass, &gas, false, true);  // cfl.rs:66: a cold-start solve
+  if (rc) return rc;
+  const size_t ng = gas.size();
+  if (u) {
+    std::vector<double> gu(ng);
+    for (size_t k = 0; k < ng; ++k) gu[k] = u[gas[k]];
+    GX_CK(h, cudaMemcpy(h->sph.gu, gu.data(), ng * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const StepBufs& b = h->ar.b;
+  sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, nullptr, true, false, b.ctl, h->stream);
+  sph_enqueue_cfl(h->sph, b.pos, b.vel, c_cfl, true, b.ctl, h->stream);
+  unsigned long long enc = 0;
+  std::vector<double> dt(ng);
+  GX_CK(h, cudaMemcpyAsync(&enc, &h->sph.sc->min_dt_enc, sizeof enc, cudaMemcpyDeviceToHost, h->stream));
+  GX_CK(h, cudaMemcpyAsync(dt.data(), h->sph.dtv, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  rc = finish(h, false);
+  if (rc) return rc;
+  if (dt_out)
+    for (size_t k = 0; k < ng; ++k) dt_out[gas[k]] = dt[k];
+  if (min_out) *min_out = -dec_max_host(enc);
+  return GX_OK;
+}
+
 int gx_sph_coupled_pairs(gx_handle* h, size_t n, const double* pos, const double* mass, const uint8_t* kind,
                          uint64_t* pairs_out, size_t cap, size_t* count_out) {
   if (!h || !count_out) return GX_ERR_INVALID_ARG;

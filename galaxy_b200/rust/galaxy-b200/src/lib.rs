@@ -76,6 +76,8 @@ extern "C" {
                                    active: *const u32, acc: *mut f64) -> c_int;
     fn gx_sph_sf_fields(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
                         kind: *const u8, rho: *mut f64, div: *mut f64) -> c_int;
+    fn gx_sph_max_stable_dt(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
+                            kind: *const u8, u: *const f64, c_cfl: f64, dt: *mut f64, min: *mut f64) -> c_int;
     fn gx_sph_coupled_pairs(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, kind: *const u8,
                             pairs: *mut u64, cap: usize, count: *mut usize) -> c_int;
 }
@@ -318,6 +320,27 @@ impl ForceSolver for GpuGravitySphB200 {
         let rc = unsafe { gx_potential_energy(self.h, state.len(), as_f64(&state.pos), state.mass.as_ptr(), &mut out) };
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
         out
+    }
+
+    fn max_stable_dt(&self, state: &State) -> f64 {
+        let mut m = f64::INFINITY;
+        let rc = unsafe {
+            gx_sph_max_stable_dt(self.h, state.len(), as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                 state.kind.as_ptr() as *const u8, state.u.as_ptr(), 1.0, std::ptr::null_mut(), &mut m)
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+        m
+    }
+
+    fn max_stable_dt_per_particle(&self, state: &State) -> Vec<f64> {
+        let mut dt = vec![f64::INFINITY; state.len()];
+        let mut m = f64::INFINITY;
+        let rc = unsafe {
+            gx_sph_max_stable_dt(self.h, state.len(), as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                 state.kind.as_ptr() as *const u8, state.u.as_ptr(), 1.0, dt.as_mut_ptr(), &mut m)
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+        dt
     }
 
     fn sf_fields(&self, state: &State) -> SfFields {

@@ -241,6 +241,12 @@ int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const
  * collisionless rows 0. */
 int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                      const uint8_t* kind, double* rho_out, double* div_out);
+/* GravitySph::max_stable_dt_per_particle / max_stable_dt (gravity_sph.rs:364-380;
+ * cfl.rs:49-185): after a cold-start density solve of the gas, dt_out[n] (nullable) gets
+ * c_cfl h_i / v_sig,i on gas rows and +inf elsewhere; *min_out (nullable) its minimum
+ * (+inf without gas). The reference's trait methods use c_cfl = 1. */
+int gx_sph_max_stable_dt(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                         const uint8_t* kind, const double* u, double c_cfl, double* dt_out, double* min_out);
 /* GravitySph::coupled_pairs (cfl.rs:195-228): the gas pairs the force couples, 0 < r <
  * 2 max(h_a, h_b) after a cold-start density solve, as (global a, global b), a < b, in
  * ascending order; up to cap pairs are written to pairs_out[2 cap], *count_out = all. */

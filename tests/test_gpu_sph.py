@@ -356,3 +356,13 @@ def test_sf_fields_and_coupled_pairs_match_oracle(oracle):
     assert np.array_equal(pairs, ref)
     empty = gb.State(st.pos, st.vel, st.mass)  # no gas
     assert s.coupled_pairs(empty).shape == (0, 2) and not s.sf_fields(empty)[0].any()
+
+
+def test_max_stable_dt_per_particle_matches_oracle(oracle):
+    # cfl.rs:134-185 through one call: state-indexed, +inf on collisionless rows
+    st = mix_state(oracle, 0xA5F0, 400, 800)
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5)
+    dt = s.max_stable_dt_per_particle(st, 0.25)
+    m, ref = oracle.sph_max_stable_dt(st.pos, st.vel, st.mass, st.kind, 0.25, per_particle=True)
+    assert np.all(np.isinf(dt[st.kind == 0]))
+    assert np.array_equal(dt, ref) and s.max_stable_dt(st, 0.25) == m
