@@ -519,7 +519,7 @@ def run_precision(args):
 # Kernels a gas-mode step adds to the 8 of the gravity step: gather, scalars, 3 grids
 # (keys, histogram, 4 sort passes, fill, mixed flags), seeds, density cell, density, h_max,
 # hydro cell, pack, hydro, scatter.
-SPH_LAUNCHES_PER_STEP = 2 + 3 * 8 + 9
+SPH_LAUNCHES_PER_STEP = 2 + 3 * 8 + 8
 
 
 def sph_roofline(n_gas: int, stage: dict, peaks: dict) -> dict:
