@@ -168,3 +168,48 @@ def test_state_species_columns():
     assert list(st.gas()) == [0, 2] and st.u.shape == (4,)
     with pytest.raises(ValueError):
         gb.State(np.zeros((4, 3)), np.zeros((4, 3)), np.ones(4), kind=[1, 0])
+
+
+def test_active_path_semantics(oracle):
+    # gravity_sph.rs:101-150, 247-286: the first call refreshes every gas particle (equal to
+    # the full pass); later calls leave inactive gas rows at gravity alone.
+    pos, vel, mass, kind = oracle.fixture_gas_star_mix(0xA5F0, 300, 600)
+    full = oracle.GravitySph(1.0, 0.05, 0.5).accelerations(pos, vel, mass, kind)
+    g = oracle.GravitySph(1.0, 0.05, 0.5)
+    assert np.array_equal(g.accelerations_active(pos, vel, mass, kind, np.arange(len(pos))), full)
+    act = np.arange(0, len(pos), 5)
+    moved = pos + 1e-4
+    a = g.accelerations_active(moved, vel, mass, kind, act)
+    grav = oracle.lbvh_accelerations(moved, mass, 1.0, 0.05, 0.5)
+    stale = np.setdiff1d(np.flatnonzero(kind == 1), act)
+    assert np.array_equal(a[stale], grav[stale])
+    fresh = np.intersect1d(np.flatnonzero(kind == 1), act)
+    assert not np.array_equal(a[fresh], grav[fresh])
+
+
+def test_coupled_pairs_against_brute_force(oracle):
+    # cfl.rs:195-228: every pair with 0 < r < 2 max(h_a, h_b), once, ascending
+    pos, vel, mass, kind = oracle.fixture_gas_star_mix(0x1111, 150, 300)
+    pairs = oracle.sph_coupled_pairs(pos, mass, kind)
+    gas = np.flatnonzero(kind == 1)
+    _, h = oracle.sph_density_adaptive(pos[gas], mass[gas])
+    want = []
+    for a in range(gas.size):
+        for b in range(a + 1, gas.size):
+            r = np.sqrt(np.sum((pos[gas[a]] - pos[gas[b]]) ** 2))
+            if 0.0 < r < 2.0 * max(h[a], h[b]):
+                want.append((gas[a], gas[b]))
+    assert np.array_equal(pairs, np.array(want, dtype=np.uint64).reshape(-1, 2))
+
+
+def test_velocity_divergence_sign(oracle):
+    # divergence.rs docs: a converging linear flow gives div v < 0, a diverging one > 0
+    pos = oracle.fixture_sph_points(3, 800, 2.0)
+    mass = np.ones(800)
+    rho, h = oracle.sph_density_adaptive(pos, mass)
+    assert np.all(oracle.sph_velocity_divergence(pos, -0.5 * pos, mass, rho, h) < 0)
+    assert np.all(oracle.sph_velocity_divergence(pos, 0.5 * pos, mass, rho, h) > 0)
+    kind = np.ones(800, np.uint8)
+    kind[::2] = 0
+    r, d = oracle.sph_sf_fields(pos, -0.5 * pos, mass, kind)
+    assert not r[kind == 0].any() and not d[kind == 0].any() and np.all(r[kind == 1] > 0)
