@@ -1,4 +1,5 @@
-// gx_sph.cu -- SPH on the gas subset: adaptive-h density, hydro force, CFL bound.
+// gx_sph.cu -- SPH on the gas subset: adaptive-h density, hydro force, CFL bound,
+// velocity divergence and coupled pairs.
 //
 // Reference (file:line in the galaxy project):
 //   solvers/src/sph/kernel.rs:23-53      cubic spline W(r, h) and grad W
@@ -7,29 +8,33 @@
 //                                        solve_one (bracket, expand, shrink, bisection)
 //   solvers/src/sph/forces.rs:223-379    HydroCtx::force_one: symmetric P/rho^2 + Monaghan
 //                                        viscosity, grad-averaged kernel, du/dt partner
-//   solvers/src/sph/cfl.rs:49-185        v_sig,i and dt_i = c_cfl h_i / v_sig,i
-//   solvers/src/sph/gravity_sph.rs:172-207  hydro added to the gas rows after gravity
+//   solvers/src/sph/cfl.rs:49-228        v_sig,i and dt_i = c_cfl h_i / v_sig,i; coupled pairs
+//   solvers/src/sph/divergence.rs:34-72  div v for the star-formation fields
+//   solvers/src/sph/gravity_sph.rs       hydro added to the gas rows after gravity; the
+//                                        active-subset pass over a persistent scratch
 //   gpu/src/gpu_resident.rs:1537-1565    the resident order: gravity walk, then density,
 //                                        hydro and the scatter-add into the gas rows
 //
 // Design. Every stage is FP64 and keeps the reference's per-pair operation order (this
-// file is compiled without FMA contraction). The gas is binned into a uniform grid whose
+// file is compiled without FMA contraction). The gas is binned into uniform grids whose
 // cells are hashed into T = 2^k buckets; a stable radix sort by bucket (the library's
 // onesweep sort) makes every bucket a contiguous run of cell-sorted copies of the gas
-// (positions + mass, cell coordinates), so a query reads whole runs. A cell's bucket may
-// also hold another cell's particles; queries accept a particle only when its stored cell
-// is the queried one, so each particle is seen once. Cell coordinates are clamped to the
-// int32 range (monotone, so a clamped query box still covers its ball). One warp serves
-// one target: its lanes walk the query box's buckets 32 at a time as one flattened list.
-// The density warp keeps its candidates (radius, sorted slot) in shared memory and
-// evaluates every bisection step from there (streaming the box again only when more than
-// kCandCap candidates fall inside). It gathers a ball of 2.5 x the bracket seed instead
-// of the reference's 2 x hi = 4 x seed: a comparison whose count needs a wider ball is
-// settled by the lower bound of the gathered part when that clears n_ngb, else the
-// gather widens first, so every comparison is the reference's. Sums are lane-strided and reduced by a
-// fixed shuffle tree, so results are deterministic; against the reference's ascending
-// serial sum they differ by rounding only. The CFL bound is a max over pairs and a min
-// over targets, so it is exact given the same h.
+// (positions + mass, cell coordinates), so a query reads whole runs. A bucket may also
+// hold another cell's particles: a bucket of one cell is matched against the queried cell
+// once, a mixed bucket particle by particle, so each particle is seen once. Cell
+// coordinates are clamped to the int32 range (monotone, so a clamped query box still
+// covers its ball). One warp serves one target: its lanes walk the query box's buckets
+// 32 at a time as one flattened list. The density warp keeps its candidates (radius,
+// sorted slot) in shared memory and evaluates every bisection step from there (streaming
+// the box again only when more than kCandCap candidates fall inside). It gathers a ball
+// of 2.5 x the bracket seed instead of the reference's 2 x hi = 4 x seed: a comparison
+// whose count needs a wider ball is settled by the lower bound of the gathered part when
+// that clears n_ngb, else the gather widens first, so every comparison is the reference's.
+// The hydro warp lists the neighbours that pass a support test, then runs the pair
+// arithmetic 32 pairs at a time. Sums are lane-strided and reduced by a fixed shuffle
+// tree, so results are deterministic; against the reference's ascending serial sums they
+// differ by rounding only. The CFL bound is a max over pairs and a min over targets, and
+// the coupled pairs a set, so both are exact given the same h.
 #include <cmath>
 #include <cstring>
 #include <mutex>
