@@ -213,3 +213,19 @@ def test_velocity_divergence_sign(oracle):
     kind[::2] = 0
     r, d = oracle.sph_sf_fields(pos, -0.5 * pos, mass, kind)
     assert not r[kind == 0].any() and not d[kind == 0].any() and np.all(r[kind == 1] > 0)
+
+
+def test_cfl_vector_min_and_static_closed_form(oracle):
+    # solvers/tests/sph_cfl_vector.rs:56-80, 153-180: the per-particle vector's min is the
+    # scalar bound bit for bit; a static isothermal cloud has dt_i = c_cfl h_i / (2 c_s).
+    pos = oracle.fixture_sph_points(21, 600, 2.5)
+    vel = oracle.fixture_sph_points(22, 600, 1.5)
+    kind = np.ones(600, np.uint8)
+    m, vec = oracle.sph_max_stable_dt(pos, vel, np.ones(600), kind, 0.25, per_particle=True)
+    assert vec.min() == m
+    c_s = 2.0
+    pos = oracle.fixture_sph_points(11, 800, 3.0)
+    _, h = oracle.sph_density_adaptive(pos, np.ones(800))
+    _, vec = oracle.sph_max_stable_dt(pos, np.zeros((800, 3)), np.ones(800), np.ones(800, np.uint8), 0.25,
+                                      per_particle=True, eos=0, eos_param=c_s)
+    assert np.max(np.abs(vec - 0.25 * h / (2.0 * c_s)) / (0.25 * h / (2.0 * c_s))) < 1e-9
