@@ -136,6 +136,41 @@ def cpu_sample_step(st, params, threads: int, n_targets: int, rng) -> float:
     return t_build + max(t_walk, 0.0) * n / n_targets
 
 
+def run_reference_sph(args, threads: int):
+    """The gas-mode reference arm: the oracle's GravitySph (Lbvh gravity + adaptive-h density
+    + hydro, h warm-started across steps) driving LeapfrogKdk on a bounded sample of the
+    same gas/star mix (--gas / 16 gas particles and as many stars), per particle."""
+    from galaxy_b200 import workloads
+    from oracle import oracle
+
+    ng = max(args.gas // 16, 4096)
+    st = workloads.gas_star_mix(ng, ng, seed=0)
+    n = len(st)
+    gs = oracle.GravitySph(1.0, 0.01, 0.5, threads=threads)
+    pos, vel = st.pos.copy(), st.vel.copy()
+    gs.step_many(pos, vel, st.mass, st.kind, 1e-4, max(args.warmup, 1))  # prime + warm-up steps
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        gs.step_many(pos, vel, st.mass, st.kind, 1e-4, 1)
+        times.append(time.perf_counter() - t0)
+    t_step = statistics.mean(times)
+    value = n / t_step
+    sample = (f"per step: one KDK step of a {n}-particle gas/star mix ({ng} gas) through the oracle's "
+              f"GravitySph with {threads} threads (C++ restatement of the reference; the Rust crate cannot "
+              f"be built here), per particle")
+    line = {"impl": "reference", "metric": "particle-steps/s (resident KDK step with SPH on the gas subset)",
+            "value": value, "unit": "particle-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"gas-star-mix-{args.gas}+{args.gas}", "sample_particles": n, "gas": ng,
+                       "eps": 0.01, "theta": 0.5, "dt": 1e-4},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     dist, rank, ws, local = ranks.init()
     if rank != 0:
@@ -146,6 +181,11 @@ def run_reference(args):
     from oracle import oracle
 
     threads = os.cpu_count() or 1
+    if args.config == "sph":
+        run_reference_sph(args, threads)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     st, p = workload(args.config, 0)
     n = len(st)
     rng = np.random.default_rng(1)
