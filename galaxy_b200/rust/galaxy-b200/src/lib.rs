@@ -76,6 +76,8 @@ extern "C" {
                                    active: *const u32, acc: *mut f64) -> c_int;
     fn gx_sph_sf_fields(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
                         kind: *const u8, rho: *mut f64, div: *mut f64) -> c_int;
+    fn gx_sph_accel_and_dudt(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
+                             kind: *const u8, u: *const f64, acc: *mut f64, dudt: *mut f64) -> c_int;
     fn gx_sph_max_stable_dt(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
                             kind: *const u8, u: *const f64, c_cfl: f64, dt: *mut f64, min: *mut f64) -> c_int;
     fn gx_sph_coupled_pairs(h: *mut GxHandle, n: usize, pos: *const f64, mass: *const f64, kind: *const u8,
@@ -299,6 +301,18 @@ impl ForceSolver for GpuGravitySphB200 {
         let rc = unsafe {
             gx_sph_accelerations(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
                                  state.kind.as_ptr() as *const u8, state.u.as_ptr(), acc.as_mut_ptr() as *mut f64)
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    fn accel_and_dudt(&mut self, state: &State, acc: &mut [DVec3], dudt: &mut [f64]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        assert_eq!(dudt.len(), n, "dudt length must match particle count");
+        let rc = unsafe {
+            gx_sph_accel_and_dudt(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                  state.kind.as_ptr() as *const u8, state.u.as_ptr(), acc.as_mut_ptr() as *mut f64,
+                                  dudt.as_mut_ptr())
         };
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
     }
