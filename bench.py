@@ -333,7 +333,7 @@ def run_ours(args):
                            "l2": (f"working set ~{352 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)" if 352 * n > 126e6 else
                                   f"working set ~{352 * n / 1e6:.0f} MB fits in L2: steps replay back to back with the state resident, as a resident integrator runs (not a flushed-cache number)"),
                            "cuda_graph": True,
-                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}},
+                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm", "walk_group")}},
                 "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "walk_counts": counts}
         print(json.dumps(line), flush=True)
@@ -410,7 +410,7 @@ def run_batched(args):
                                "how": "same systems, one single-system handle each, stepped one after another "
                                       "(device time of each step summed)"},
                 "batched_over_plain": value / plain, "gpu_launches": (12 if k63 else 8) * args.steps, "clocks": clk,
-                "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}}
+                "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm", "walk_group")}}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -678,7 +678,7 @@ def run_sph(args):
                                                         "beta 2, warm-started h",
                            "parallelism": "replicas" if ws > 1 else "single system", "cuda_graph": True,
                            "l2": f"working set ~{900 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)",
-                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}},
+                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm", "walk_group")}},
                 "gas_particle_steps_per_s": ng * ws * args.steps / (ms_max / 1e3),
                 "e2e": e2e, "gpu_launches": (8 + SPH_LAUNCHES_PER_STEP) * args.steps, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "sph_share_of_step": gas_frac, "min_stable_dt_c0.25": cfl,

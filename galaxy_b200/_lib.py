@@ -48,6 +48,7 @@ class Options(C.Structure):
         ("device", C.c_int32),
         ("walk_block", C.c_uint32),
         ("walk_ctas_per_sm", C.c_uint32),
+        ("walk_group", C.c_uint32),
     ]
 
 
@@ -90,11 +91,12 @@ class Tuning(C.Structure):
     _fields_ = [
         ("walk_block", C.c_uint32),
         ("walk_ctas_per_sm", C.c_uint32),
+        ("walk_group", C.c_uint32),
         ("ms", C.c_float),
     ]
 
 
-GX_TUNE_MAX_CANDIDATES = 8
+GX_TUNE_MAX_CANDIDATES = 24
 
 
 class BatchStats(C.Structure):

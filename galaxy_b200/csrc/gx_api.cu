@@ -60,6 +60,22 @@ bool check_device(int device, std::string& err) {
   return true;
 }
 
+bool options_valid(const gx_options& o) {
+  return o.precision <= GX_PREC_F64 && o.multipole <= GX_MULTIPOLE_QUAD &&
+         !(o.walk_block && (o.walk_block % 32 || o.walk_block > static_cast<uint32_t>(kWalkThreads))) &&
+         (o.walk_group == 0 || o.walk_group == 8 || o.walk_group == 16 || o.walk_group == 32);
+}
+
+// Once per device, with the device current: kernel attributes the launches rely on.
+void prepare_device(int dev) {
+  static std::mutex mu;
+  static uint64_t done = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64 || (done >> dev) & 1u) return;
+  walk_prepare();
+  done |= 1ull << dev;
+}
+
 // ---- Arena: one system's device buffers -------------------------------------------
 void Arena::release() {
   for (void* p : allocs)
@@ -95,7 +111,7 @@ size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
   s += n * 8;                                 // slots
   if (quad) s += 2 * n * 16 + 6 * n * 8;
   if (f64rec) s += n * sizeof(Node64);
-  s += tiles * sizeof(TileDesc) + (n / 32 + nsys + 1) * sizeof(WalkItem);
+  s += tiles * sizeof(TileDesc) + (n / 8 + nsys + 1) * sizeof(WalkItem);
   s += nsys * (sizeof(SysDesc) + sizeof(Bounds) + 48 + kMaxRadixPasses * kRadixBins * 4);
   s += kMaxRadixPasses * tiles * kRadixBins * 4 + 64;
   s += (n / 256 + 1) * 8 * 8;  // diagnostic partials
@@ -211,7 +227,8 @@ void make_tables(const std::vector<SysDesc>& in, std::vector<SysDesc>& sys, std:
       tiles.push_back(t);
     }
     d.ntiles = static_cast<uint32_t>(tiles.size()) - d.first_tile;
-    for (uint32_t b0 = 0; b0 < d.n; b0 += 32) items.push_back(WalkItem{d.off + b0, s});
+    if (d.group != 8 && d.group != 16) d.group = 32;
+    for (uint32_t b0 = 0; b0 < d.n; b0 += d.group) items.push_back(WalkItem{d.off + b0, s});
   }
 }
 
@@ -250,15 +267,32 @@ void tuned_store(int device, const gx_options& opt, int batched, size_t n, const
   g_tune[tune_key(device, opt, batched, n)] = t;
 }
 
-std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid) {
+// Targets a warp of the FP32 walk when nothing is tuned: narrow groups for small systems,
+// whose walk is the latency of few warps (more warps, tighter group boxes), 32 targets
+// for large ones.
+uint32_t default_walk_group(size_t n) { return n < (size_t{1} << 16) ? 8u : n < (size_t{1} << 19) ? 16u : 32u; }
+
+uint32_t system_walk_group(int device, const gx_options& opt, size_t n) {
+  if (opt.precision == GX_PREC_F64) return 32u;  // the FP64 walk takes 32 targets a warp
+  if (opt.walk_group) return opt.walk_group;
+  gx_tuning t;
+  if (tuned_lookup(device, opt, 0, n, &t) && t.walk_group) return t.walk_group;
+  return default_walk_group(n);
+}
+
+std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid, bool with_groups) {
   std::vector<gx_tuning> out;
-  for (int block : {64, kWalkThreads}) {
-    WalkCfg c = base;
-    c.block = block;
-    const int full = walk_resident_ctas(c);
-    if (with_grid) out.push_back(gx_tuning{static_cast<uint32_t>(block), 0u, 0.f});
-    if (full / 2 >= 1) out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full / 2), 0.f});
-    out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full), 0.f});
+  const std::vector<uint32_t> groups = with_groups ? std::vector<uint32_t>{8u, 16u, 32u} : std::vector<uint32_t>{0u};
+  for (uint32_t grp : groups) {
+    for (int block : {64, kWalkThreads}) {
+      WalkCfg c = base;
+      c.block = block;
+      const int full = walk_resident_ctas(c);
+      if (with_grid) out.push_back(gx_tuning{static_cast<uint32_t>(block), 0u, grp, 0.f});
+      if (full / 2 >= 1)
+        out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full / 2), grp, 0.f});
+      out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full), grp, 0.f});
+    }
   }
   if (out.size() > GX_TUNE_MAX_CANDIDATES) out.resize(GX_TUNE_MAX_CANDIDATES);
   return out;
@@ -281,6 +315,7 @@ struct gx_handle {
   // current layout
   size_t n_layout = 0;
   double dt_layout = 0.0;
+  uint32_t group_layout = 0;  // targets a warp of the laid-out walk items
   // resident state
   size_t n = 0;
   double time = 0.0;
@@ -348,7 +383,9 @@ WalkCfg walk_cfg(const gx_handle* h) {
 // Lay out one system of n particles (tables + SysDesc) with step dt.
 int layout(gx_handle* h, size_t n, double dt) {
   if (n > (1u << 30)) return fail(h, GX_ERR_INVALID_ARG, "N above 2^30 is not supported (30-bit look-back counts)");
-  if (n == h->n_layout && dt == h->dt_layout && h->ar.cap_n >= n) return GX_OK;
+  if (n == h->n_layout && dt == h->dt_layout && h->ar.cap_n >= n &&
+      system_walk_group(h->device, h->opt, n) == h->group_layout)
+    return GX_OK;
   std::vector<SysDesc> in(1), sys;
   in[0].off = 0;
   in[0].n = static_cast<uint32_t>(n);
@@ -356,12 +393,15 @@ int layout(gx_handle* h, size_t n, double dt) {
   in[0].eps = h->eps;
   in[0].theta = h->theta;
   in[0].dt = dt;
+  in[0].group = system_walk_group(h->device, h->opt, n);
   std::vector<TileDesc> tiles;
   std::vector<WalkItem> items;
   make_tables(in, sys, tiles, items);
   const int quad = h->opt.multipole == GX_MULTIPOLE_QUAD;
   const int f64 = h->opt.precision == GX_PREC_F64;
-  GX_CK(h, h->ar.ensure(n, tiles.size(), items.size(), 1, quad, f64, h->stream));
+  // Items are sized for the narrowest grouping, so a new grouping never reallocates
+  // (which would lose the resident state).
+  GX_CK(h, h->ar.ensure(n, tiles.size(), std::max(items.size(), n / 8 + 2), 1, quad, f64, h->stream));
   StepBufs& b = h->ar.b;
   b.n = static_cast<uint32_t>(n);
   b.key64 = (h->opt.flags & GX_FLAG_MORTON63) ? 1 : 0;
@@ -378,6 +418,7 @@ int layout(gx_handle* h, size_t n, double dt) {
   GX_CK(h, cudaStreamSynchronize(h->stream));
   h->n_layout = n;
   h->dt_layout = dt;
+  h->group_layout = sys[0].group;
   if (h->step_graph) {
     cudaGraphExecDestroy(h->step_graph);
     h->step_graph = nullptr;
@@ -518,8 +559,7 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
     }
     o = *opt;
   }
-  if (o.precision > GX_PREC_F64 || o.multipole > GX_MULTIPOLE_QUAD ||
-      (o.walk_block && (o.walk_block % 32 || o.walk_block > static_cast<uint32_t>(kWalkThreads)))) {
+  if (!options_valid(o)) {
     set_global_err("invalid gx_options");
     return GX_ERR_INVALID_ARG;
   }
@@ -538,6 +578,7 @@ int gx_create(double g, double softening, double theta, const gx_options* opt, g
   h->device = dev;
   cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaSetDevice(dev);
+  if (e == cudaSuccess) prepare_device(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
   for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&h->chunk_ev[i], cudaEventDisableTiming);
@@ -1159,12 +1200,17 @@ int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* trie
   const gx_options user = h->opt;
   const uint32_t reps = repeats ? repeats : 3;
   WalkCfg base = walk_cfg(h);
-  std::vector<gx_tuning> cand = tune_candidates(base, true);
+  // the FP64 walk has one grouping
+  std::vector<gx_tuning> cand = tune_candidates(base, true, h->opt.precision != GX_PREC_F64);
   StepBufs& b = h->ar.b;
+  const double dt_keep = h->dt_layout;
   int best_i = -1;
   for (size_t i = 0; i < cand.size() && rc == GX_OK; ++i) {
     h->opt.walk_block = cand[i].walk_block;
     h->opt.walk_ctas_per_sm = cand[i].walk_ctas_per_sm;
+    h->opt.walk_group = cand[i].walk_group;
+    rc = layout(h, h->n, dt_keep);  // walk items of this grouping
+    if (rc) break;
     // Force evaluations on the current positions recompute a(x) bit for bit, so the
     // resident state is untouched whatever the candidate.
     enqueue_force(h, b, 0, 0, false);
@@ -1189,9 +1235,19 @@ int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* trie
     cudaGraphExecDestroy(h->step_graph);
     h->step_graph = nullptr;
   }
-  if (rc) return rc;
+  if (rc) {
+    layout(h, h->n, dt_keep);
+    return rc;
+  }
   *best = cand[best_i];
   tuned_store(h->device, user, 0, h->n, *best);
+  rc = layout(h, h->n, dt_keep);  // the tuned grouping (unless the options fix one)
+  if (rc) return rc;
+  // The resident accelerations are those of the configuration the handle now uses (the
+  // grouping sets the FP32 summation order), not of the last candidate timed.
+  enqueue_force(h, b, 0, 0, false);
+  rc = finish(h, false);
+  if (rc) return rc;
   if (tried) std::copy(cand.begin(), cand.end(), tried);
   if (n_tried) *n_tried = static_cast<uint32_t>(cand.size());
   return GX_OK;

@@ -106,6 +106,8 @@ int upload_tables(gx_batch* bt, const std::vector<size_t>& which, bool* inside) 
     d.theta = s.theta;
     d.dt = s.dt;
     d.flags = s.pending ? kSysPendingKick : 0u;
+    // the grouping the system would have alone, so its result equals the alone result
+    d.group = system_walk_group(bt->device, bt->opt, s.n);
     in.push_back(d);
     *inside = *inside || s.theta >= 0.57;
   }
@@ -159,7 +161,7 @@ int bfinish(gx_batch* bt) {
 // the systems already resident.
 int grow(gx_batch* bt, size_t n_total, size_t nsys) {
   const size_t tiles = n_total / kTile + nsys + 1;
-  const size_t items = n_total / 32 + nsys + 1;
+  const size_t items = n_total / 8 + nsys + 1;  // systems' walk items of 8 targets at the narrowest
   Arena& ar = bt->ar;
   const int quad = bt->opt.multipole == GX_MULTIPOLE_QUAD;
   const int f64 = bt->opt.precision == GX_PREC_F64;
@@ -265,8 +267,7 @@ int gx_batch_create(size_t budget_bytes, const gx_options* opt, gx_batch** out) 
     if (opt->struct_size < sizeof(gx_options)) return GX_ERR_INVALID_ARG;
     o = *opt;
   }
-  if (o.precision > GX_PREC_F64 || o.multipole > GX_MULTIPOLE_QUAD ||
-      (o.walk_block && (o.walk_block % 32 || o.walk_block > static_cast<uint32_t>(kWalkThreads)))) {
+  if (!options_valid(o)) {
     set_global_err("invalid gx_options");
     return GX_ERR_INVALID_ARG;
   }
@@ -282,6 +283,7 @@ int gx_batch_create(size_t budget_bytes, const gx_options* opt, gx_batch** out) 
   if (dev < 0) cudaGetDevice(&dev);
   bt->device = dev;
   cudaSetDevice(dev);
+  prepare_device(dev);
   cudaDeviceGetAttribute(&bt->sm_count, cudaDevAttrMultiProcessorCount, dev);
   if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&bt->e0) != cudaSuccess || cudaEventCreate(&bt->e1) != cudaSuccess) {
@@ -416,7 +418,7 @@ int gx_batch_autotune(gx_batch* bt, uint32_t repeats, gx_tuning* best, gx_tuning
   const gx_options user = bt->opt;
   const uint32_t reps = repeats ? repeats : 3;
   // The batch always walks with a persistent kernel (items of uneven systems).
-  std::vector<gx_tuning> cand = tune_candidates(bcfg(bt, inside), false);
+  std::vector<gx_tuning> cand = tune_candidates(bcfg(bt, inside), false, false);
   int best_i = -1;
   for (size_t i = 0; i < cand.size() && rc == GX_OK; ++i) {
     bt->opt.walk_block = cand[i].walk_block;

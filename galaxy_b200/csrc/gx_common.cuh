@@ -104,11 +104,12 @@ struct SysDesc {
   uint32_t first_tile, ntiles;  // its tiles
   double g, eps, theta, dt;
   uint32_t flags;               // kSysPendingKick: the closing half kick is still owed
-  uint32_t pad;
+  uint32_t group;               // targets a warp of the FP32 walk (8, 16 or 32; walk items hold this many)
 };
 constexpr uint32_t kSysPendingKick = 1u;
 
-// 32 consecutive sorted targets of one system, walked by one warp.
+// Consecutive sorted targets of one system (its group: 8, 16 or 32 of them), walked
+// by one warp.
 struct WalkItem {
   uint32_t begin, sys;
 };

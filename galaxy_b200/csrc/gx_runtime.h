@@ -45,6 +45,8 @@ struct Arena {
 void make_tables(const std::vector<SysDesc>& in, std::vector<SysDesc>& sys, std::vector<TileDesc>& tiles,
                  std::vector<WalkItem>& items);
 bool check_device(int device, std::string& err);
+// Once per device, with the device current: kernel attributes the launches rely on.
+void prepare_device(int dev);
 void set_global_err(const std::string& s);
 const char* global_err();
 
@@ -54,6 +56,13 @@ bool tuned_lookup(int device, const gx_options& opt, int batched, size_t n, gx_t
 void tuned_store(int device, const gx_options& opt, int batched, size_t n, const gx_tuning& t);
 // Walk launch candidates: blocks of 64 and 128 threads, each as a grid of one warp per
 // item (ctas 0, when with_grid) and as a persistent kernel at half and full residency.
-std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid);
+// Walk launch candidates: block sizes x schedulings (a grid when with_grid) x groupings
+// (8, 16, 32 targets a warp when with_groups).
+std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid, bool with_groups);
+// Targets a warp of the FP32 walk of one system of n particles: the option, else the
+// single-system tuning table's entry for n, else default_walk_group(n).
+uint32_t system_walk_group(int device, const gx_options& opt, size_t n);
+uint32_t default_walk_group(size_t n);
+bool options_valid(const gx_options& o);
 
 }  // namespace gx

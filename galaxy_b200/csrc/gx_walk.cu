@@ -298,26 +298,110 @@ __device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double th
 }  // namespace
 
 #ifndef GX_WALK_MINB
-#define GX_WALK_MINB 7  // resident kWalkThreads-thread blocks per SM (72 registers a thread)
+#define GX_WALK_MINB 4  // resident kWalkThreads-thread blocks per SM (shared memory bounds it at 4)
 #endif
 
-// FP32 walk over sibling-pair records. Each iteration decides both children of one
-// opened internal node for every lane that opened it: the pair's record is five
-// float4 loads, laid out so that every component pair is a float2 (left, right), and
-// the distance, threshold and force arithmetic of the two children runs as sm_100
-// packed FP32 instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn). Terms of four
-// iterations are summed and added to the lane's Kahan-compensated accumulator. The
-// record carries the children's indices, so the next pair is known from the record
-// just loaded (one dependent load per iteration); the warp's stack of pending pairs
-// lives in shared memory. Indices are clamped into the record array, so even a
-// corrupt tree cannot read out of bounds; a clamp or an exhausted iteration budget
-// raises the device error word. Each lane takes exactly the reference's set of
-// terms; only the order of summation differs from the FP64 walk.
+namespace {
+
+// Margins of the warp-wide (group) opening test. A child is taken for every target of
+// the warp when the squared distance from its centre of mass to the targets' bounding
+// box, times (1 - 2^-20), exceeds the child's take threshold, and opened for every
+// target when the squared distance to the box's farthest corner, times (1 + 2^-20),
+// is below its open threshold. The box is padded by 2^-21 of its coordinates, which
+// covers the float-float split of every target, and the margins cover the FP32
+// rounding of the box distances (a few ulps), so a group decision is the decision
+// the reference's exact test makes for each target: the thresholds already hold the
+// 4e-6 band around rcrit^2.
+constexpr float kGroupLo = 1.0f - 0x1p-20f;
+// Per-warp stack and list sizes of the FP32 walk (see WarpLists).
+constexpr int kWalkStack = 512;  // stack entries
+constexpr int kWalkDeep = 224;   // above this many stacked entries a round takes one entry
+constexpr int kWalkList = 96;    // entries per list: at most 31 left after an evaluation + 64 a round
+constexpr int kWalkFlush = 32;   // a list is evaluated once it holds this many entries
+constexpr float kGroupHi = 1.0f + 0x1p-20f;
+
+// Order-preserving map of a float onto a signed int (for warp min / max reductions).
+__device__ __forceinline__ int ford(float f) {
+  const int i = __float_as_int(f);
+  return i ^ ((i >> 31) & 0x7fffffff);
+}
+__device__ __forceinline__ float fdeord(int i) { return __int_as_float(i ^ ((i >> 31) & 0x7fffffff)); }
+
+// Two list entries share each float4: entry e is half (e & 1) of float4 e >> 1, so a
+// broadcast load of one float4 yields (entry 2p, entry 2p + 1) operand pairs for the
+// packed FP32 instructions.
+__device__ __forceinline__ void put2(float4* a, int e, float v0, float v1) {
+  float* p = reinterpret_cast<float*>(a + (e >> 1)) + (e & 1);
+  p[0] = v0;
+  p[2] = v1;
+}
+
+}  // namespace
+
+// Per-warp shared memory of the FP32 walk.
+//   stk: (internal node, lane mask) -- the node was opened by the lanes in the mask and
+//        its two children are still to be decided for them;
+//   dense list: children every lane of their mask takes (leaves, or nodes the group
+//        test accepted for the whole warp): evaluated with no per-lane decision;
+//   undecided list: children some lanes take and others open (or that need the FP64
+//        re-decision), evaluated with each lane's own decision.
+struct WarpLists {
+  uint2 stk[kWalkStack];
+  float4 da[kWalkList / 2], db[kWalkList / 2], dc[kWalkList / 2], dd[kWalkList / 2];  // (xh,yh) (zh,m) (xl,yl) (zl,mask)
+  float4 ua[kWalkList / 2], ub[kWalkList / 2], uc[kWalkList / 2], ud[kWalkList / 2], ue[kWalkList / 2],
+      uf[kWalkList / 2];  // (xh,yh) (zh,m) (xl,yl) (zl,take) (open,code) (mask,-)
+  uint32_t dcode[kWalkList];  // child code of each dense entry (quadrupole terms, statistics)
+};
+
+// Bound of the stack: a normal round starts at most kWalkDeep entries high and pushes at
+// most one entry per popped one (2 children each, <= 32 popped), an undecided evaluation
+// pushes at most one entry per list entry (< kWalkList), the first deep round at most
+// 2 + 33, and then the depth-first growth adds at most one entry per tree level.
+static_assert(kWalkDeep + 32 + (kWalkList - 1) + 35 + kMaxDepth <= kWalkStack, "walk stack bound");
+
+// Quadrupole mode: each listed internal node's traceless moments (xx, xy, xz, yy), (yz, zz),
+// fetched once by the lane that lists it.
+struct WarpQuads {
+  float4 dqa[kWalkList];
+  float2 dqb[kWalkList];
+  float4 uqa[kWalkList];
+  float2 uqb[kWalkList];
+};
+
+size_t walk_smem_bytes(int block, bool quad) {
+  return static_cast<size_t>(block / 32) * (sizeof(WarpLists) + (quad ? sizeof(WarpQuads) : 0));
+}
+
+// FP32 walk: one warp per 32 Morton-consecutive targets; the warp visits the union of
+// their walks (each node is decided once for every lane that reached it) but not one
+// node at a time. A round pops up to 32 opened nodes from the warp's stack, one per
+// lane, loads each one's sibling-pair record (both children: float-float centre of mass,
+// mass, FP32 take / open thresholds, child codes) and decides each child for the whole
+// warp against the bounding box of the warp's targets:
+//   - taken by every target (or a leaf): appended to the dense list;
+//   - opened by every target: pushed back on the stack with the same lane mask;
+//   - otherwise: appended to the undecided list.
+// A list holding 32 entries is evaluated by all 32 lanes together, two entries per
+// packed-FP32 instruction: the dense list with no decisions, the undecided list with
+// each lane's exact test (FP64 re-decision in the band, the inside test for
+// theta >= 1/sqrt 3), and the lanes that open an undecided child push it with their
+// mask. Rounds, lists and entries are independent of one another, so the walk has no
+// dependent chain of one record per step. While the stack holds more than kWalkDeep
+// entries, a round takes only the top entry (and evaluates its undecided children at
+// once): the stack then grows like a depth-first walk, by at most one entry per tree
+// level, which bounds it within kWalkStack. Every lane takes exactly the reference's set
+// of terms; only the order of summation differs from the FP64 walk. Terms are summed
+// four at a time into a Kahan-compensated accumulator. Node indices are clamped into the
+// record array and the number of records a warp visits is bounded by the system's node
+// count, so even a corrupt tree cannot read out of bounds or loop; a clamp, an exhausted
+// budget or a full stack raises the device error word.
 template <bool QUAD, bool KAHAN, bool STATS, bool INSIDE, bool LIST>
 __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBufs b, int persistent) {
-  __shared__ uint2 s_stack[kWalkThreads / 32][kStackCap];  // (internal node, lane mask)
+  extern __shared__ __align__(16) unsigned char s_walk_raw[];
+  WarpLists& L = reinterpret_cast<WarpLists*>(s_walk_raw)[threadIdx.x >> 5];
+  WarpQuads& Q = reinterpret_cast<WarpQuads*>(s_walk_raw + (blockDim.x >> 5) * sizeof(WarpLists))[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  uint2* stack = s_stack[threadIdx.x >> 5];
+  const uint32_t lt = (1u << lane) - 1u;
   const uint32_t warps_total = (gridDim.x * blockDim.x) >> 5;
   uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_total = b.n;
@@ -326,11 +410,19 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
     const WalkItem it = b.items[item];
     const SysDesc sd = b.sys[it.sys];
     const uint32_t end = sd.off + sd.n;
-    // a target list (active-subset walk) names the item's targets; else they are the
-    // 32 sorted positions from it.begin
-    const uint32_t li = it.begin + lane;
-    const bool valid = LIST ? (lane < static_cast<int>(b.group) && li < *b.ntargets) : li < end;
+    // G targets a warp (the system's group, or the target list's), R = 32 / G lanes a
+    // target: lane = sub * G + target, so the lanes of one sub-lane index hold contiguous
+    // ballot bits. Masks have one bit per target.
+    const uint32_t G = LIST ? b.group : sd.group;
+    const int lg = __ffs(G) - 1;
+    const uint32_t gmask = G == 32 ? 0xffffffffu : (1u << G) - 1u;
+    const int tg = lane & (G - 1), sl = lane >> lg, R = 32 >> lg;
+    // a target list (active-subset walk) names the item's G targets; else they are the
+    // G sorted positions from it.begin
+    const uint32_t li = it.begin + tg;
+    const bool valid = LIST ? li < *b.ntargets : li < end;
     const uint32_t k = LIST ? (valid ? b.targets[li] : 0u) : li;
+    const uint32_t vmask = __ballot_sync(0xffffffffu, valid) & gmask;
     // Kahan state: (x, y) packed, z scalar.
     float2 sxy = f2(0.f, 0.f), cxy = f2(0.f, 0.f);
     float sz = 0.f, cz = 0.f;
@@ -339,9 +431,14 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
     // The root's box is the system's box, so every target is inside it and every lane
     // opens it -- unless the whole system is massless, when nothing is added.
     const uint32_t root = sd.off;  // internal node 0 of the system
-    if (sd.n > 1 && __ldg(&b.agg64[root].m) > 0.0) {
+    if (sd.n > 1 && vmask && __ldg(&b.agg64[root].m) > 0.0) {
       const float eps2f = __double2float_rn(dmul(sd.eps, sd.eps));
       const float2 eps2 = f2(eps2f, eps2f);
+      // The inside rule (a target inside a node's box opens it) can only bind for
+      // theta >= 1/sqrt(3); it follows the system's own theta (as the single-system
+      // handle's choice of kernel does), so a system's terms and their order do not
+      // depend on the other systems of a batch.
+      const bool inside_rule = INSIDE && sd.theta >= 0.57;
       float xh[3] = {0.f, 0.f, 0.f}, xl[3] = {0.f, 0.f, 0.f};
       if (valid) {
         const double4 p = b.leaf64[k];
@@ -349,99 +446,33 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         split_ff(p.y, xh[1], xl[1]);
         split_ff(p.z, xh[2], xl[2]);
       }
-      // negated target coordinates, duplicated for both children
+      // negated target coordinates, duplicated for both entries of a packed pair
       const float2 nxh = f2(-xh[0], -xh[0]), nyh = f2(-xh[1], -xh[1]), nzh = f2(-xh[2], -xh[2]);
       const float2 nxl = f2(-xl[0], -xl[0]), nyl = f2(-xl[1], -xl[1]), nzl = f2(-xl[2], -xl[2]);
+      // The targets' padded bounding box as negated faces (lo, hi), duplicated. A target
+      // that is not finite turns the box into all of space: no group decisions.
+      const bool fin = isfinite(xh[0]) && isfinite(xh[1]) && isfinite(xh[2]);
+      const bool all_fin = __all_sync(0xffffffffu, !valid || fin);
+      float2 nlo[3], nhi[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float l = fdeord(__reduce_min_sync(0xffffffffu, valid ? ford(xh[c]) : 0x7fffffff));
+        float h = fdeord(__reduce_max_sync(0xffffffffu, valid ? ford(xh[c]) : static_cast<int>(0x80000000u)));
+        const float pad = (fabsf(l) + fabsf(h)) * 0x1p-21f + 1e-30f;
+        l = all_fin ? l - pad : -INFINITY;
+        h = all_fin ? h + pad : INFINITY;
+        nlo[c] = f2(-l, -l);
+        nhi[c] = f2(-h, -h);
+      }
       const uint32_t gmax = n_total - 1;
-      int sp = 0;
-      uint32_t g = root;
-      uint32_t mask = __ballot_sync(0xffffffffu, valid);
-      const uint32_t max_iters = sd.n + 64u;
-      uint32_t iters = 0;
-      float2 tx = f2(0.f, 0.f), ty = f2(0.f, 0.f), tz = f2(0.f, 0.f);  // per-child term sums
-      // One pair: decide both children for every active lane, add the taken terms,
-      // move to the next pair. Returns false when the walk is over (or went wrong).
-      auto pair_step = [&]() -> bool {
-        bad |= g > gmax;
-        g = min(g, gmax);
-        if (STATS) ++n_vis;
-        const float4* pr = pairs + 5 * (size_t)g;
-        const float4 r0 = __ldg(pr), r1 = __ldg(pr + 1), r2 = __ldg(pr + 2), r3 = __ldg(pr + 3), r4 = __ldg(pr + 4);
-        // child codes: internal node index, or kLeafCode | leaf index
-        const uint32_t cL = __float_as_uint(r4.z), cR = __float_as_uint(r4.w);
-        const bool act = (mask >> lane) & 1u;
-        // d = (c_hi - x_hi) + (c_lo - x_lo) for both children at once
-        const float2 dx = __fadd2_rn(__fadd2_rn(f2(r0.x, r0.y), nxh), __fadd2_rn(f2(r2.x, r2.y), nxl));
-        const float2 dy = __fadd2_rn(__fadd2_rn(f2(r0.z, r0.w), nyh), __fadd2_rn(f2(r2.z, r2.w), nyl));
-        const float2 dz = __fadd2_rn(__fadd2_rn(f2(r1.x, r1.y), nzh), __fadd2_rn(f2(r3.x, r3.y), nzl));
-        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-        bool tL = act && d2.x > r3.z, tR = act && d2.y > r3.w;
-        bool oL = act && d2.x < r4.x, oR = act && d2.y < r4.y;
-        bool aL = act && !tL && !oL, aR = act && !tR && !oR;
-        if (INSIDE) {
-          if (tL && !(cL & kLeafCode)) inside_test(b, xh, cL, tL, oL, aL);
-          if (tR && !(cR & kLeafCode)) inside_test(b, xh, cR, tR, oR, aR);
-        }
-        if (__any_sync(0xffffffffu, aL || aR)) {
-          if (STATS) n_re += (aL ? 1 : 0) + (aR ? 1 : 0);
-          if (aL) resolve(b, k, sd.theta, cL, tL, oL);
-          if (aR) resolve(b, k, sd.theta, cR, tR, oR);
-        }
-        // Plummer-softened monopole terms; r^2 > 0 keeps the target's own leaf (d = 0)
-        // an exact zero term.
-        const float2 r2s = __fadd2_rn(d2, eps2);
-        const float invL = rsqrtf(fmaxf(r2s.x, 1e-30f)), invR = rsqrtf(fmaxf(r2s.y, 1e-30f));
-        const float2 inv = f2(invL, invR);
-        const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
-        float2 f = __fmul2_rn(f2(r1.z, r1.w), inv3);
-        f.x = tL ? f.x : 0.f;
-        f.y = tR ? f.y : 0.f;
-        tx = __ffma2_rn(dx, f, tx);
-        ty = __ffma2_rn(dy, f, ty);
-        tz = __ffma2_rn(dz, f, tz);
-        if (QUAD) {
-          float tq[3] = {0.f, 0.f, 0.f};
-          if (tL && !(cL & kLeafCode))
-            quad_term(__ldg(&b.nodeQ[2 * (size_t)cL]), __ldg(&b.nodeQ[2 * (size_t)cL + 1]), dx.x, dy.x, dz.x, invL, tq);
-          if (tR && !(cR & kLeafCode))
-            quad_term(__ldg(&b.nodeQ[2 * (size_t)cR]), __ldg(&b.nodeQ[2 * (size_t)cR + 1]), dx.y, dy.y, dz.y, invR, tq);
-          tx.x += tq[0];
-          ty.x += tq[1];
-          tz.x += tq[2];
-        }
-        if (STATS) {
-          const uint32_t self = kLeafCode | k;
-          n_leaf += (tL && (cL & kLeafCode) && cL != self ? 1 : 0) + (tR && (cR & kLeafCode) && cR != self ? 1 : 0);
-          n_far += (tL && !(cL & kLeafCode) ? 1 : 0) + (tR && !(cR & kLeafCode) ? 1 : 0);
-          n_open += (oL ? 1 : 0) + (oR ? 1 : 0);
-        }
-        const uint32_t m0 = __ballot_sync(0xffffffffu, oL);
-        const uint32_t m1 = __ballot_sync(0xffffffffu, oR);
-        if (m0) {
-          if (m1) {
-            // push the right child; continue with the left one
-            if (sp >= kStackCap) {
-              bad = true;
-              return false;
-            }
-            if (lane == 0) stack[sp] = make_uint2(cR, m1);
-            ++sp;
-          }
-          g = cL;
-          mask = m0;
-        } else if (m1) {
-          g = cR;
-          mask = m1;
-        } else {
-          if (sp == 0) return false;
-          __syncwarp();
-          const uint2 e = stack[--sp];
-          g = e.x;
-          mask = e.y;
-        }
-        return true;
-      };
-      // fold the children's sums of the last four pairs and add them with compensation
+      const uint32_t max_pairs = sd.n + 64u;
+      uint32_t pairs_done = 0;
+      int sp = 1, dl = 0, ul = 0, pend = 0;
+      if (lane == 0) L.stk[0] = make_uint2(root, vmask);
+      __syncwarp();
+      float2 tx = f2(0.f, 0.f), ty = f2(0.f, 0.f), tz = f2(0.f, 0.f);  // per-entry term sums
+      // list entries a lane evaluates: pairs p = q R + sl of the list, q = 0, 1, ...
+      // add the term sums of the last entries to the lane's compensated accumulator
       auto fold = [&]() {
         const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
         const float tzz = tz.x + tz.y;
@@ -459,41 +490,295 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
           sz += tzz;
         }
         tx = ty = tz = f2(0.f, 0.f);
+        pend = 0;
+      };
+      auto put_dense = [&](int e, float xh_, float yh_, float zh_, float m_, float xl_, float yl_, float zl_,
+                           uint32_t mask, uint32_t code) {
+        put2(L.da, e, xh_, yh_);
+        put2(L.db, e, zh_, m_);
+        put2(L.dc, e, xl_, yl_);
+        put2(L.dd, e, zl_, __uint_as_float(mask));
+        L.dcode[e] = code;
+      };
+      auto put_und = [&](int e, float xh_, float yh_, float zh_, float m_, float xl_, float yl_, float zl_,
+                         float take, float open, uint32_t code, uint32_t mask) {
+        put2(L.ua, e, xh_, yh_);
+        put2(L.ub, e, zh_, m_);
+        put2(L.uc, e, xl_, yl_);
+        put2(L.ud, e, zl_, take);
+        put2(L.ue, e, open, __uint_as_float(code));
+        put2(L.uf, e, __uint_as_float(mask), 0.f);
+      };
+      // One round: the top kk stack entries, one per lane, each child decided for the
+      // whole warp and appended to a list or pushed back.
+      auto round = [&](int kk) {
+        const bool act = lane < kk;
+        uint32_t g = 0, M = 0;
+        if (act) {
+          const uint2 e = L.stk[sp - kk + lane];
+          g = e.x;
+          M = e.y;
+        }
+        sp -= kk;
+        __syncwarp();  // popped before the pushes below overwrite the slots
+        bad |= act && g > gmax;
+        g = min(g, gmax);
+        float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0, r2 = r0, r3 = r0, r4 = r0;
+        if (act) {
+          const float4* pr = pairs + 5 * (size_t)g;
+          r0 = __ldg(pr);
+          r1 = __ldg(pr + 1);
+          r2 = __ldg(pr + 2);
+          r3 = __ldg(pr + 3);
+          r4 = __ldg(pr + 4);
+        }
+        const uint32_t cL = __float_as_uint(r4.z), cR = __float_as_uint(r4.w);
+        const float2 chx = f2(r0.x, r0.y), chy = f2(r0.z, r0.w), chz = f2(r1.x, r1.y);
+        const float2 clx = f2(r2.x, r2.y), cly = f2(r2.z, r2.w), clz = f2(r3.x, r3.y);
+        // c - lo and c - hi per axis, both children at once
+        const float2 lx = __fadd2_rn(__fadd2_rn(chx, nlo[0]), clx), hx = __fadd2_rn(__fadd2_rn(chx, nhi[0]), clx);
+        const float2 ly = __fadd2_rn(__fadd2_rn(chy, nlo[1]), cly), hy = __fadd2_rn(__fadd2_rn(chy, nhi[1]), cly);
+        const float2 lz = __fadd2_rn(__fadd2_rn(chz, nlo[2]), clz), hz = __fadd2_rn(__fadd2_rn(chz, nhi[2]), clz);
+        // distance to the box (0 inside) and to its farthest corner, per axis
+        const float2 nx = f2(fmaxf(fmaxf(-lx.x, hx.x), 0.f), fmaxf(fmaxf(-lx.y, hx.y), 0.f));
+        const float2 ny = f2(fmaxf(fmaxf(-ly.x, hy.x), 0.f), fmaxf(fmaxf(-ly.y, hy.y), 0.f));
+        const float2 nz = f2(fmaxf(fmaxf(-lz.x, hz.x), 0.f), fmaxf(fmaxf(-lz.y, hz.y), 0.f));
+        const float2 fx = f2(fmaxf(lx.x, -hx.x), fmaxf(lx.y, -hx.y));
+        const float2 fy = f2(fmaxf(ly.x, -hy.x), fmaxf(ly.y, -hy.y));
+        const float2 fz = f2(fmaxf(lz.x, -hz.x), fmaxf(lz.y, -hz.y));
+        const float2 dmin2 = __ffma2_rn(nx, nx, __ffma2_rn(ny, ny, __fmul2_rn(nz, nz)));
+        const float2 dmax2 = __ffma2_rn(fx, fx, __ffma2_rn(fy, fy, __fmul2_rn(fz, fz)));
+        bool accL = act && dmin2.x * kGroupLo > r3.z, accR = act && dmin2.y * kGroupLo > r3.w;
+        if (inside_rule) {
+          // the group test does not cover the inside rule: nodes go to the lanes' tests
+          accL = accL && (cL & kLeafCode);
+          accR = accR && (cR & kLeafCode);
+        }
+        const bool opnL = act && !accL && dmax2.x * kGroupHi < r4.x;
+        const bool opnR = act && !accR && dmax2.y * kGroupHi < r4.y;
+        const bool undL = act && !accL && !opnL, undR = act && !accR && !opnR;
+        const uint32_t bAL = __ballot_sync(0xffffffffu, accL), bAR = __ballot_sync(0xffffffffu, accR);
+        const uint32_t bUL = __ballot_sync(0xffffffffu, undL), bUR = __ballot_sync(0xffffffffu, undR);
+        const uint32_t bOL = __ballot_sync(0xffffffffu, opnL), bOR = __ballot_sync(0xffffffffu, opnR);
+        const int eAL = dl + __popc(bAL & lt), eAR = dl + __popc(bAL) + __popc(bAR & lt);
+        const int eUL = ul + __popc(bUL & lt), eUR = ul + __popc(bUL) + __popc(bUR & lt);
+        if (QUAD) {
+          // the moments of the listed internal children, loaded side by side
+          const bool qL = (accL || undL) && !(cL & kLeafCode), qR = (accR || undR) && !(cR & kLeafCode);
+          float4 qaL = make_float4(0.f, 0.f, 0.f, 0.f), qbL = qaL, qaR = qaL, qbR = qaL;
+          if (qL) {
+            qaL = __ldg(&b.nodeQ[2 * (size_t)cL]);
+            qbL = __ldg(&b.nodeQ[2 * (size_t)cL + 1]);
+          }
+          if (qR) {
+            qaR = __ldg(&b.nodeQ[2 * (size_t)cR]);
+            qbR = __ldg(&b.nodeQ[2 * (size_t)cR + 1]);
+          }
+          if (qL && accL) {
+            Q.dqa[eAL] = qaL;
+            Q.dqb[eAL] = make_float2(qbL.x, qbL.y);
+          }
+          if (qL && undL) {
+            Q.uqa[eUL] = qaL;
+            Q.uqb[eUL] = make_float2(qbL.x, qbL.y);
+          }
+          if (qR && accR) {
+            Q.dqa[eAR] = qaR;
+            Q.dqb[eAR] = make_float2(qbR.x, qbR.y);
+          }
+          if (qR && undR) {
+            Q.uqa[eUR] = qaR;
+            Q.uqb[eUR] = make_float2(qbR.x, qbR.y);
+          }
+        }
+        if (accL) put_dense(eAL, chx.x, chy.x, chz.x, r1.z, clx.x, cly.x, clz.x, M, cL);
+        if (accR) put_dense(eAR, chx.y, chy.y, chz.y, r1.w, clx.y, cly.y, clz.y, M, cR);
+        dl += __popc(bAL) + __popc(bAR);
+        if (undL) put_und(eUL, chx.x, chy.x, chz.x, r1.z, clx.x, cly.x, clz.x, r3.z, r4.x, cL, M);
+        if (undR) put_und(eUR, chx.y, chy.y, chz.y, r1.w, clx.y, cly.y, clz.y, r3.w, r4.y, cR, M);
+        ul += __popc(bUL) + __popc(bUR);
+        const int npush = __popc(bOL) + __popc(bOR);
+        if (sp + npush > kWalkStack) {
+          bad = true;
+        } else {
+          if (opnL) L.stk[sp + __popc(bOL & lt)] = make_uint2(cL, M);
+          if (opnR) L.stk[sp + __popc(bOL) + __popc(bOR & lt)] = make_uint2(cR, M);
+          sp += npush;
+        }
+        if (STATS) {
+          n_vis += kk;
+          n_open += (opnL ? __popc(M) : 0) + (opnR ? __popc(M) : 0);
+        }
+        __syncwarp();
+      };
+      // Evaluate the dense list: every lane adds the terms of the entries in its mask.
+      auto flush_dense = [&]() {
+        if (dl & 1) {
+          if (lane == 0) put_dense(dl, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0u, kLeafCode);
+          __syncwarp();
+        }
+        const int np = (dl + 1) >> 1;
+        for (int q = 0; q * R < np; ++q) {
+          // lanes past the list's end read its last pair with no target bit
+          const int p0 = q * R + sl, p = min(p0, np - 1), e = 2 * p;
+          const uint32_t on = p0 < np ? 1u : 0u;
+          const float4 A = L.da[p], B = L.db[p], C = L.dc[p], D = L.dd[p];
+          const float2 dx = __fadd2_rn(__fadd2_rn(f2(A.x, A.y), nxh), __fadd2_rn(f2(C.x, C.y), nxl));
+          const float2 dy = __fadd2_rn(__fadd2_rn(f2(A.z, A.w), nyh), __fadd2_rn(f2(C.z, C.w), nyl));
+          const float2 dz = __fadd2_rn(__fadd2_rn(f2(B.x, B.y), nzh), __fadd2_rn(f2(D.x, D.y), nzl));
+          const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+          // Plummer-softened monopole terms; the target's own leaf (d = 0) is an exact zero
+          const float2 r2s = __fadd2_rn(d2, eps2);
+          const float i0 = rsqrtf(fmaxf(r2s.x, 1e-30f)), i1 = rsqrtf(fmaxf(r2s.y, 1e-30f));
+          const float2 inv = f2(i0, i1);
+          const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
+          float2 f = __fmul2_rn(f2(B.z, B.w), inv3);
+          const bool t0 = (__float_as_uint(D.z) >> tg) & on, t1 = (__float_as_uint(D.w) >> tg) & on;
+          f.x = t0 ? f.x : 0.f;
+          f.y = t1 ? f.y : 0.f;
+          tx = __ffma2_rn(dx, f, tx);
+          ty = __ffma2_rn(dy, f, ty);
+          tz = __ffma2_rn(dz, f, tz);
+          if (QUAD || STATS) {
+            const uint32_t c0 = L.dcode[e], c1 = L.dcode[e + 1];
+            if (QUAD) {
+              float tq[3] = {0.f, 0.f, 0.f};
+              if (t0 && !(c0 & kLeafCode)) {
+                const float2 qb = Q.dqb[e];
+                quad_term(Q.dqa[e], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
+              }
+              if (t1 && !(c1 & kLeafCode)) {
+                const float2 qb = Q.dqb[e + 1];
+                quad_term(Q.dqa[e + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
+              }
+              tx.x += tq[0];
+              ty.x += tq[1];
+              tz.x += tq[2];
+            }
+            if (STATS) {
+              const uint32_t self = kLeafCode | k;
+              n_leaf += (t0 && (c0 & kLeafCode) && c0 != self ? 1 : 0) + (t1 && (c1 & kLeafCode) && c1 != self ? 1 : 0);
+              n_far += (t0 && !(c0 & kLeafCode) ? 1 : 0) + (t1 && !(c1 & kLeafCode) ? 1 : 0);
+            }
+          }
+          pend += 2;
+          if (pend >= 4) fold();
+        }
+        dl = 0;
+        __syncwarp();  // read before the next round overwrites the list
+      };
+      // Evaluate the undecided list: each lane decides each entry of its mask; the lanes
+      // that open an entry push it with their mask.
+      auto flush_und = [&]() {
+        if (ul & 1) {
+          if (lane == 0) put_und(ul, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, kLeafCode, 0u);
+          __syncwarp();
+        }
+        const int np = (ul + 1) >> 1;
+        for (int q = 0; q * R < np; ++q) {
+          const int p0 = q * R + sl, p = min(p0, np - 1);
+          const uint32_t on = p0 < np ? 1u : 0u;
+          const float4 A = L.ua[p], B = L.ub[p], C = L.uc[p], D = L.ud[p], E = L.ue[p], F = L.uf[p];
+          const float2 dx = __fadd2_rn(__fadd2_rn(f2(A.x, A.y), nxh), __fadd2_rn(f2(C.x, C.y), nxl));
+          const float2 dy = __fadd2_rn(__fadd2_rn(f2(A.z, A.w), nyh), __fadd2_rn(f2(C.z, C.w), nyl));
+          const float2 dz = __fadd2_rn(__fadd2_rn(f2(B.x, B.y), nzh), __fadd2_rn(f2(D.x, D.y), nzl));
+          const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+          const uint32_t cL = __float_as_uint(E.z), cR = __float_as_uint(E.w);
+          const bool a0 = (__float_as_uint(F.x) >> tg) & on, a1 = (__float_as_uint(F.y) >> tg) & on;
+          bool tL = a0 && d2.x > D.z, tR = a1 && d2.y > D.w;
+          bool oL = a0 && d2.x < E.x, oR = a1 && d2.y < E.y;
+          bool aL = a0 && !tL && !oL, aR = a1 && !tR && !oR;
+          if (inside_rule) {
+            if (tL && !(cL & kLeafCode)) inside_test(b, xh, cL, tL, oL, aL);
+            if (tR && !(cR & kLeafCode)) inside_test(b, xh, cR, tR, oR, aR);
+          }
+          if (__any_sync(0xffffffffu, aL || aR)) {
+            if (STATS) n_re += (aL ? 1 : 0) + (aR ? 1 : 0);
+            if (aL) resolve(b, k, sd.theta, cL, tL, oL);
+            if (aR) resolve(b, k, sd.theta, cR, tR, oR);
+          }
+          const float2 r2s = __fadd2_rn(d2, eps2);
+          const float i0 = rsqrtf(fmaxf(r2s.x, 1e-30f)), i1 = rsqrtf(fmaxf(r2s.y, 1e-30f));
+          const float2 inv = f2(i0, i1);
+          const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
+          float2 f = __fmul2_rn(f2(B.z, B.w), inv3);
+          f.x = tL ? f.x : 0.f;
+          f.y = tR ? f.y : 0.f;
+          tx = __ffma2_rn(dx, f, tx);
+          ty = __ffma2_rn(dy, f, ty);
+          tz = __ffma2_rn(dz, f, tz);
+          if (QUAD) {
+            float tq[3] = {0.f, 0.f, 0.f};
+            if (tL && !(cL & kLeafCode)) {
+              const float2 qb = Q.uqb[2 * p];
+              quad_term(Q.uqa[2 * p], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
+            }
+            if (tR && !(cR & kLeafCode)) {
+              const float2 qb = Q.uqb[2 * p + 1];
+              quad_term(Q.uqa[2 * p + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
+            }
+            tx.x += tq[0];
+            ty.x += tq[1];
+            tz.x += tq[2];
+          }
+          if (STATS) {
+            const uint32_t self = kLeafCode | k;
+            n_leaf += (tL && (cL & kLeafCode) && cL != self ? 1 : 0) + (tR && (cR & kLeafCode) && cR != self ? 1 : 0);
+            n_far += (tL && !(cL & kLeafCode) ? 1 : 0) + (tR && !(cR & kLeafCode) ? 1 : 0);
+            n_open += (oL ? 1 : 0) + (oR ? 1 : 0);
+          }
+          // the targets that open this lane's entries; lane sl * G pushes them
+          const uint32_t m0 = (__ballot_sync(0xffffffffu, oL) >> (sl * G)) & gmask;
+          const uint32_t m1 = (__ballot_sync(0xffffffffu, oR) >> (sl * G)) & gmask;
+          const uint32_t b0 = __ballot_sync(0xffffffffu, tg == 0 && m0), b1 = __ballot_sync(0xffffffffu, tg == 0 && m1);
+          const int npush = __popc(b0) + __popc(b1);
+          if (sp + npush > kWalkStack) {
+            bad = true;
+          } else {
+            if (tg == 0 && m0) L.stk[sp + __popc(b0 & lt)] = make_uint2(cL, m0);
+            if (tg == 0 && m1) L.stk[sp + __popc(b0) + __popc(b1 & lt)] = make_uint2(cR, m1);
+            sp += npush;
+          }
+          pend += 2;
+          if (pend >= 4) fold();
+        }
+        ul = 0;
+        __syncwarp();  // pushes visible to the next round; list read before it is refilled
       };
       for (;;) {
-        // the iteration budget is checked once per four pairs
-        iters += 4;
-        if (iters > max_iters) {
+        if (__any_sync(0xffffffffu, bad)) break;
+        if (sp == 0) {
+          if (ul == 0) break;
+          flush_und();
+          continue;
+        }
+        const bool deep = sp > kWalkDeep;
+        const int kk = deep ? 1 : min(32, sp);
+        pairs_done += kk;
+        if (pairs_done > max_pairs) {
           bad = true;
           break;
         }
-        if (!pair_step() || !pair_step() || !pair_step() || !pair_step()) break;
-        fold();
+        round(kk);
+        if (dl >= kWalkFlush) flush_dense();
+        if (ul >= kWalkFlush || (deep && ul > 0)) flush_und();
       }
-      // fold what is left
-      const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
-      const float tzz = tz.x + tz.y;
-      if (KAHAN) {
-        const float2 y = __fadd2_rn(txy, f2(-cxy.x, -cxy.y));
-        const float2 u = __fadd2_rn(sxy, y);
-        cxy = __fadd2_rn(__fadd2_rn(u, f2(-sxy.x, -sxy.y)), f2(-y.x, -y.y));
-        sxy = u;
-        const float yz = tzz - cz;
-        const float uz = sz + yz;
-        cz = (uz - sz) - yz;
-        sz = uz;
-      } else {
-        sxy = __fadd2_rn(sxy, txy);
-        sz += tzz;
-      }
-      __syncwarp();  // the next item's pushes must not race this item's last pop
+      if (dl > 0 && !__any_sync(0xffffffffu, bad)) flush_dense();
+      fold();
+      __syncwarp();  // the next item's stack writes must not race this item's last reads
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) raise_err(b.ctl, kErrBadIndex);
-    if (valid) {
+    float ax = KAHAN ? __fsub_rn(sxy.x, cxy.x) : sxy.x;
+    float ay = KAHAN ? __fsub_rn(sxy.y, cxy.y) : sxy.y;
+    float az = KAHAN ? __fsub_rn(sz, cz) : sz;
+    // the R lanes of a target hold partial sums over disjoint entries
+    for (int o = G; o < 32; o <<= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+      az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    if (valid && sl == 0) {
       const uint32_t o = b.order[k];
-      const float ax = KAHAN ? __fsub_rn(sxy.x, cxy.x) : sxy.x;
-      const float ay = KAHAN ? __fsub_rn(sxy.y, cxy.y) : sxy.y;
-      const float az = KAHAN ? __fsub_rn(sz, cz) : sz;
       b.acc[3 * (size_t)o + 0] = dmul(static_cast<double>(ax), sd.g);
       b.acc[3 * (size_t)o + 1] = dmul(static_cast<double>(ay), sd.g);
       b.acc[3 * (size_t)o + 2] = dmul(static_cast<double>(az), sd.g);
@@ -503,7 +788,7 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
       n_far = warp_sum64(n_far);
       n_open = warp_sum64(n_open);
       n_re = warp_sum64(n_re);
-      const uint32_t n_valid = __popc(__ballot_sync(0xffffffffu, valid));  // the root, opened by all
+      const uint32_t n_valid = __popc(vmask);  // the root, opened by all
       if (lane == 0) {
         atomicAdd(&b.ctl->stats[0], n_leaf);
         atomicAdd(&b.ctl->stats[1], n_far);
@@ -525,29 +810,30 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
 namespace {
 
 template <class K>
-void launch_k(K kern, const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
-  const int block = cfg.block > 0 ? cfg.block : 256;
+void launch_k(K kern, const StepBufs& b, const WalkCfg& cfg, size_t smem, cudaStream_t st) {
+  const int block = cfg.block > 0 ? cfg.block : kWalkThreads;
   const int wpb = block / 32;
   if (cfg.persistent_ctas > 0) {
-    kern<<<cfg.persistent_ctas, block, 0, st>>>(b, 1);
+    kern<<<cfg.persistent_ctas, block, smem, st>>>(b, 1);
   } else {
     const uint32_t grid = (b.nitems + wpb - 1) / wpb;
-    if (grid) kern<<<grid, block, 0, st>>>(b, 0);
+    if (grid) kern<<<grid, block, smem, st>>>(b, 0);
   }
 }
 
 template <bool QUAD, bool KAHAN, bool LIST>
 void dispatch_f32(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
+  const size_t smem = walk_smem_bytes(cfg.block > 0 ? cfg.block : kWalkThreads, QUAD);
   if (cfg.stats) {
     if (cfg.inside_test)
-      launch_k(k_walk_f32<QUAD, KAHAN, true, true, LIST>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, true, true, LIST>, b, cfg, smem, st);
     else
-      launch_k(k_walk_f32<QUAD, KAHAN, true, false, LIST>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, true, false, LIST>, b, cfg, smem, st);
   } else {
     if (cfg.inside_test)
-      launch_k(k_walk_f32<QUAD, KAHAN, false, true, LIST>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, false, true, LIST>, b, cfg, smem, st);
     else
-      launch_k(k_walk_f32<QUAD, KAHAN, false, false, LIST>, b, cfg, st);
+      launch_k(k_walk_f32<QUAD, KAHAN, false, false, LIST>, b, cfg, smem, st);
   }
 }
 
@@ -557,9 +843,9 @@ void dispatch(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
     // The FP64 walk has no quadrupole or compensation variants: it is the
     // reference's arithmetic.
     if (cfg.stats)
-      launch_k(k_walk_f64<true, LIST>, b, cfg, st);
+      launch_k(k_walk_f64<true, LIST>, b, cfg, 0, st);
     else
-      launch_k(k_walk_f64<false, LIST>, b, cfg, st);
+      launch_k(k_walk_f64<false, LIST>, b, cfg, 0, st);
   } else if (cfg.quad) {
     if (cfg.kahan)
       dispatch_f32<true, true, LIST>(b, cfg, st);
@@ -573,24 +859,49 @@ void dispatch(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {
   }
 }
 
-}  // namespace
-
-namespace {
-
 template <class K>
-int resident(K kern, int block) {
+int resident(K kern, int block, size_t smem) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, block, 0) != cudaSuccess) n = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, block, smem) != cudaSuccess) n = 1;
   return n > 0 ? n : 1;
+}
+
+// The FP32 walk's blocks take (block / 32) x (sizeof(WarpLists) [+ sizeof(WarpQuads)]) of
+// shared memory: ask for the largest shared-memory carveout, and let quadrupole blocks
+// go past the default 48 KB.
+template <class K>
+void smem_attrs(K kern, bool quad) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(walk_smem_bytes(kWalkThreads, quad)));
+}
+
+template <bool QUAD, bool KAHAN, bool LIST>
+void carveout_f32() {
+  smem_attrs(k_walk_f32<QUAD, KAHAN, false, false, LIST>, QUAD);
+  smem_attrs(k_walk_f32<QUAD, KAHAN, false, true, LIST>, QUAD);
+  smem_attrs(k_walk_f32<QUAD, KAHAN, true, false, LIST>, QUAD);
+  smem_attrs(k_walk_f32<QUAD, KAHAN, true, true, LIST>, QUAD);
 }
 
 }  // namespace
 
+void walk_prepare() {
+  carveout_f32<false, false, false>();
+  carveout_f32<false, true, false>();
+  carveout_f32<true, false, false>();
+  carveout_f32<true, true, false>();
+  carveout_f32<false, false, true>();
+  carveout_f32<false, true, true>();
+  carveout_f32<true, false, true>();
+  carveout_f32<true, true, true>();
+}
+
 int walk_resident_ctas(const WalkCfg& cfg) {
   const int block = cfg.block > 0 ? cfg.block : kWalkThreads;
-  if (cfg.precision == 1) return resident(k_walk_f64<false, false>, block);
-  if (cfg.quad) return resident(k_walk_f32<true, true, false, false, false>, block);
-  return resident(k_walk_f32<false, true, false, false, false>, block);
+  if (cfg.precision == 1) return resident(k_walk_f64<false, false>, block, 0);
+  if (cfg.quad) return resident(k_walk_f32<true, true, false, false, false>, block, walk_smem_bytes(block, true));
+  return resident(k_walk_f32<false, true, false, false, false>, block, walk_smem_bytes(block, false));
 }
 
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st) {

@@ -24,6 +24,7 @@ pub struct GxOptions {
     pub device: i32,
     pub walk_block: u32,
     pub walk_ctas_per_sm: u32,
+    pub walk_group: u32,
 }
 
 #[repr(C)]

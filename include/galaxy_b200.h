@@ -62,7 +62,11 @@ typedef struct gx_options {
   uint32_t walk_block;     /* threads per block of the tree walk: 0 = default (128), else a
                               multiple of 32 up to 128 */
   uint32_t walk_ctas_per_sm; /* >0: persistent work-stealing walk with this many CTAs per SM;
-                                0: tuned default (one warp per 32 targets for a single system) */
+                                0: tuned default (one warp per item for a single system) */
+  uint32_t walk_group;     /* targets per warp of the FP32 walk: 8, 16 or 32; 0 = the tuning
+                              table's entry for the system's N, else a rule of N. It changes
+                              the order in which the walk sums its terms (never which terms),
+                              so FP32 results can differ in their last bits between groups */
 } gx_options;
 
 typedef struct gx_handle gx_handle;
@@ -265,21 +269,24 @@ int gx_sph_cfl(gx_handle* h, size_t n, const double* pos, const double* vel, con
                double c_cfl, double* dt_out, double* min_out);
 
 /* ---- autotuning of the walk launch (no counterpart in the reference) -------------
- * The walk's block size and its scheduling (one warp per 32 targets over a grid, or a
- * persistent kernel with CTAs per SM stealing items) are picked per N bucket
- * (floor(log2 N)) by timing candidates on a resident state: force evaluations only,
- * so the state, its trajectory and every result stay bit-identical. The winner is
- * recorded in a process-wide table keyed by (device, precision, multipole, Morton key
- * width, single system or batch, N bucket); handles and batches created with
- * walk_block == 0 and walk_ctas_per_sm == 0 use the table's entry for their N. The
- * radix sort keeps fixed 8-bit digits (4 passes, 8 with 63-bit keys): it is about 1%
- * of a step at N = 2^20, so its digit width is not a tuning knob. */
+ * The walk's block size, its scheduling (one warp per item over a grid, or a persistent
+ * kernel with CTAs per SM stealing items) and, for a single system, its warp grouping
+ * (targets per warp) are picked per N bucket (floor(log2 N)) by timing candidates on a
+ * resident state: force evaluations only, so the resident state is untouched. Block size
+ * and scheduling never change a result; the grouping changes the FP32 walk's summation
+ * order only. The winner is recorded in a process-wide table keyed by (device, precision,
+ * multipole, Morton key width, single system or batch, N bucket); handles and batches
+ * created with walk_block == 0 and walk_ctas_per_sm == 0 use the table's entry for
+ * their N, and every system (alone or in a batch) created with walk_group == 0 takes the
+ * single-system entry's grouping for its own N, so a system's result in a batch equals
+ * its result alone. */
 typedef struct gx_tuning {
   uint32_t walk_block;       /* threads per block of the walk */
   uint32_t walk_ctas_per_sm; /* 0 = grid of one warp per item; > 0 persistent CTAs per SM */
+  uint32_t walk_group;       /* targets per warp (single-system entries; 0 in batch entries) */
   float ms;                  /* median device time of one force evaluation with it */
 } gx_tuning;
-#define GX_TUNE_MAX_CANDIDATES 8
+#define GX_TUNE_MAX_CANDIDATES 24
 /* Time every candidate `repeats` times (median) on the handle's resident state; best
  * (and, if non-NULL, tried[GX_TUNE_MAX_CANDIDATES] with *n_tried) receive the results. */
 int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* tried, uint32_t* n_tried);

@@ -1,21 +1,40 @@
 """Autotuning of the walk launch (gx_autotune / gx_batch_autotune): the sweep leaves
-the state bit-identical, records its winner for the N bucket, and the launch
-configuration never changes a result."""
+the state bit-identical, records its winner for the N bucket, block size and scheduling
+never change a result, and the warp grouping changes only the FP32 summation order."""
 
 import numpy as np
 import pytest
 
 import galaxy_b200 as gb
+from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
 
 def test_launch_configuration_never_changes_results():
     st = gb.ic.collision(65_536, 11)
-    ref = gb.GpuLbvh(1.0, 0.02, 0.5, walk_block=128).accelerations(st)
-    for block, ctas in ((64, 0), (128, 7), (64, 3), (96, 1)):
-        got = gb.GpuLbvh(1.0, 0.02, 0.5, walk_block=block, walk_ctas_per_sm=ctas).accelerations(st)
-        assert np.array_equal(got, ref), (block, ctas)
+    for group in (8, 16, 32):
+        ref = gb.GpuLbvh(1.0, 0.02, 0.5, walk_block=128, walk_group=group).accelerations(st)
+        for block, ctas in ((64, 0), (128, 4), (64, 3), (96, 1)):
+            got = gb.GpuLbvh(1.0, 0.02, 0.5, walk_block=block, walk_ctas_per_sm=ctas,
+                             walk_group=group).accelerations(st)
+            assert np.array_equal(got, ref), (group, block, ctas)
+
+
+def test_walk_groups_take_the_same_terms():
+    """8, 16 or 32 targets a warp: the same interaction counts (every lane's exact
+    decisions) and accelerations within the FP32 parity bounds of the reference walk."""
+    st = gb.ic.plummer(20_000, 5)
+    ref = oracle.lbvh_accelerations(st.pos, st.mass, 1.0, 0.01, 0.5, threads=oracle.max_threads())
+    counts = set()
+    for group in (8, 16, 32):
+        h = gb.GpuLbvh(1.0, 0.01, 0.5, walk_group=group, stats=True)
+        a = h.accelerations(st)
+        s = h.stats()
+        counts.add((s["leaf_interactions"], s["far_interactions"], s["nodes_opened"]))
+        err = oracle.per_particle_rel_err(a, ref)
+        assert np.median(err) <= 1e-6 and np.percentile(err, 99) <= 1e-5, group
+    assert len(counts) == 1
 
 
 def test_autotune_keeps_state_and_records_bucket():
@@ -27,22 +46,29 @@ def test_autotune_keeps_state_and_records_bucket():
     acc_before = r.accelerations()
     best = r.autotune(repeats=2)
     assert best["tried"] and best["ms"] == min(t["ms"] for t in best["tried"])
-    assert best["walk_block"] in (64, 128)
+    assert best["walk_block"] in (64, 128) and best["walk_group"] in (8, 16, 32)
+    assert {t["walk_group"] for t in best["tried"]} == {8, 16, 32}
     after = r.snapshot()
     assert np.array_equal(before.pos, after.pos) and np.array_equal(before.vel, after.vel)
-    assert np.array_equal(acc_before, r.accelerations())
+    # the handle now walks with the tuned grouping: a handle given it explicitly agrees
+    acc_after = r.accelerations()
+    fixed = gb.GpuLbvh(1.0, 0.02, 0.5, walk_group=best["walk_group"]).accelerations(after)
+    assert np.array_equal(acc_after, fixed)
+    err = oracle.per_particle_rel_err(acc_after, acc_before)
+    assert np.percentile(err, 99) <= 1e-5
+    key = ("walk_block", "walk_ctas_per_sm", "walk_group")
     for n in (65_536, 100_000, 131_071):
         rec = gb.tuning_lookup(n)
-        assert rec is not None and (rec["walk_block"], rec["walk_ctas_per_sm"]) == (best["walk_block"],
-                                                                                 best["walk_ctas_per_sm"])
+        assert rec is not None and tuple(rec[k] for k in key) == tuple(best[k] for k in key)
     assert gb.tuning_lookup(98_304, precision="f64") is None
-    # the trajectory continues exactly as an untuned twin's
-    twin = gb.GpuResidentLeapfrog(1.0, 0.02, 0.5, walk_block=128)
-    twin.upload(st)
-    twin.step_many(5e-4, 3)
-    r.step_many(5e-4, 4)
-    twin.step_many(5e-4, 4)
-    assert np.array_equal(r.snapshot().pos, twin.snapshot().pos)
+    # new handles of this bucket take the table's entry: one with the tuned options given
+    # explicitly follows the same trajectory
+    twin = gb.GpuResidentLeapfrog(1.0, 0.02, 0.5)
+    explicit = gb.GpuResidentLeapfrog(1.0, 0.02, 0.5, **{k: best[k] for k in key})
+    for h in (twin, explicit):
+        h.upload(st)
+        h.step_many(5e-4, 4)
+    assert np.array_equal(twin.snapshot().pos, explicit.snapshot().pos)
 
 
 def test_batch_autotune_keeps_state():
