@@ -339,18 +339,22 @@ __device__ __forceinline__ void put2(float4* a, int e, float v0, float v1) {
 }  // namespace
 
 // Per-warp shared memory of the FP32 walk.
-//   stk: (internal node, lane mask) -- the node was opened by the lanes in the mask and
-//        its two children are still to be decided for them;
-//   dense list: children every lane of their mask takes (leaves, or nodes the group
-//        test accepted for the whole warp): evaluated with no per-lane decision;
-//   undecided list: children some lanes take and others open (or that need the FP64
-//        re-decision), evaluated with each lane's own decision.
+//   stk: (internal node, target mask) -- the node was opened for the targets in the mask
+//        and its two children are still to be decided for them;
+//   dense list: children every target of their mask takes (leaves, or nodes the group
+//        test accepted for the whole warp): evaluated with no per-target decision, in
+//        FP32 coordinates relative to the centre of the warp's target box;
+//   undecided list: children some targets take and others open (or that need the FP64
+//        re-decision), evaluated with each target's own decision on float-float
+//        coordinates; afterwards each entry holds the mask of the targets that opened it.
+// Two entries share each float4: entry e is half (e & 1) of float4 e >> 1.
 struct WarpLists {
   uint2 stk[kWalkStack];
-  float4 da[kWalkList / 2], db[kWalkList / 2], dc[kWalkList / 2], dd[kWalkList / 2];  // (xh,yh) (zh,m) (xl,yl) (zl,mask)
+  float4 da[kWalkList / 2], db[kWalkList / 2];  // (x, y) (z, m) relative to the box centre
+  uint2 dm[kWalkList / 2];                      // target masks
+  uint32_t dcode[kWalkList];                    // child codes (quadrupole terms, statistics)
   float4 ua[kWalkList / 2], ub[kWalkList / 2], uc[kWalkList / 2], ud[kWalkList / 2], ue[kWalkList / 2],
-      uf[kWalkList / 2];  // (xh,yh) (zh,m) (xl,yl) (zl,take) (open,code) (mask,-)
-  uint32_t dcode[kWalkList];  // child code of each dense entry (quadrupole terms, statistics)
+      uf[kWalkList / 2];  // (xh,yh) (zh,m) (xl,yl) (zl,take) (open,code) (mask,opened)
 };
 
 // Bound of the stack: a normal round starts at most kWalkDeep entries high and pushes at
@@ -372,25 +376,50 @@ size_t walk_smem_bytes(int block, bool quad) {
   return static_cast<size_t>(block / 32) * (sizeof(WarpLists) + (quad ? sizeof(WarpQuads) : 0));
 }
 
-// FP32 walk: one warp per 32 Morton-consecutive targets; the warp visits the union of
-// their walks (each node is decided once for every lane that reached it) but not one
-// node at a time. A round pops up to 32 opened nodes from the warp's stack, one per
+namespace {
+
+// Plummer-softened monopole terms of two entries for one target: t += d m / (d^2 + eps^2)^1.5
+// where the target takes the entry (t0, t1). r^2 is clamped at 1e-24 so that a zero
+// distance (the target's own leaf) gives an exact zero term even without softening.
+__device__ __forceinline__ void mono2(float2 dx, float2 dy, float2 dz, float2 m, float2 eps2, bool t0, bool t1,
+                                      float2& tx, float2& ty, float2& tz, float& i0, float& i1) {
+  const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+  const float2 r2s = __fadd2_rn(d2, eps2);
+  i0 = rsqrtf(fmaxf(r2s.x, 1e-24f));
+  i1 = rsqrtf(fmaxf(r2s.y, 1e-24f));
+  const float2 inv = f2(i0, i1);
+  const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
+  float2 f = __fmul2_rn(m, inv3);
+  f.x = t0 ? f.x : 0.f;
+  f.y = t1 ? f.y : 0.f;
+  tx = __ffma2_rn(dx, f, tx);
+  ty = __ffma2_rn(dy, f, ty);
+  tz = __ffma2_rn(dz, f, tz);
+}
+
+}  // namespace
+
+// FP32 walk: one warp per G Morton-consecutive targets (G = 8, 16 or 32: the system's
+// grouping, or the target list's), R = 32 / G lanes a target; the warp visits the union
+// of their walks (each node is decided once for every target that reached it) but not
+// one node at a time. A round pops up to 32 opened nodes from the warp's stack, one per
 // lane, loads each one's sibling-pair record (both children: float-float centre of mass,
 // mass, FP32 take / open thresholds, child codes) and decides each child for the whole
-// warp against the bounding box of the warp's targets:
+// warp against the padded bounding box of the warp's targets:
 //   - taken by every target (or a leaf): appended to the dense list;
-//   - opened by every target: pushed back on the stack with the same lane mask;
+//   - opened by every target: pushed back on the stack with the same target mask;
 //   - otherwise: appended to the undecided list.
-// A list holding 32 entries is evaluated by all 32 lanes together, two entries per
-// packed-FP32 instruction: the dense list with no decisions, the undecided list with
-// each lane's exact test (FP64 re-decision in the band, the inside test for
-// theta >= 1/sqrt 3), and the lanes that open an undecided child push it with their
-// mask. Rounds, lists and entries are independent of one another, so the walk has no
+// A list holding 32 entries is evaluated by all lanes together (the R lanes of a target
+// take turns over its entries), four entries a lane-iteration with packed FP32: the dense
+// list with no decisions, the undecided list with each target's exact test (FP64
+// re-decision in the band, the inside test for theta >= 1/sqrt 3); the targets that open
+// an undecided entry are recorded in it, and one pass afterwards pushes the opened
+// entries. Rounds, lists and entries are independent of one another, so the walk has no
 // dependent chain of one record per step. While the stack holds more than kWalkDeep
 // entries, a round takes only the top entry (and evaluates its undecided children at
 // once): the stack then grows like a depth-first walk, by at most one entry per tree
-// level, which bounds it within kWalkStack. Every lane takes exactly the reference's set
-// of terms; only the order of summation differs from the FP64 walk. Terms are summed
+// level, which bounds it within kWalkStack. Every target takes exactly the reference's
+// set of terms; only the order of summation differs from the FP64 walk. Terms are summed
 // four at a time into a Kahan-compensated accumulator. Node indices are clamped into the
 // record array and the number of records a warp visits is bounded by the system's node
 // count, so even a corrupt tree cannot read out of bounds or loop; a clamp, an exhausted
@@ -410,9 +439,8 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
     const WalkItem it = b.items[item];
     const SysDesc sd = b.sys[it.sys];
     const uint32_t end = sd.off + sd.n;
-    // G targets a warp (the system's group, or the target list's), R = 32 / G lanes a
-    // target: lane = sub * G + target, so the lanes of one sub-lane index hold contiguous
-    // ballot bits. Masks have one bit per target.
+    // G targets a warp, R = 32 / G lanes a target: lane = sub * G + target, so the lanes of
+    // one sub-lane index hold contiguous ballot bits. Masks have one bit per target.
     const uint32_t G = LIST ? b.group : sd.group;
     const int lg = __ffs(G) - 1;
     const uint32_t gmask = G == 32 ? 0xffffffffu : (1u << G) - 1u;
@@ -428,7 +456,7 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
     float sz = 0.f, cz = 0.f;
     unsigned long long n_leaf = 0, n_far = 0, n_open = 0, n_re = 0, n_vis = 0;
     bool bad = false;
-    // The root's box is the system's box, so every target is inside it and every lane
+    // The root's box is the system's box, so every target is inside it and every target
     // opens it -- unless the whole system is massless, when nothing is added.
     const uint32_t root = sd.off;  // internal node 0 of the system
     if (sd.n > 1 && vmask && __ldg(&b.agg64[root].m) > 0.0) {
@@ -449,29 +477,34 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
       // negated target coordinates, duplicated for both entries of a packed pair
       const float2 nxh = f2(-xh[0], -xh[0]), nyh = f2(-xh[1], -xh[1]), nzh = f2(-xh[2], -xh[2]);
       const float2 nxl = f2(-xl[0], -xl[0]), nyl = f2(-xl[1], -xl[1]), nzl = f2(-xl[2], -xl[2]);
-      // The targets' padded bounding box as negated faces (lo, hi), duplicated. A target
-      // that is not finite turns the box into all of space: no group decisions.
+      // The targets' padded bounding box as negated faces (lo, hi), duplicated, and its
+      // centre o (an FP32 value): dense entries and targets are stored relative to o. A
+      // target that is not finite turns the box into all of space: no group decisions.
       const bool fin = isfinite(xh[0]) && isfinite(xh[1]) && isfinite(xh[2]);
       const bool all_fin = __all_sync(0xffffffffu, !valid || fin);
-      float2 nlo[3], nhi[3];
+      float2 nlo[3], nhi[3], no[3];
+      float xr[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         float l = fdeord(__reduce_min_sync(0xffffffffu, valid ? ford(xh[c]) : 0x7fffffff));
         float h = fdeord(__reduce_max_sync(0xffffffffu, valid ? ford(xh[c]) : static_cast<int>(0x80000000u)));
+        const float o = all_fin ? 0.5f * l + 0.5f * h : 0.f;
         const float pad = (fabsf(l) + fabsf(h)) * 0x1p-21f + 1e-30f;
         l = all_fin ? l - pad : -INFINITY;
         h = all_fin ? h + pad : INFINITY;
         nlo[c] = f2(-l, -l);
         nhi[c] = f2(-h, -h);
+        no[c] = f2(-o, -o);
+        xr[c] = (xh[c] - o) + xl[c];  // the target relative to o
       }
+      const float2 nxr = f2(-xr[0], -xr[0]), nyr = f2(-xr[1], -xr[1]), nzr = f2(-xr[2], -xr[2]);
       const uint32_t gmax = n_total - 1;
       const uint32_t max_pairs = sd.n + 64u;
       uint32_t pairs_done = 0;
-      int sp = 1, dl = 0, ul = 0, pend = 0;
+      int sp = 1, dl = 0, ul = 0;
       if (lane == 0) L.stk[0] = make_uint2(root, vmask);
       __syncwarp();
       float2 tx = f2(0.f, 0.f), ty = f2(0.f, 0.f), tz = f2(0.f, 0.f);  // per-entry term sums
-      // list entries a lane evaluates: pairs p = q R + sl of the list, q = 0, 1, ...
       // add the term sums of the last entries to the lane's compensated accumulator
       auto fold = [&]() {
         const float2 txy = f2(tx.x + tx.y, ty.x + ty.y);
@@ -490,14 +523,11 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
           sz += tzz;
         }
         tx = ty = tz = f2(0.f, 0.f);
-        pend = 0;
       };
-      auto put_dense = [&](int e, float xh_, float yh_, float zh_, float m_, float xl_, float yl_, float zl_,
-                           uint32_t mask, uint32_t code) {
-        put2(L.da, e, xh_, yh_);
-        put2(L.db, e, zh_, m_);
-        put2(L.dc, e, xl_, yl_);
-        put2(L.dd, e, zl_, __uint_as_float(mask));
+      auto put_dense = [&](int e, float x_, float y_, float z_, float m_, uint32_t mask, uint32_t code) {
+        put2(L.da, e, x_, y_);
+        put2(L.db, e, z_, m_);
+        reinterpret_cast<uint32_t*>(L.dm + (e >> 1))[e & 1] = mask;
         L.dcode[e] = code;
       };
       auto put_und = [&](int e, float xh_, float yh_, float zh_, float m_, float xl_, float yl_, float zl_,
@@ -550,7 +580,7 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         const float2 dmax2 = __ffma2_rn(fx, fx, __ffma2_rn(fy, fy, __fmul2_rn(fz, fz)));
         bool accL = act && dmin2.x * kGroupLo > r3.z, accR = act && dmin2.y * kGroupLo > r3.w;
         if (inside_rule) {
-          // the group test does not cover the inside rule: nodes go to the lanes' tests
+          // the group test does not cover the inside rule: nodes go to the targets' tests
           accL = accL && (cL & kLeafCode);
           accR = accR && (cR & kLeafCode);
         }
@@ -591,8 +621,14 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
             Q.uqb[eUR] = make_float2(qbR.x, qbR.y);
           }
         }
-        if (accL) put_dense(eAL, chx.x, chy.x, chz.x, r1.z, clx.x, cly.x, clz.x, M, cL);
-        if (accR) put_dense(eAR, chx.y, chy.y, chz.y, r1.w, clx.y, cly.y, clz.y, M, cR);
+        if (accL || accR) {
+          // dense entries relative to the box centre: (c_hi - o) + c_lo
+          const float2 rx = __fadd2_rn(__fadd2_rn(chx, no[0]), clx);
+          const float2 ry = __fadd2_rn(__fadd2_rn(chy, no[1]), cly);
+          const float2 rz = __fadd2_rn(__fadd2_rn(chz, no[2]), clz);
+          if (accL) put_dense(eAL, rx.x, ry.x, rz.x, r1.z, M, cL);
+          if (accR) put_dense(eAR, rx.y, ry.y, rz.y, r1.w, M, cR);
+        }
         dl += __popc(bAL) + __popc(bAR);
         if (undL) put_und(eUL, chx.x, chy.x, chz.x, r1.z, clx.x, cly.x, clz.x, r3.z, r4.x, cL, M);
         if (undR) put_und(eUR, chx.y, chy.y, chz.y, r1.w, clx.y, cly.y, clz.y, r3.w, r4.y, cR, M);
@@ -611,111 +647,28 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         }
         __syncwarp();
       };
-      // Evaluate the dense list: every lane adds the terms of the entries in its mask.
-      auto flush_dense = [&]() {
-        if (dl & 1) {
-          if (lane == 0) put_dense(dl, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0u, kLeafCode);
-          __syncwarp();
-        }
-        const int np = (dl + 1) >> 1;
-        for (int q = 0; q * R < np; ++q) {
-          // lanes past the list's end read its last pair with no target bit
-          const int p0 = q * R + sl, p = min(p0, np - 1), e = 2 * p;
-          const uint32_t on = p0 < np ? 1u : 0u;
-          const float4 A = L.da[p], B = L.db[p], C = L.dc[p], D = L.dd[p];
-          const float2 dx = __fadd2_rn(__fadd2_rn(f2(A.x, A.y), nxh), __fadd2_rn(f2(C.x, C.y), nxl));
-          const float2 dy = __fadd2_rn(__fadd2_rn(f2(A.z, A.w), nyh), __fadd2_rn(f2(C.z, C.w), nyl));
-          const float2 dz = __fadd2_rn(__fadd2_rn(f2(B.x, B.y), nzh), __fadd2_rn(f2(D.x, D.y), nzl));
-          const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-          // Plummer-softened monopole terms; the target's own leaf (d = 0) is an exact zero
-          const float2 r2s = __fadd2_rn(d2, eps2);
-          const float i0 = rsqrtf(fmaxf(r2s.x, 1e-30f)), i1 = rsqrtf(fmaxf(r2s.y, 1e-30f));
-          const float2 inv = f2(i0, i1);
-          const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
-          float2 f = __fmul2_rn(f2(B.z, B.w), inv3);
-          const bool t0 = (__float_as_uint(D.z) >> tg) & on, t1 = (__float_as_uint(D.w) >> tg) & on;
-          f.x = t0 ? f.x : 0.f;
-          f.y = t1 ? f.y : 0.f;
-          tx = __ffma2_rn(dx, f, tx);
-          ty = __ffma2_rn(dy, f, ty);
-          tz = __ffma2_rn(dz, f, tz);
-          if (QUAD || STATS) {
-            const uint32_t c0 = L.dcode[e], c1 = L.dcode[e + 1];
-            if (QUAD) {
-              float tq[3] = {0.f, 0.f, 0.f};
-              if (t0 && !(c0 & kLeafCode)) {
-                const float2 qb = Q.dqb[e];
-                quad_term(Q.dqa[e], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
-              }
-              if (t1 && !(c1 & kLeafCode)) {
-                const float2 qb = Q.dqb[e + 1];
-                quad_term(Q.dqa[e + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
-              }
-              tx.x += tq[0];
-              ty.x += tq[1];
-              tz.x += tq[2];
-            }
-            if (STATS) {
-              const uint32_t self = kLeafCode | k;
-              n_leaf += (t0 && (c0 & kLeafCode) && c0 != self ? 1 : 0) + (t1 && (c1 & kLeafCode) && c1 != self ? 1 : 0);
-              n_far += (t0 && !(c0 & kLeafCode) ? 1 : 0) + (t1 && !(c1 & kLeafCode) ? 1 : 0);
-            }
-          }
-          pend += 2;
-          if (pend >= 4) fold();
-        }
-        dl = 0;
-        __syncwarp();  // read before the next round overwrites the list
-      };
-      // Evaluate the undecided list: each lane decides each entry of its mask; the lanes
-      // that open an entry push it with their mask.
-      auto flush_und = [&]() {
-        if (ul & 1) {
-          if (lane == 0) put_und(ul, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, kLeafCode, 0u);
-          __syncwarp();
-        }
-        const int np = (ul + 1) >> 1;
-        for (int q = 0; q * R < np; ++q) {
-          const int p0 = q * R + sl, p = min(p0, np - 1);
-          const uint32_t on = p0 < np ? 1u : 0u;
-          const float4 A = L.ua[p], B = L.ub[p], C = L.uc[p], D = L.ud[p], E = L.ue[p], F = L.uf[p];
-          const float2 dx = __fadd2_rn(__fadd2_rn(f2(A.x, A.y), nxh), __fadd2_rn(f2(C.x, C.y), nxl));
-          const float2 dy = __fadd2_rn(__fadd2_rn(f2(A.z, A.w), nyh), __fadd2_rn(f2(C.z, C.w), nyl));
-          const float2 dz = __fadd2_rn(__fadd2_rn(f2(B.x, B.y), nzh), __fadd2_rn(f2(D.x, D.y), nzl));
-          const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-          const uint32_t cL = __float_as_uint(E.z), cR = __float_as_uint(E.w);
-          const bool a0 = (__float_as_uint(F.x) >> tg) & on, a1 = (__float_as_uint(F.y) >> tg) & on;
-          bool tL = a0 && d2.x > D.z, tR = a1 && d2.y > D.w;
-          bool oL = a0 && d2.x < E.x, oR = a1 && d2.y < E.y;
-          bool aL = a0 && !tL && !oL, aR = a1 && !tR && !oR;
-          if (inside_rule) {
-            if (tL && !(cL & kLeafCode)) inside_test(b, xh, cL, tL, oL, aL);
-            if (tR && !(cR & kLeafCode)) inside_test(b, xh, cR, tR, oR, aR);
-          }
-          if (__any_sync(0xffffffffu, aL || aR)) {
-            if (STATS) n_re += (aL ? 1 : 0) + (aR ? 1 : 0);
-            if (aL) resolve(b, k, sd.theta, cL, tL, oL);
-            if (aR) resolve(b, k, sd.theta, cR, tR, oR);
-          }
-          const float2 r2s = __fadd2_rn(d2, eps2);
-          const float i0 = rsqrtf(fmaxf(r2s.x, 1e-30f)), i1 = rsqrtf(fmaxf(r2s.y, 1e-30f));
-          const float2 inv = f2(i0, i1);
-          const float2 inv3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
-          float2 f = __fmul2_rn(f2(B.z, B.w), inv3);
-          f.x = tL ? f.x : 0.f;
-          f.y = tR ? f.y : 0.f;
-          tx = __ffma2_rn(dx, f, tx);
-          ty = __ffma2_rn(dy, f, ty);
-          tz = __ffma2_rn(dz, f, tz);
+      // The dense terms of pair p (entries 2p, 2p + 1) for this lane's target; on = 0 for
+      // a lane past the list's end (it reads the last pair with no target bit).
+      auto dense_pair = [&](int p, uint32_t on) {
+        const float4 A = L.da[p], B = L.db[p];
+        const uint2 Mk = L.dm[p];
+        const float2 dx = __fadd2_rn(f2(A.x, A.y), nxr);
+        const float2 dy = __fadd2_rn(f2(A.z, A.w), nyr);
+        const float2 dz = __fadd2_rn(f2(B.x, B.y), nzr);
+        const bool t0 = (Mk.x >> tg) & on, t1 = (Mk.y >> tg) & on;
+        float i0, i1;
+        mono2(dx, dy, dz, f2(B.z, B.w), eps2, t0, t1, tx, ty, tz, i0, i1);
+        if (QUAD || STATS) {
+          const uint32_t c0 = L.dcode[2 * p], c1 = L.dcode[2 * p + 1];
           if (QUAD) {
             float tq[3] = {0.f, 0.f, 0.f};
-            if (tL && !(cL & kLeafCode)) {
-              const float2 qb = Q.uqb[2 * p];
-              quad_term(Q.uqa[2 * p], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
+            if (t0 && !(c0 & kLeafCode)) {
+              const float2 qb = Q.dqb[2 * p];
+              quad_term(Q.dqa[2 * p], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
             }
-            if (tR && !(cR & kLeafCode)) {
-              const float2 qb = Q.uqb[2 * p + 1];
-              quad_term(Q.uqa[2 * p + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
+            if (t1 && !(c1 & kLeafCode)) {
+              const float2 qb = Q.dqb[2 * p + 1];
+              quad_term(Q.dqa[2 * p + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
             }
             tx.x += tq[0];
             ty.x += tq[1];
@@ -723,24 +676,104 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
           }
           if (STATS) {
             const uint32_t self = kLeafCode | k;
-            n_leaf += (tL && (cL & kLeafCode) && cL != self ? 1 : 0) + (tR && (cR & kLeafCode) && cR != self ? 1 : 0);
-            n_far += (tL && !(cL & kLeafCode) ? 1 : 0) + (tR && !(cR & kLeafCode) ? 1 : 0);
-            n_open += (oL ? 1 : 0) + (oR ? 1 : 0);
+            n_leaf += (t0 && (c0 & kLeafCode) && c0 != self ? 1 : 0) + (t1 && (c1 & kLeafCode) && c1 != self ? 1 : 0);
+            n_far += (t0 && !(c0 & kLeafCode) ? 1 : 0) + (t1 && !(c1 & kLeafCode) ? 1 : 0);
           }
-          // the targets that open this lane's entries; lane sl * G pushes them
-          const uint32_t m0 = (__ballot_sync(0xffffffffu, oL) >> (sl * G)) & gmask;
-          const uint32_t m1 = (__ballot_sync(0xffffffffu, oR) >> (sl * G)) & gmask;
-          const uint32_t b0 = __ballot_sync(0xffffffffu, tg == 0 && m0), b1 = __ballot_sync(0xffffffffu, tg == 0 && m1);
-          const int npush = __popc(b0) + __popc(b1);
-          if (sp + npush > kWalkStack) {
+        }
+      };
+      // Evaluate the dense list: every target adds the terms of the entries in its mask.
+      // The R lanes of a target take pairs (2u, 2u + 1) of quads u = q R + sl.
+      auto flush_dense = [&]() {
+        if (dl & 1) {
+          if (lane == 0) put_dense(dl, 0.f, 0.f, 0.f, 0.f, 0u, kLeafCode);
+          __syncwarp();
+        }
+        const int np = (dl + 1) >> 1;
+        for (int q = 0; 2 * q * R < np; ++q) {
+          const int pa = 2 * (q * R + sl), pb = pa + 1;
+          dense_pair(min(pa, np - 1), pa < np ? 1u : 0u);
+          dense_pair(min(pb, np - 1), pb < np ? 1u : 0u);
+          fold();
+        }
+        dl = 0;
+        __syncwarp();  // read before the next round overwrites the list
+      };
+      // The undecided pair p for this lane's target; records the targets that open each
+      // entry in the entry (lane sub * G of each sub-lane writes its pair's).
+      auto und_pair = [&](int p, uint32_t on) {
+        const float4 A = L.ua[p], B = L.ub[p], C = L.uc[p], D = L.ud[p], E = L.ue[p], F = L.uf[p];
+        const float2 dx = __fadd2_rn(__fadd2_rn(f2(A.x, A.y), nxh), __fadd2_rn(f2(C.x, C.y), nxl));
+        const float2 dy = __fadd2_rn(__fadd2_rn(f2(A.z, A.w), nyh), __fadd2_rn(f2(C.z, C.w), nyl));
+        const float2 dz = __fadd2_rn(__fadd2_rn(f2(B.x, B.y), nzh), __fadd2_rn(f2(D.x, D.y), nzl));
+        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        const uint32_t cL = __float_as_uint(E.z), cR = __float_as_uint(E.w);
+        const bool a0 = (__float_as_uint(F.x) >> tg) & on, a1 = (__float_as_uint(F.y) >> tg) & on;
+        bool tL = a0 && d2.x > D.z, tR = a1 && d2.y > D.w;
+        bool oL = a0 && d2.x < E.x, oR = a1 && d2.y < E.y;
+        bool aL = a0 && !tL && !oL, aR = a1 && !tR && !oR;
+        if (inside_rule) {
+          if (tL && !(cL & kLeafCode)) inside_test(b, xh, cL, tL, oL, aL);
+          if (tR && !(cR & kLeafCode)) inside_test(b, xh, cR, tR, oR, aR);
+        }
+        if (__any_sync(0xffffffffu, aL || aR)) {
+          if (STATS) n_re += (aL ? 1 : 0) + (aR ? 1 : 0);
+          if (aL) resolve(b, k, sd.theta, cL, tL, oL);
+          if (aR) resolve(b, k, sd.theta, cR, tR, oR);
+        }
+        float i0, i1;
+        mono2(dx, dy, dz, f2(B.z, B.w), eps2, tL, tR, tx, ty, tz, i0, i1);
+        if (QUAD) {
+          float tq[3] = {0.f, 0.f, 0.f};
+          if (tL && !(cL & kLeafCode)) {
+            const float2 qb = Q.uqb[2 * p];
+            quad_term(Q.uqa[2 * p], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
+          }
+          if (tR && !(cR & kLeafCode)) {
+            const float2 qb = Q.uqb[2 * p + 1];
+            quad_term(Q.uqa[2 * p + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
+          }
+          tx.x += tq[0];
+          ty.x += tq[1];
+          tz.x += tq[2];
+        }
+        if (STATS) {
+          const uint32_t self = kLeafCode | k;
+          n_leaf += (tL && (cL & kLeafCode) && cL != self ? 1 : 0) + (tR && (cR & kLeafCode) && cR != self ? 1 : 0);
+          n_far += (tL && !(cL & kLeafCode) ? 1 : 0) + (tR && !(cR & kLeafCode) ? 1 : 0);
+          n_open += (oL ? 1 : 0) + (oR ? 1 : 0);
+        }
+        const uint32_t m0 = (__ballot_sync(0xffffffffu, oL) >> (sl * G)) & gmask;
+        const uint32_t m1 = (__ballot_sync(0xffffffffu, oR) >> (sl * G)) & gmask;
+        if (tg == 0 && on) reinterpret_cast<uint2*>(L.uf + p)[1] = make_uint2(m0, m1);
+      };
+      // Evaluate the undecided list, then push every entry some target opened.
+      auto flush_und = [&]() {
+        if (ul & 1) {
+          if (lane == 0) put_und(ul, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, kLeafCode, 0u);
+          __syncwarp();
+        }
+        const int np = (ul + 1) >> 1;
+        for (int q = 0; 2 * q * R < np; ++q) {
+          const int pa = 2 * (q * R + sl), pb = pa + 1;
+          und_pair(min(pa, np - 1), pa < np ? 1u : 0u);
+          und_pair(min(pb, np - 1), pb < np ? 1u : 0u);
+          fold();
+        }
+        __syncwarp();  // the opened masks are written
+        for (int e0 = 0; e0 < ul; e0 += 32) {
+          const int e = e0 + lane;
+          uint32_t om = 0, code = 0;
+          if (e < ul) {
+            om = reinterpret_cast<const uint32_t*>(L.uf + (e >> 1))[2 + (e & 1)];
+            code = reinterpret_cast<const uint32_t*>(L.ue + (e >> 1))[2 + (e & 1)];
+          }
+          const uint32_t bp = __ballot_sync(0xffffffffu, om != 0u);
+          if (sp + __popc(bp) > kWalkStack) {
             bad = true;
           } else {
-            if (tg == 0 && m0) L.stk[sp + __popc(b0 & lt)] = make_uint2(cL, m0);
-            if (tg == 0 && m1) L.stk[sp + __popc(b0) + __popc(b1 & lt)] = make_uint2(cR, m1);
-            sp += npush;
+            if (om) L.stk[sp + __popc(bp & lt)] = make_uint2(code, om);
+            sp += __popc(bp);
           }
-          pend += 2;
-          if (pend >= 4) fold();
         }
         ul = 0;
         __syncwarp();  // pushes visible to the next round; list read before it is refilled
