@@ -96,13 +96,51 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+WORKLOADS = {
+    "collision": dict(eps=0.02, theta=0.5, dt=5e-4, name="collision-2x524288", multipole="mono",
+                      n=2 * N_PER_GALAXY),
+    "plummer": dict(eps=0.01, theta=0.5, dt=1e-3, name="plummer-16384", multipole="quad", n=16_384),
+}
+
+
 def workload(config: str, seed: int):
+    """The seeded workload state (product library's generator) and its parameters."""
     import galaxy_b200 as gb
 
+    p = WORKLOADS["plummer" if config == "plummer" else "collision"]
     if config == "plummer":
-        return gb.ic.plummer(16_384, seed), dict(eps=0.01, theta=0.5, dt=1e-3, name="plummer-16384", multipole="quad")
-    st = gb.ic.collision(2 * N_PER_GALAXY, seed, mass_ratio=1.0, pericentre=4.0, incl1_deg=30.0, incl2_deg=60.0)
-    return st, dict(eps=0.02, theta=0.5, dt=5e-4, name="collision-2x524288", multipole="mono")
+        return gb.ic.plummer(p["n"], seed), p
+    return gb.ic.collision(p["n"], seed, mass_ratio=1.0, pericentre=4.0, incl1_deg=30.0, incl2_deg=60.0), p
+
+
+def workload_oracle(config: str, seed: int):
+    """The same inputs from the oracle library's copy of the generator, so the CPU
+    reference arm never loads the product library."""
+    from oracle import oracle
+
+    p = WORKLOADS["plummer" if config == "plummer" else "collision"]
+    if config == "plummer":
+        return oracle.ic_plummer(p["n"], seed), p
+    return oracle.ic_collision(p["n"], seed, 1.0, 4.0, 30.0, 60.0), p
+
+
+def native_libraries() -> list:
+    """Shared libraries of this repository mapped into this process (from /proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so")}
+    except OSError:
+        return []
+    return sorted(os.path.relpath(q, ROOT) for q in paths if q.startswith(ROOT + os.sep))
+
+
+def shared_config(p: dict, n: int) -> dict:
+    """The workload as both arms print it (the same dict in the GPU and the CPU line)."""
+    return {"workload": p["name"], "particles": n, "theta": p["theta"], "eps": p["eps"], "dt": p["dt"], "g": 1.0,
+            "multipole": p["multipole"], "seed": 0,
+            "l2": (f"working set ~{352 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)" if 352 * n > 126e6 else
+                   f"working set ~{352 * n / 1e6:.0f} MB fits in L2: steps replay back to back with the state "
+                   f"resident, as a resident integrator runs (not a flushed-cache number)")}
 
 
 # ---- algorithmic work per launch (bytes / flops) ----------------------------------------
@@ -119,21 +157,64 @@ def profiled_walk(workload_name: str, key: str):
         return None
 
 
-def cpu_sample_step(st, params, threads: int, n_targets: int, rng) -> float:
-    """Seconds for one CPU step estimated from a bounded sample: the oracle's full tree
-    build plus the walk of n_targets random targets, scaled to all N targets."""
+def cpu_sample_step(pos, mass, params, threads: int, n_targets: int, rng) -> float:
+    """Seconds for one CPU force evaluation estimated from a bounded sample: the oracle's
+    full tree build plus the walk of n_targets random targets, scaled to all N targets."""
     from oracle import oracle
 
-    n = len(st)
+    n = len(mass)
     t0 = time.perf_counter()
-    oracle.lbvh_accelerations_subset(st.pos, st.mass, 1.0, params["eps"], params["theta"], np.zeros(1, np.uint32),
+    oracle.lbvh_accelerations_subset(pos, mass, 1.0, params["eps"], params["theta"], np.zeros(1, np.uint32),
                                      threads=threads)
     t_build = time.perf_counter() - t0
     tg = rng.choice(n, n_targets, replace=False).astype(np.uint32)
     t0 = time.perf_counter()
-    oracle.lbvh_accelerations_subset(st.pos, st.mass, 1.0, params["eps"], params["theta"], tg, threads=threads)
+    oracle.lbvh_accelerations_subset(pos, mass, 1.0, params["eps"], params["theta"], tg, threads=threads)
     t_walk = time.perf_counter() - t0 - t_build
     return t_build + max(t_walk, 0.0) * n / n_targets
+
+
+def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict) -> dict:
+    """Roofline of the dominant kernel (the FP32 walk) and the HBM fractions of the other
+    stages: algorithmic flops (or bytes) per launch over the launch's CUDA-event time."""
+    quad = p["multipole"] == "quad"
+    sb = roofline.stage_bytes(n, key64=False, quad=quad)
+    flops = roofline.walk_flops(counts["leaf"], counts["far"], counts["open"], quad=quad)
+    walk_s = stage["ms_walk"] / 1e3
+    mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    achieved = flops / walk_s / 1e12
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    sort_gbs = roofline.hbm_fraction(sb["sort"], stage["ms_sort"], hbm)[0]
+    build_gbs = roofline.hbm_fraction(sb["build"], stage["ms_build"], hbm)[0]
+    mort_gbs = roofline.hbm_fraction(sb["kick_drift_bbox"] + sb["morton"], stage["ms_bbox_morton"], hbm)[0]
+    prof = f"profiles/k_walk_f32_{p['name'].replace('collision-', 'collision_')}.md"
+    traffic = profiled_walk(p["name"], "traffic_bytes_per_launch")
+    inst = profiled_walk(p["name"], "instructions_per_launch")
+    issue = None
+    if inst:
+        rate, frac = roofline.issue_fraction(inst, stage["ms_walk"], 148, mhz)
+        issue = {"achieved_ginst_s": rate, "peak_ginst_s": 148 * 4 * mhz / 1e3, "frac": frac,
+                 "source": f"warp instructions per launch from {prof} over this run's walk time; peak = one warp "
+                           f"instruction per scheduler per clock"}
+    return {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+            "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, {prof}"
+                              if traffic else None,
+            "algorithmic_bytes_per_launch": sb["walk"],
+            "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm (MEASURED_PEAKS.json "
+                           "has no FP32 figure); no tensor-core work in this path",
+            "flops_per_launch": flops, "ms_per_launch": stage["ms_walk"], "issue": issue,
+            "interactions_per_particle": (counts["leaf"] + counts["far"]) / n,
+            "hbm_stages": {
+                "sort (4 onesweep passes)": {"achieved_gbs": sort_gbs, "frac": sort_gbs / hbm, "ms": stage["ms_sort"],
+                                             "bytes": sb["sort"]},
+                "build + aggregation": {"achieved_gbs": build_gbs, "frac": build_gbs / hbm, "ms": stage["ms_build"],
+                                        "bytes": sb["build"]},
+                "kick/drift/bbox + Morton": {"achieved_gbs": mort_gbs, "frac": mort_gbs / hbm,
+                                             "ms": stage["ms_bbox_morton"],
+                                             "bytes": sb["kick_drift_bbox"] + sb["morton"]},
+                "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
 
 
 def run_reference_sph(args, threads: int):
@@ -186,28 +267,108 @@ def run_reference(args):
         if dist is not None:
             dist.destroy_process_group()
         return
-    st, p = workload(args.config, 0)
-    n = len(st)
-    rng = np.random.default_rng(1)
-    n_targets = min(n, 16_384)
+    (pos, vel, mass), p = workload_oracle(args.config, 0)
+    n = len(mass)
+    # Whole KDK steps of the full system (LeapfrogKdk + Lbvh: a serial tree build and the
+    # walk over every target on all host threads, then the kicks and the drift), the
+    # oracle's C++ restatement of the reference (the Rust crate cannot be built here).
+    # The priming force evaluation runs before the warm-up steps.
+    kdk = oracle.LeapfrogKdkLbvh(1.0, p["eps"], p["theta"], threads=threads)
+    kdk.step_many(pos, vel, mass, p["dt"], 0)
+    kdk.prime(pos, mass)
     for _ in range(args.warmup):
-        cpu_sample_step(st, p, threads, min(n_targets, 1024), rng)
-    times = [cpu_sample_step(st, p, threads, n_targets, rng) for _ in range(args.steps)]
+        kdk.step_many(pos, vel, mass, p["dt"], 1)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        kdk.step_many(pos, vel, mass, p["dt"], 1)
+        times.append(time.perf_counter() - t0)
     t_step = statistics.mean(times)
     value = n / t_step
-    sample = (f"per step: full {n}-particle tree build + walk of {n_targets} random targets with {threads} "
-              f"threads, scaled to all targets (C++ restatement of the reference Lbvh; the Rust crate "
-              f"cannot be built here)")
+    ref_config = shared_config(p, n)
+    if p["multipole"] != "mono":
+        ref_config["multipole"] = "mono (the reference has no quadrupole nodes)"
+    sample = (f"whole KDK steps of the full {n}-particle system: tree build, walk of every target with "
+              f"{threads} threads, kicks and drift (the oracle's C++ restatement of LeapfrogKdk + Lbvh; monopole, "
+              f"as the reference)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": p["name"], "particles": n, "theta": p["theta"], "eps": p["eps"], "dt": p["dt"]},
+            "config": ref_config,
+            "step_ms_p50": float(np.percentile(times, 50)) * 1e3, "step_ms_p99": float(np.percentile(times, 99)) * 1e3,
+            "native_libraries": native_libraries(),
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def measure_mix(args, dist, rank, ws, local, steps: int, warmup: int) -> dict:
+    """The batched uneven-systems mix (N log-uniform in [4096, 262144], half Plummer
+    spheres, half disk + halo galaxies, eps 0.01, theta 0.5, dt 1e-3 / 5e-4): the batch
+    (one launch per stage, persistent work-stealing walk, CUDA-graph replay) against the
+    plain single-system path stepping the same systems one after another. Per-step device
+    times (CUDA events) of both; the max over ranks; each rank builds only its shard."""
+    import galaxy_b200 as gb
+    from galaxy_b200 import workloads
+
+    sizes = workloads.batched_sizes(args.systems * ws, seed=0)
+    mine = ranks.shard(sizes, ws)[rank]
+    mix = workloads.batched_mix(args.systems * ws, seed=0, indices=mine)
+    n_tot = sum(len(m.state) for m in mix)
+    k63 = args.morton63
+    b = gb.Batch(device=local, morton63=k63)
+    for m in mix:
+        b.add(m.state, m.g, m.eps, m.theta, m.dt)
+    b.step(max(warmup, 1))
+    tune = b.autotune(repeats=2)  # persistent walk launch for this batch (untimed)
+    b.step(1)  # re-capture the step graph outside the timed region
+    gb.device_synchronize(local)
+    ranks.barrier(dist, local)
+    ms = []
+    for _ in range(steps):
+        b.step(1)
+        ms.append(b.stats()["ms_last_step"])
+    gb.device_synchronize(local)
+    ranks.barrier(dist, local)
+    t = ranks.max_over_ranks(dist, sum(ms) / 1e3, local)
+    n_all = ranks.sum_over_ranks(dist, n_tot, local)  # particles on all ranks
+    value = n_all * steps / t
+    del b
+    # plain path: the same systems, each stepped alone by the single-system handle
+    hs = []
+    for m in mix:
+        r = gb.GpuResidentLeapfrog(m.g, m.eps, m.theta, device=local, morton63=k63)
+        r.upload(m.state)
+        r.step_many(m.dt, 1)
+        if gb.tuning_lookup(len(m.state), morton63=k63, device=local) is None:
+            r.autotune(repeats=2)  # the plain path is tuned per N bucket too
+        r.step_many(m.dt, 2)  # capture the handle's step graph before timing (as the batch's)
+        hs.append((r, m))
+    k_plain = max(1, min(steps, 3))
+    t_plain = 0.0
+    plain_ms = []
+    for _ in range(k_plain):
+        t_pass = 0.0
+        for r, m in hs:
+            t_pass += r.step_many_timed(m.dt, 1)
+        plain_ms.append(t_pass)
+        t_plain += t_pass / 1e3
+    t_plain = ranks.max_over_ranks(dist, t_plain, local)
+    plain = n_all * k_plain / t_plain
+    del hs
+    return {"workload": f"batched-{args.systems}-systems", "systems": args.systems * ws, "particles": n_all,
+            "morton_bits": 63 if k63 else 30, "n_range": [4096, 262144], "theta": 0.5, "eps": 0.01,
+            "dt": [1e-3, 5e-4], "value": value, "unit": "particle-steps/s", "steps": steps,
+            "step_ms_p50": float(np.percentile(ms, 50)), "step_ms_p99": float(np.percentile(ms, 99)),
+            "plain_value": plain, "plain_steps": k_plain,
+            "plain_pass_ms_p50": float(np.percentile(plain_ms, 50)),
+            "plain_how": "same systems, one single-system handle each, stepped one after another (device time of "
+                         "each step summed)",
+            "batched_over_plain": value / plain, "gpu_launches_per_step": 12 if k63 else 8,
+            "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}}
 
 
 def run_ours(args):
@@ -236,6 +397,8 @@ def run_ours(args):
     clk = clocks.stop()
     ms_max = ranks.max_over_ranks(dist, ms, local)
     value = n * ws * args.steps / (ms_max / 1e3)
+    # per-step latency of the same path: single graph replays, each timed on the device
+    lat = [r.step_many_timed(dt, 1) for _ in range(max(args.steps, 10))]
 
     # --- e2e: the reference-facing ForceSolver path (LeapfrogKdk on host arrays) ---
     pinned = gb.PinnedState.from_state(st)
@@ -257,7 +420,7 @@ def run_ours(args):
     e2e = {"value": n * ws * k_e2e / t_e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * n,
            "d2h_bytes_per_step": 24 * n, "steps": k_e2e, "repetitions": 3,
            "path": "LeapfrogKdk on pinned host f64 arrays, gx_accelerations per step (upload pos+mass, download acc)"}
-    del pinned
+    del pinned, h
 
     # --- per-stage device times (eager launches with CUDA events on the handle's stream) ---
     rs = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], multipole=mp, device=local, stage_times=True)
@@ -270,147 +433,76 @@ def run_ours(args):
         s = rs.stats()
         for k in stage:
             stage[k] += s[k] / k_st
+    del rs
     counts_h = gb.GpuLbvh(1.0, p["eps"], p["theta"], multipole=mp, device=local, stats=True)
     counts_h.accelerations(st)
     c = counts_h.stats()
+    del counts_h
     counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"],
-              "warp_visits": c["warp_node_visits"], "f64_rechecks": c["f64_rechecks"]}
-    quad = mp == "quad"
-    sb = roofline.stage_bytes(n, key64=False, quad=quad)
-    alg = {"walk_flops": roofline.walk_flops(counts["leaf"], counts["far"], counts["open"], quad=quad)}
-    walk_s = stage["ms_walk"] / 1e3
-    sm_clock = (clk["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0))
-    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    achieved = alg["walk_flops"] / walk_s / 1e12
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    sort_gbs = roofline.hbm_fraction(sb["sort"], stage["ms_sort"], hbm)[0]
-    build_gbs = roofline.hbm_fraction(sb["build"], stage["ms_build"], hbm)[0]
-    mort_gbs = roofline.hbm_fraction(sb["kick_drift_bbox"] + sb["morton"], stage["ms_bbox_morton"], hbm)[0]
-    traffic = profiled_walk(p["name"], "traffic_bytes_per_launch")
-    inst = profiled_walk(p["name"], "instructions_per_launch")
-    roof = {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
-                                  "profiles/k_walk_f32_collision_2x524288.md" if traffic else None,
-                "algorithmic_bytes_per_launch": sb["walk"],
-                "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm "
-                               "(MEASURED_PEAKS.json has no FP32 figure); no tensor-core work in this path",
-                "flops_per_launch": alg["walk_flops"], "ms_per_launch": stage["ms_walk"],
-                "issue": ({"achieved_ginst_s": roofline.issue_fraction(inst, stage["ms_walk"], 148, peaks.get("sm_max_mhz", 1965.0))[0],
-                           "peak_ginst_s": 148 * 4 * peaks.get("sm_max_mhz", 1965.0) / 1e3,
-                           "frac": roofline.issue_fraction(inst, stage["ms_walk"], 148, peaks.get("sm_max_mhz", 1965.0))[1],
-                           "source": "warp instructions per launch from the ncu summary in profiles/ over this "
-                                     "run's walk time; peak = one warp instruction per scheduler per clock"}
-                          if inst else None),
-                "interactions_per_particle": (counts["leaf"] + counts["far"]) / n,
-                "lane_utilisation": (counts["leaf"] + counts["far"] + counts["open"]) / (64.0 * counts["warp_visits"]),
-                "hbm_stages": {
-                    "sort (4 onesweep passes)": {"achieved_gbs": sort_gbs, "frac": sort_gbs / hbm,
-                                                 "ms": stage["ms_sort"], "bytes": sb["sort"]},
-                    "build + aggregation": {"achieved_gbs": build_gbs, "frac": build_gbs / hbm,
-                                            "ms": stage["ms_build"], "bytes": sb["build"]},
-                    "kick/drift/bbox + Morton": {"achieved_gbs": mort_gbs, "frac": mort_gbs / hbm,
-                                                 "ms": stage["ms_bbox_morton"],
-                                                 "bytes": sb["kick_drift_bbox"] + sb["morton"]},
-                    "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
+              "pair_records": c["warp_node_visits"], "f64_rechecks": c["f64_rechecks"]}
+    roof = walk_roofline(p, n, stage, counts, peaks)
+
+    # --- the batched mix (BASELINE metric: batched vs plain, p50/p99), default workload ---
+    mix = None
+    if args.config == "collision" and not args.no_batched:
+        mix = measure_mix(args, dist, rank, ws, local, steps=max(3, min(args.steps, 5)), warmup=args.warmup)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
+        from oracle import oracle
+
+        # the serial reference (one thread: Lbvh's per-target loop, solvers/src/lbvh.rs:673-675)
         rng = np.random.default_rng(1)
-        t = statistics.mean(cpu_sample_step(st, p, threads, 8192, rng) for _ in range(2))
-        cpu = {"value": n / t, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-               "sample": f"2 samples of: full {n}-particle tree build + walk of 8192 random targets, "
-                         f"{threads} threads, scaled to all targets (oracle C++ restatement of Lbvh)"}
+        t = statistics.mean(cpu_sample_step(st.pos, st.mass, p, 1, 8192, rng) for _ in range(2))
+        cpu = {"value": n / t, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+               "sample": f"2 samples of: the full {n}-particle tree build + the walk of 8192 random targets on one "
+                         f"thread, scaled to all targets (the oracle's serial C++ restatement of Lbvh, as the "
+                         f"reference's serial per-target loop); whole all-core KDK steps are the reference arm"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": p["name"], "particles_per_gpu": n, "theta": p["theta"], "eps": p["eps"],
-                           "dt": p["dt"], "multipole": mp, "precision": "FP32 walk (Kahan), FP64 pos/vel and opening re-checks",
-                           "parallelism": "replicas" if ws > 1 else "single system",
-                           "l2": (f"working set ~{352 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)" if 352 * n > 126e6 else
-                                  f"working set ~{352 * n / 1e6:.0f} MB fits in L2: steps replay back to back with the state resident, as a resident integrator runs (not a flushed-cache number)"),
-                           "cuda_graph": True,
-                           "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm", "walk_group")}},
+                "config": shared_config(p, n),
+                "implementation": {"precision": "FP32 walk (Kahan), FP64 pos/vel and opening re-checks",
+                                   "parallelism": "replicas" if ws > 1 else "single system", "cuda_graph": True,
+                                   "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm",
+                                                                        "walk_group")}},
+                "step_ms_p50": float(np.percentile(lat, 50)), "step_ms_p99": float(np.percentile(lat, 99)),
                 "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "walk_counts": counts}
+        if mix is not None:
+            line["batched_over_plain"] = mix["batched_over_plain"]
+            line["batched"] = mix
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
 
 def run_batched(args):
-    """256 independent systems (N log-uniform in [4096, 262144], half Plummer, half disk +
-    halo, eps 0.01, theta 0.5, dt 1e-3 / 5e-4) in one batch vs the plain single-system
-    path stepping the same systems one at a time."""
+    """256 independent systems in one batch vs the plain single-system path stepping
+    the same systems one at a time (see measure_mix)."""
     import galaxy_b200 as gb
-    from galaxy_b200 import workloads
 
     dist, rank, ws, local = ranks.init()
-    # A global mix of systems x ranks systems, partitioned by particle count (no
-    # collective touches the data path); each rank builds only its own systems.
-    sizes = workloads.batched_sizes(args.systems * ws, seed=0)
-    mine = ranks.shard(sizes, ws)[rank]
-    mix = workloads.batched_mix(args.systems * ws, seed=0, indices=mine)
-    n_tot = sum(len(m.state) for m in mix)
-    k63 = args.morton63
-    b = gb.Batch(device=local, morton63=k63)
-    for m in mix:
-        b.add(m.state, m.g, m.eps, m.theta, m.dt)
-    b.step(args.warmup)
-    tune = b.autotune(repeats=2)  # persistent walk launch for this batch (untimed)
-    b.step(1)  # re-capture the step graph outside the timed region
     clocks = ClockSampler(local)
     clocks.start()
-    gb.device_synchronize(local)
-    ranks.barrier(dist, local)
-    ms = []
-    for _ in range(args.steps):
-        b.step(1)
-        ms.append(b.stats()["ms_last_step"])
-    gb.device_synchronize(local)
-    ranks.barrier(dist, local)
+    mix = measure_mix(args, dist, rank, ws, local, steps=args.steps, warmup=args.warmup)
     clk = clocks.stop()
-    t = ranks.max_over_ranks(dist, sum(ms) / 1e3, local)
-    n_all = ranks.sum_over_ranks(dist, n_tot, local)  # particles on all ranks
-    value = n_all * args.steps / t
-    del b
-    # plain path: the same systems, each stepped alone by the single-system handle
-    hs = []
-    for m in mix:
-        r = gb.GpuResidentLeapfrog(m.g, m.eps, m.theta, device=local, morton63=k63)
-        r.upload(m.state)
-        r.step_many(m.dt, 1)
-        if gb.tuning_lookup(len(m.state), morton63=k63, device=local) is None:
-            r.autotune(repeats=2)  # the plain path is tuned per N bucket too
-        r.step_many(m.dt, 2)  # capture the handle's step graph before timing (as the batch's)
-        hs.append((r, m))
-    k_plain = max(1, min(args.steps, 3))
-    t_plain = 0.0
-    for _ in range(k_plain):
-        for r, m in hs:
-            t_plain += r.step_many_timed(m.dt, 1) / 1e3
-    t_plain = ranks.max_over_ranks(dist, t_plain, local)
-    plain = n_all * k_plain / t_plain
-    del hs
+    del gb
     if rank == 0:
-        line = {"metric": "particle-steps/s at theta=0.5, batched uneven systems", "value": value,
+        line = {"metric": "particle-steps/s at theta=0.5, batched uneven systems", "value": mix["value"],
                 "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
+                "ms_per_step": mix["step_ms_p50"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"batched-{args.systems}-systems", "particles_per_gpu": n_all / ws,
-                           "morton_bits": 63 if k63 else 30,
-                           "systems": args.systems, "n_range": [4096, 262144], "theta": 0.5, "eps": 0.01,
-                           "dt": [1e-3, 5e-4], "cuda_graph": True,
-                           "parallelism": f"{args.systems * ws} systems sharded by particle count over {ws} ranks" if ws > 1 else "1 GPU"},
-                "step_ms_p50": float(np.percentile(ms, 50)), "step_ms_p99": float(np.percentile(ms, 99)),
-                "plain_path": {"value": plain, "unit": "particle-steps/s", "steps": k_plain,
-                               "how": "same systems, one single-system handle each, stepped one after another "
-                                      "(device time of each step summed)"},
-                "batched_over_plain": value / plain, "gpu_launches": (12 if k63 else 8) * args.steps, "clocks": clk,
-                "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm", "walk_group")}}
+                "config": {k: mix[k] for k in ("workload", "systems", "particles", "morton_bits", "n_range", "theta",
+                                               "eps", "dt")},
+                "step_ms_p50": mix["step_ms_p50"], "step_ms_p99": mix["step_ms_p99"],
+                "plain_path": {"value": mix["plain_value"], "unit": "particle-steps/s", "steps": mix["plain_steps"],
+                               "how": mix["plain_how"]},
+                "batched_over_plain": mix["batched_over_plain"],
+                "gpu_launches": mix["gpu_launches_per_step"] * args.steps, "clocks": clk,
+                "walk_launch": mix["walk_launch"]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -700,8 +792,11 @@ def main():
     ap.add_argument("--systems", type=int, default=256, help="batched: number of systems")
     ap.add_argument("--requests", type=int, default=24, help="serving: requests in the stream")
     ap.add_argument("--horizon", type=float, default=60.0, help="serving: seconds to serve")
-    ap.add_argument("--morton63", action="store_true", help="batched/serving: 63-bit Morton keys")
+    ap.add_argument("--morton30", dest="morton63", action="store_false",
+                    help="batched mix / serving: the reference's 30-bit Morton keys (default 63-bit)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.set_defaults(morton63=True)
+    ap.add_argument("--no-batched", action="store_true", help="default workload: skip the batched-mix measurement")
     ap.add_argument("--fp64-steps", type=int, default=100, help="precision: horizon of the FP64 run")
     ap.add_argument("--snapshot-every", type=int, default=0, help="serving: emit GLXYSNAP v4 files every K steps")
     args = ap.parse_args()

@@ -15,7 +15,9 @@
 // The array's name is only a host-side stand-in in host code, never a device address:
 // the first call on each device, with that device current, looks the real address up
 // with cudaGetSymbolAddress and caches it; that first call should therefore come
-// before any stream capture. All calls share the one array, which keeps the last
+// before any stream capture. The cached address belongs to the device's primary
+// context: after cudaDeviceReset (which also invalidates every other handle of this
+// library on that device) the process must not call gx_sort_noalloc again. All calls share the one array, which keeps the last
 // call's contents: each call clears what must start at zero (histograms, look-back
 // status, tile counters, error word) on its stream before sorting. Calls that overlap
 // on the GPU (two host threads, or two streams, sorting at once on one device) race

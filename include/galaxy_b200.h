@@ -332,9 +332,10 @@ int gx_stage_build(gx_handle* h, size_t n, const uint32_t* sorted_codes, const d
  * n may not exceed GX_NOALLOC_MAX_KEYS (GX_ERR_CAPACITY otherwise). Enqueued on
  * `stream` (a cudaStream_t; NULL = default stream) and waited for before returning.
  * Calls no cudaMalloc/cudaFree. The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream capture.
- * All calls share the array: calls overlapping on one GPU race and must be
- * serialised by the caller. Errors: gx_last_error(NULL). */
+ * device address (cudaGetSymbolAddress) and should come before any stream capture;
+ * that address is kept for the life of the device's primary context (no calls after a
+ * cudaDeviceReset). All calls share the array: calls overlapping on one GPU race and
+ * must be serialised by the caller. Errors: gx_last_error(NULL). */
 #define GX_NOALLOC_MAX_KEYS (1u << 20)
 int gx_sort_noalloc(const uint32_t* d_codes, uint32_t* d_sorted_codes, uint32_t* d_order, size_t n, void* stream);
 

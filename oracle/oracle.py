@@ -299,9 +299,47 @@ class LeapfrogKdkLbvh:
         if self.acc is None or self.acc.shape[0] != n:
             self.acc = np.zeros((n, 3))
             self.primed = C.c_int(0)
+        if steps == 0:
+            return
         lib().or_kdk_lbvh(n, pos.reshape(-1), vel.reshape(-1), np.ascontiguousarray(mass, np.float64),
                           self.acc.reshape(-1), C.byref(self.primed), self.g, self.softening, self.theta, dt, steps,
                           self.threads)
+
+    def prime(self, pos, mass):
+        """The integrator's first force evaluation (what its first step does before kicking)."""
+        n = pos.shape[0]
+        if self.acc is None or self.acc.shape[0] != n:
+            self.acc = np.zeros((n, 3))
+        if not self.primed.value:
+            self.acc[:] = lbvh_accelerations(pos, mass, self.g, self.softening, self.theta, threads=self.threads)
+            self.primed = C.c_int(1)
+
+
+# ---- workloads -----------------------------------------------------------------------
+# The seeded workload generator (galaxy_b200/csrc/gx_ic.cpp) is compiled into this
+# library too, so the CPU baseline builds the benchmark's inputs without loading the
+# product library. The two copies are the same source: identical inputs.
+def _ic(name, n, *args):
+    pos, vel, mass = np.empty((n, 3)), np.empty((n, 3)), np.empty(n)
+    fn = getattr(lib(), name)
+    fn.restype = C.c_int
+    rc = fn(C.c_size_t(n), *args, pos.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p),
+            mass.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise ValueError(f"{name} failed ({rc})")
+    return pos, vel, mass
+
+
+def ic_plummer(n: int, seed: int = 0, g: float = 1.0, total_mass: float = 1.0, scale_radius: float = 1.0):
+    """(pos, vel, mass) of Plummer::sample (ic/src/plummer.rs:94-175)."""
+    return _ic("gx_ic_plummer", n, C.c_uint64(seed), C.c_double(g), C.c_double(total_mass), C.c_double(scale_radius))
+
+
+def ic_collision(n_total: int, seed: int = 0, mass_ratio: float = 1.0, pericentre: float = 4.0,
+                 incl1_deg: float = 30.0, incl2_deg: float = 60.0):
+    """(pos, vel, mass) of the two-galaxy collision workload."""
+    return _ic("gx_ic_collision", n_total, C.c_uint64(seed), C.c_double(mass_ratio), C.c_double(pericentre),
+               C.c_double(incl1_deg), C.c_double(incl2_deg))
 
 
 # ---- reference test fixtures ---------------------------------------------------------

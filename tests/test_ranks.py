@@ -64,12 +64,16 @@ def test_two_gloo_ranks_partition_and_reduce():
 
 
 def test_bench_reference_arm_two_ranks():
-    """Under torchrun rank 0 alone times the CPU reference and prints one line; the
-    other rank exits 0 without work."""
-    res = _torchrun(2, "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0")
+    """Under torchrun rank 0 alone times the CPU reference (whole KDK steps of the
+    oracle, inputs from the oracle's copy of the generator) and prints one line; the
+    other rank exits 0 without work. The product library is never loaded."""
+    res = _torchrun(2, "bench.py", "--impl", "reference", "--gpus", "2", "--steps", "2", "--warmup", "1",
+                    "--config", "plummer")
     assert res.returncode == 0, res.stderr[-2000:]
     lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1, res.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["value"] == d["value"]
     assert d["cpu_baseline"]["kind"] == "port" and np.isfinite(d["ms_per_step"])
+    assert d["steps"] == 2 and d["warmup"] == 1 and d["config"]["particles"] == 16_384
+    assert d["native_libraries"] == ["oracle/liblbvh_oracle.so"]

@@ -6,8 +6,9 @@ buffers for the input codes and the outputs; the entry point keeps its working
 memory in a static device array of the library. This test hands it device buffers
 (allocated here by torch, as such a caller's pool would) and checks two calls in a
 row -- of different sizes, so stale scratch from the first would show in the
-second -- against the existing allocating entry point gx_stage_sort, bit for bit
-(the sort is integer work). It runs last so that a failure here leaves every other
+second -- against the existing allocating entry point gx_stage_sort and against the
+oracle's restatement of the reference's stable sort, bit for bit (the sort is integer
+work). It runs last so that a failure here leaves every other
 test already run, and it passes alone in a fresh process as well."""
 
 import ctypes
@@ -45,6 +46,10 @@ def test_noalloc_sort_matches_allocating_sort_on_two_calls():
         ref_order, ref_sorted = gb.stage_sort(codes)
         assert np.array_equal(order, ref_order)
         assert np.array_equal(sorted_codes, ref_sorted)
+        # and the reference's own stable sort by (code, index) (solvers/src/lbvh.rs:143-147)
+        oracle_order = oracle.reference_sort(codes)
+        assert np.array_equal(order, oracle_order)
+        assert np.array_equal(sorted_codes, codes[oracle_order])
 
 
 def test_noalloc_sort_rejects_oversize():
