@@ -174,11 +174,12 @@ def cpu_sample_step(pos, mass, params, threads: int, n_targets: int, rng) -> flo
     return t_build + max(t_walk, 0.0) * n / n_targets
 
 
-def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict) -> dict:
+def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict, radix_bits: int = 8) -> dict:
     """Roofline of the dominant kernel (the FP32 walk) and the HBM fractions of the other
     stages: algorithmic flops (or bytes) per launch over the launch's CUDA-event time."""
     quad = p["multipole"] == "quad"
-    sb = roofline.stage_bytes(n, key64=False, quad=quad)
+    sb = roofline.stage_bytes(n, key64=False, quad=quad, radix_bits=radix_bits)
+    passes = roofline.sort_passes(False, radix_bits)
     flops = roofline.walk_flops(counts["leaf"], counts["far"], counts["open"], quad=quad)
     walk_s = stage["ms_walk"] / 1e3
     mhz = peaks.get("sm_max_mhz", 1965.0)
@@ -207,8 +208,8 @@ def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict) -> di
             "flops_per_launch": flops, "ms_per_launch": stage["ms_walk"], "issue": issue,
             "interactions_per_particle": (counts["leaf"] + counts["far"]) / n,
             "hbm_stages": {
-                "sort (4 onesweep passes)": {"achieved_gbs": sort_gbs, "frac": sort_gbs / hbm, "ms": stage["ms_sort"],
-                                             "bytes": sb["sort"]},
+                f"sort ({passes} onesweep passes, {radix_bits}-bit digits)": {
+                    "achieved_gbs": sort_gbs, "frac": sort_gbs / hbm, "ms": stage["ms_sort"], "bytes": sb["sort"]},
                 "build + aggregation": {"achieved_gbs": build_gbs, "frac": build_gbs / hbm, "ms": stage["ms_build"],
                                         "bytes": sb["build"]},
                 "kick/drift/bbox + Morton": {"achieved_gbs": mort_gbs, "frac": mort_gbs / hbm,
@@ -440,7 +441,7 @@ def run_ours(args):
     del counts_h
     counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"],
               "pair_records": c["warp_node_visits"], "f64_rechecks": c["f64_rechecks"]}
-    roof = walk_roofline(p, n, stage, counts, peaks)
+    roof = walk_roofline(p, n, stage, counts, peaks, tune["radix_bits"])
 
     # --- the batched mix (BASELINE metric: batched vs plain, p50/p99), default workload ---
     mix = None
@@ -467,9 +468,11 @@ def run_ours(args):
                 "implementation": {"precision": "FP32 walk (Kahan), FP64 pos/vel and opening re-checks",
                                    "parallelism": "replicas" if ws > 1 else "single system", "cuda_graph": True,
                                    "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm",
-                                                                        "walk_group")}},
+                                                                        "walk_group")},
+                                   "sort": {"radix_bits": tune["radix_bits"], "sort_ms": tune["sort_ms"]}},
                 "step_ms_p50": float(np.percentile(lat, 50)), "step_ms_p99": float(np.percentile(lat, 99)),
-                "e2e": e2e, "gpu_launches": 8 * args.steps, "roofline": roof, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": (4 + roofline.sort_passes(False, tune["radix_bits"])) * args.steps,
+                "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "walk_counts": counts}
         if mix is not None:
             line["batched_over_plain"] = mix["batched_over_plain"]

@@ -120,7 +120,8 @@ class ForceSolver:
 
 
 def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: int, walk_block: int,
-             stage_times: bool = False, walk_ctas_per_sm: int = 0, morton63: bool = False, walk_group: int = 0):
+             stage_times: bool = False, walk_ctas_per_sm: int = 0, morton63: bool = False, walk_group: int = 0,
+             radix_bits: int = 0):
     o = _lib.Options()
     o.struct_size = C.sizeof(_lib.Options)
     o.precision = {"f32": GX_PREC_F32, "f64": GX_PREC_F64}[precision]
@@ -131,16 +132,17 @@ def _options(precision: str, multipole: str, kahan: bool, stats: bool, device: i
     o.walk_block = walk_block
     o.walk_ctas_per_sm = walk_ctas_per_sm
     o.walk_group = walk_group
+    o.radix_bits = radix_bits
     return o
 
 
 class _Handle:
     def __init__(self, g, softening, theta, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
-                 walk_block=0, stage_times=False, walk_ctas_per_sm=0, morton63=False, walk_group=0):
+                 walk_block=0, stage_times=False, walk_ctas_per_sm=0, morton63=False, walk_group=0, radix_bits=0):
         self.g, self.softening, self.theta = float(g), float(softening), float(theta)
         self._h = C.c_void_p()
         o = _options(precision, multipole, kahan, stats, device, walk_block, stage_times, walk_ctas_per_sm, morton63,
-                     walk_group)
+                     walk_group, radix_bits)
         rc = lib().gx_create(self.g, self.softening, self.theta, C.byref(o), C.byref(self._h))
         if rc != 0:
             check(rc, None)
@@ -635,10 +637,10 @@ class Batch:
     """Many independent systems, one launch per stage (see include/galaxy_b200.h)."""
 
     def __init__(self, budget_bytes: int = 0, precision="f32", multipole="mono", kahan=True, stats=False, device=-1,
-                 walk_block=0, walk_ctas_per_sm=0, morton63=False, walk_group=0):
+                 walk_block=0, walk_ctas_per_sm=0, morton63=False, walk_group=0, radix_bits=0):
         self._b = C.c_void_p()
         o = _options(precision, multipole, kahan, stats, device, walk_block, False, walk_ctas_per_sm, morton63,
-                     walk_group)
+                     walk_group, radix_bits)
         rc = lib().gx_batch_create(int(budget_bytes), C.byref(o), C.byref(self._b))
         if rc != 0:
             check(rc, None)
@@ -842,7 +844,7 @@ def _tune(call, ck) -> dict:
     n = C.c_uint32()
     ck(call(C.byref(best), tried, C.byref(n)))
     row = lambda t: {"walk_block": t.walk_block, "walk_ctas_per_sm": t.walk_ctas_per_sm,  # noqa: E731
-                     "walk_group": t.walk_group, "ms": t.ms}
+                     "walk_group": t.walk_group, "radix_bits": t.radix_bits, "ms": t.ms, "sort_ms": t.sort_ms}
     return {**row(best), "tried": [row(tried[i]) for i in range(n.value)]}
 
 
@@ -856,7 +858,7 @@ def tuning_lookup(n: int, batched: bool = False, precision: str = "f32", multipo
         return None
     check(rc, None)
     return {"walk_block": t.walk_block, "walk_ctas_per_sm": t.walk_ctas_per_sm, "walk_group": t.walk_group,
-            "ms": t.ms}
+            "radix_bits": t.radix_bits, "ms": t.ms, "sort_ms": t.sort_ms}
 
 
 def device_synchronize(device: int = -1) -> None:

@@ -49,6 +49,7 @@ class Options(C.Structure):
         ("walk_block", C.c_uint32),
         ("walk_ctas_per_sm", C.c_uint32),
         ("walk_group", C.c_uint32),
+        ("radix_bits", C.c_uint32),
     ]
 
 
@@ -92,7 +93,9 @@ class Tuning(C.Structure):
         ("walk_block", C.c_uint32),
         ("walk_ctas_per_sm", C.c_uint32),
         ("walk_group", C.c_uint32),
+        ("radix_bits", C.c_uint32),
         ("ms", C.c_float),
+        ("sort_ms", C.c_float),
     ]
 
 

@@ -63,7 +63,8 @@ bool check_device(int device, std::string& err) {
 bool options_valid(const gx_options& o) {
   return o.precision <= GX_PREC_F64 && o.multipole <= GX_MULTIPOLE_QUAD &&
          !(o.walk_block && (o.walk_block % 32 || o.walk_block > static_cast<uint32_t>(kWalkThreads))) &&
-         (o.walk_group == 0 || o.walk_group == 8 || o.walk_group == 16 || o.walk_group == 32);
+         (o.walk_group == 0 || o.walk_group == 8 || o.walk_group == 16 || o.walk_group == 32) &&
+         (o.radix_bits == 0 || o.radix_bits == kRadixBits || o.radix_bits == kRadixBitsWide);
 }
 
 // Once per device, with the device current: kernel attributes the launches rely on.
@@ -112,8 +113,8 @@ size_t Arena::bytes_for(size_t n, size_t nsys, int quad, int f64rec) {
   if (quad) s += 2 * n * 16 + 6 * n * 8;
   if (f64rec) s += n * sizeof(Node64);
   s += tiles * sizeof(TileDesc) + (n / 8 + nsys + 1) * sizeof(WalkItem);
-  s += nsys * (sizeof(SysDesc) + sizeof(Bounds) + 48 + kMaxRadixPasses * kRadixBins * 4);
-  s += kMaxRadixPasses * tiles * kRadixBins * 4 + 64;
+  s += nsys * (sizeof(SysDesc) + sizeof(Bounds) + 48 + kHistWords * 4);
+  s += tiles * kStatusWordsPerTile * 4 + 64;
   s += (n / 256 + 1) * 8 * 8;  // diagnostic partials
   return s + 64 * 256;         // alignment slack
 }
@@ -181,8 +182,8 @@ cudaError_t Arena::ensure(size_t n, size_t tiles, size_t items, size_t nsys, int
   GX_A(b.bounds, ns, Bounds);
   // One zeroed region per step: bbox words, histograms, look-back status, counters.
   const size_t z_bbox = 6 * ns * sizeof(unsigned long long);
-  const size_t z_hist = ns * kMaxRadixPasses * kRadixBins * sizeof(uint32_t);
-  const size_t z_stat = (size_t)kMaxRadixPasses * nt * kRadixBins * sizeof(uint32_t);
+  const size_t z_hist = ns * kHistWords * sizeof(uint32_t);
+  const size_t z_stat = (size_t)nt * kStatusWordsPerTile * sizeof(uint32_t);
   const size_t z_ctr = kCounterWords * sizeof(uint32_t);
   char* z = nullptr;
   GX_A(z, z_bbox + z_hist + z_stat + z_ctr, char);
@@ -272,6 +273,14 @@ void tuned_store(int device, const gx_options& opt, int batched, size_t n, const
 // for large ones.
 uint32_t default_walk_group(size_t n) { return n < (size_t{1} << 16) ? 8u : n < (size_t{1} << 19) ? 16u : 32u; }
 
+uint32_t system_radix_bits(int device, const gx_options& opt, size_t n) {
+  if (opt.flags & GX_FLAG_MORTON63) return kRadixBits;
+  if (opt.radix_bits) return opt.radix_bits;
+  gx_tuning t;
+  if (tuned_lookup(device, opt, 0, n, &t) && t.radix_bits) return t.radix_bits;
+  return kRadixBits;
+}
+
 uint32_t system_walk_group(int device, const gx_options& opt, size_t n) {
   if (opt.precision == GX_PREC_F64) return 32u;  // the FP64 walk takes 32 targets a warp
   if (opt.walk_group) return opt.walk_group;
@@ -288,10 +297,10 @@ std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid, bool
       WalkCfg c = base;
       c.block = block;
       const int full = walk_resident_ctas(c);
-      if (with_grid) out.push_back(gx_tuning{static_cast<uint32_t>(block), 0u, grp, 0.f});
+      if (with_grid) out.push_back(gx_tuning{static_cast<uint32_t>(block), 0u, grp, 0u, 0.f, 0.f});
       if (full / 2 >= 1)
-        out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full / 2), grp, 0.f});
-      out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full), grp, 0.f});
+        out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full / 2), grp, 0u, 0.f, 0.f});
+      out.push_back(gx_tuning{static_cast<uint32_t>(block), static_cast<uint32_t>(full), grp, 0u, 0.f, 0.f});
     }
   }
   if (out.size() > GX_TUNE_MAX_CANDIDATES) out.resize(GX_TUNE_MAX_CANDIDATES);
@@ -384,7 +393,8 @@ WalkCfg walk_cfg(const gx_handle* h) {
 int layout(gx_handle* h, size_t n, double dt) {
   if (n > (1u << 30)) return fail(h, GX_ERR_INVALID_ARG, "N above 2^30 is not supported (30-bit look-back counts)");
   if (n == h->n_layout && dt == h->dt_layout && h->ar.cap_n >= n &&
-      system_walk_group(h->device, h->opt, n) == h->group_layout)
+      system_walk_group(h->device, h->opt, n) == h->group_layout &&
+      static_cast<int>(system_radix_bits(h->device, h->opt, n)) == h->ar.b.radix_bits)
     return GX_OK;
   std::vector<SysDesc> in(1), sys;
   in[0].off = 0;
@@ -405,6 +415,7 @@ int layout(gx_handle* h, size_t n, double dt) {
   StepBufs& b = h->ar.b;
   b.n = static_cast<uint32_t>(n);
   b.key64 = (h->opt.flags & GX_FLAG_MORTON63) ? 1 : 0;
+  b.radix_bits = static_cast<int>(system_radix_bits(h->device, h->opt, n));
   b.nsys = 1;
   b.ntiles = static_cast<uint32_t>(tiles.size());
   b.nitems = static_cast<uint32_t>(items.size());
@@ -1240,8 +1251,46 @@ int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* trie
     return rc;
   }
   *best = cand[best_i];
+  // The sort's digit width (30-bit keys): time the sort stage of force evaluations with
+  // the chosen walk launch, 8-bit then 10-bit digits.
+  best->radix_bits = kRadixBits;
+  if (!(user.flags & GX_FLAG_MORTON63)) {
+    float best_sort = 0.f;
+    for (uint32_t bits : {static_cast<uint32_t>(kRadixBits), static_cast<uint32_t>(kRadixBitsWide)}) {
+      h->opt.walk_block = best->walk_block;
+      h->opt.walk_ctas_per_sm = best->walk_ctas_per_sm;
+      h->opt.walk_group = best->walk_group;
+      h->opt.radix_bits = bits;
+      rc = layout(h, h->n, dt_keep);
+      std::vector<float> ms;
+      for (uint32_t r = 0; r <= reps && rc == GX_OK; ++r) {
+        enqueue_force(h, b, 0, 0, true);
+        rc = finish(h, false);
+        float t = 0.f;
+        if (rc == GX_OK) cudaEventElapsedTime(&t, h->ev[1], h->ev[2]);
+        if (r > 0) ms.push_back(t);  // the first evaluation warms the new layout
+      }
+      if (rc) break;
+      std::sort(ms.begin(), ms.end());
+      const float med = ms[ms.size() / 2];
+      if (bits == kRadixBits || med < best_sort) {
+        best_sort = med;
+        best->radix_bits = bits;
+      }
+    }
+    best->sort_ms = best_sort;
+    h->opt = user;
+    if (h->step_graph) {
+      cudaGraphExecDestroy(h->step_graph);
+      h->step_graph = nullptr;
+    }
+    if (rc) {
+      layout(h, h->n, dt_keep);
+      return rc;
+    }
+  }
   tuned_store(h->device, user, 0, h->n, *best);
-  rc = layout(h, h->n, dt_keep);  // the tuned grouping (unless the options fix one)
+  rc = layout(h, h->n, dt_keep);  // the tuned grouping and digit width (unless the options fix them)
   if (rc) return rc;
   // The resident accelerations are those of the configuration the handle now uses (the
   // grouping sets the FP32 summation order), not of the last candidate timed.

@@ -118,6 +118,9 @@ int upload_tables(gx_batch* bt, const std::vector<size_t>& which, bool* inside) 
   StepBufs& b = bt->ar.b;
   b.n = bt->total;
   b.key64 = (bt->opt.flags & GX_FLAG_MORTON63) ? 1 : 0;
+  // one digit width for the whole batch (the sort is exact: any width gives every system
+  // its own permutation)
+  b.radix_bits = (!b.key64 && bt->opt.radix_bits == kRadixBitsWide) ? kRadixBitsWide : kRadixBits;
   b.nsys = static_cast<uint32_t>(sys.size());
   b.ntiles = static_cast<uint32_t>(tiles.size());
   b.nitems = static_cast<uint32_t>(items.size());

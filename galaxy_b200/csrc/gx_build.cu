@@ -199,8 +199,12 @@ __global__ void __launch_bounds__(kTileThreads) k_build(const TileDesc* __restri
         pp[3] = make_float4(pl.lz, pr.lz, pl.take, pr.take);
         pp[4] = make_float4(pl.open, pr.open, __uint_as_float(child_code(lc, n_total)),
                             __uint_as_float(child_code(rc, n_total)));
-        b.nodeC[gi] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
-        b.nodeD[gi] = make_float4(__double2float_rn(hf[0]), __double2float_rn(hf[1]), __double2float_rn(hf[2]), 0.f);
+        if (theta >= 0.57) {
+          // box centre and half extents: read only by the walk's inside test, which binds
+          // only for theta >= 1/sqrt(3) (the walk applies it from 0.57 on)
+          b.nodeC[gi] = make_float4(__double2float_rn(ctr[0]), __double2float_rn(ctr[1]), __double2float_rn(ctr[2]), 0.f);
+          b.nodeD[gi] = make_float4(__double2float_rn(hf[0]), __double2float_rn(hf[1]), __double2float_rn(hf[2]), 0.f);
+        }
         if (f64rec) {
           Node64 nd;
 #pragma unroll

@@ -84,7 +84,17 @@ constexpr int kRadixBits = 8;
 constexpr int kRadixBins = 1 << kRadixBits;
 constexpr int kRadixPasses = 4;     // 30-bit codes: 8 + 8 + 8 + 6 bits
 constexpr int kRadixPasses63 = 8;   // 63-bit codes: 7 x 8 + 7 bits
-constexpr int kMaxRadixPasses = 8;  // histogram / look-back arrays are sized for this
+constexpr int kMaxRadixPasses = 8;  // tile counters are sized for this
+// The digit width of the 30-bit sort is 8 bits (4 passes) or 10 bits (3 passes): a
+// tuning choice, never a change of result. 63-bit keys use 8-bit digits.
+constexpr int kRadixBitsWide = 10;
+constexpr int kRadixPassesWide = 3;
+// Words of digit histograms per system and of look-back status per tile: the larger of
+// 8 passes x 256 bins and 3 passes x 1024 bins.
+constexpr int kHistWords = 3072;
+constexpr int kStatusWordsPerTile = 3072;
+static_assert(kMaxRadixPasses * kRadixBins <= kHistWords && kRadixPassesWide * (1 << kRadixBitsWide) <= kHistWords,
+              "histogram stride");
 // Slot of the per-step counters that the persistent walk steals items from; slots
 // [0, kMaxRadixPasses) are the sort passes' tile counters.
 constexpr int kWalkItemCounter = kMaxRadixPasses;

@@ -9,6 +9,7 @@ namespace gx {
 struct StepBufs {
   uint32_t n = 0;       // particles over all systems
   int key64 = 0;        // 63-bit Morton keys (codes/keys_alt hold u64) instead of 30-bit
+  int radix_bits = 8;   // digit width of the 30-bit sort: 8 (4 passes) or 10 (3 passes)
   uint32_t nsys = 0;
   uint32_t ntiles = 0;
   uint32_t nitems = 0;  // walk items (32 targets each)
@@ -22,8 +23,8 @@ struct StepBufs {
   const double* mass = nullptr;
   // per-step scratch (zeroed by one memset per step, see zero_begin/zero_bytes)
   unsigned long long* bbox_enc = nullptr;  // 6 per system
-  uint32_t* hist = nullptr;                // nsys * kMaxRadixPasses * 256
-  uint32_t* sort_status = nullptr;         // kMaxRadixPasses * ntiles * 256
+  uint32_t* hist = nullptr;                // nsys * kHistWords: [system][pass][digit]
+  uint32_t* sort_status = nullptr;         // ntiles * kStatusWordsPerTile: [pass][tile][digit]
   uint32_t* counters = nullptr;            // 16 words: [0..7] sort tile counters, [8] walk item counter
   void* zero_begin = nullptr;
   size_t zero_bytes = 0;

@@ -63,6 +63,9 @@ std::vector<gx_tuning> tune_candidates(const WalkCfg& base, bool with_grid, bool
 // single-system tuning table's entry for n, else default_walk_group(n).
 uint32_t system_walk_group(int device, const gx_options& opt, size_t n);
 uint32_t default_walk_group(size_t n);
+// Digit width of the sort of one system of n particles: the option, else the
+// single-system tuning table's entry for n, else 8 (always 8 with 63-bit keys).
+uint32_t system_radix_bits(int device, const gx_options& opt, size_t n);
 bool options_valid(const gx_options& o);
 
 }  // namespace gx

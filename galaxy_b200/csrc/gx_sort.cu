@@ -1,5 +1,6 @@
 // gx_sort.cu -- stable LSD radix sort of (Morton code, original index) pairs,
-// one "onesweep" kernel per 8-bit digit pass, segmented by system.
+// one "onesweep" kernel per digit pass (8-bit digits, or 10-bit ones for 30-bit keys:
+// 3 passes instead of 4), segmented by system.
 //
 // Reference: solvers/src/lbvh.rs:143-147 (`reference_sort`: the permutation that
 // sorts by (code, original index)). A stable LSD sort fed with the identity
@@ -9,8 +10,8 @@
 //   * tiles of a system are chained in index order through decoupled look-back;
 //   * the scatter is staged through shared memory so each digit's run of a tile
 //     is written as one contiguous, coalesced segment.
-// The digit histograms of all four passes come from the Morton kernel (one read
-// of the keys), so each pass reads and writes every (key, index) pair once.
+// The digit histograms of all passes come from the Morton kernel (one read of the
+// keys), so each pass reads and writes every (key, index) pair once.
 // Tiles never straddle systems and each system has its own histograms and
 // look-back chain, so a batch of systems is sorted per system in one launch.
 #include <mutex>
@@ -49,8 +50,9 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *reinterp
 }  // namespace
 
 // One onesweep pass over the tiles of every system, for 30-bit (u32) or 63-bit (u64)
-// keys. Shared memory (dynamic): the tile's keys and indices staged in sorted order.
-template <typename K>
+// keys and 2^BITS-bin digits (thread t owns digits t RPT .. t RPT + RPT - 1). Shared
+// memory (dynamic): the tile's keys and indices staged in sorted order.
+template <typename K, int BITS>
 __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __restrict__ keys_in,
                                                            const uint32_t* __restrict__ vals_in,
                                                            K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
@@ -59,19 +61,22 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __
                                                            const uint32_t* __restrict__ hist,
                                                            uint32_t* __restrict__ status, uint32_t* counters,
                                                            uint32_t ntiles, DevCtl* ctl) {
+  constexpr int BINS = 1 << BITS;
+  constexpr int RPT = BINS / kTileThreads;
+  static_assert(RPT >= 1 && RPT * kTileThreads == BINS, "digits per thread");
   extern __shared__ __align__(16) unsigned char s_dyn[];
   K* s_keys = reinterpret_cast<K*>(s_dyn);
   uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + kTile * sizeof(K));
-  __shared__ uint32_t s_whist[kWarps][kRadixBins];
-  __shared__ uint32_t s_blk_start[kRadixBins];
-  __shared__ uint32_t s_glob[kRadixBins];
+  __shared__ uint32_t s_whist[kWarps][BINS];
+  __shared__ uint32_t s_blk_start[BINS];
+  __shared__ uint32_t s_glob[BINS];
   __shared__ uint32_t s_scan[kWarps];
   __shared__ uint32_t s_tile;
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int shift = pass * kRadixBits;
+  const int shift = pass * BITS;
   if (threadIdx.x == 0) s_tile = atomicAdd(&counters[pass], 1u);
-  for (int i = threadIdx.x; i < kWarps * kRadixBins; i += kTileThreads) (&s_whist[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kWarps * BINS; i += kTileThreads) (&s_whist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   if (tile >= ntiles) {  // counters not re-armed: refuse rather than read past the table
@@ -102,7 +107,7 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __
   const uint32_t lt_mask = (1u << lane) - 1u;
 #pragma unroll
   for (int j = 0; j < kItemsPerThread; ++j) {
-    const uint32_t d = static_cast<uint32_t>(key[j] >> shift) & (kRadixBins - 1);
+    const uint32_t d = static_cast<uint32_t>(key[j] >> shift) & (BINS - 1);
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const uint32_t before = s_whist[warp][d];
     rank[j] = before + __popc(peers & lt_mask);
@@ -112,47 +117,78 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __
   }
   __syncthreads();
 
-  // Thread d owns digit d: per-warp exclusive offsets, tile total, block-local start.
-  const uint32_t d = threadIdx.x;
-  uint32_t total = 0;
+  // Thread t owns digits d = t RPT + r: per-warp exclusive offsets, tile totals, their
+  // block-local starts.
+  uint32_t total[RPT], local_excl[RPT];
+  uint32_t local = 0;
 #pragma unroll
-  for (int w = 0; w < kWarps; ++w) {
-    const uint32_t c = s_whist[w][d];
-    s_whist[w][d] = total;
-    total += c;
+  for (int r = 0; r < RPT; ++r) {
+    const uint32_t d = threadIdx.x * RPT + r;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = s_whist[w][d];
+      s_whist[w][d] = tot;
+      tot += c;
+    }
+    total[r] = tot;
+    local_excl[r] = local;
+    local += tot;
   }
-  const uint32_t blk_start = block_exclusive_scan_256(total, s_scan);
-  s_blk_start[d] = blk_start;
+  const uint32_t blk_base = block_exclusive_scan_256(local, s_scan);
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) s_blk_start[threadIdx.x * RPT + r] = blk_base + local_excl[r];
 
   // Decoupled look-back along this system's tiles (bounded waits).
-  uint32_t* st = status + (size_t)pass * ntiles * kRadixBins;
+  uint32_t* st = status + (size_t)pass * ntiles * BINS;
   const uint32_t tl = tile - sd.first_tile;
-  uint32_t excl = 0;
-  if (tl == 0) {
-    st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagPrefix | (total & kValMask));
-  } else {
-    st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagAgg | (total & kValMask));
-    uint32_t p = tile - 1;
-    for (;;) {
-      uint32_t w = wait_flagged(&st[(size_t)p * kRadixBins + d], kSpinLimit, ctl);
-      if (w == 0u) w = kFlagPrefix;  // timed out (error raised): end the look-back
-      excl += w & kValMask;
-      if ((w & ~kValMask) == kFlagPrefix || p == sd.first_tile) break;
-      --p;
+  uint32_t excl[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const uint32_t d = threadIdx.x * RPT + r;
+    excl[r] = 0;
+    if (tl == 0) {
+      st_volatile(&st[(size_t)tile * BINS + d], kFlagPrefix | (total[r] & kValMask));
+    } else {
+      st_volatile(&st[(size_t)tile * BINS + d], kFlagAgg | (total[r] & kValMask));
     }
-    st_volatile(&st[(size_t)tile * kRadixBins + d], kFlagPrefix | ((excl + total) & kValMask));
+  }
+  if (tl != 0) {
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      const uint32_t d = threadIdx.x * RPT + r;
+      uint32_t p = tile - 1;
+      for (;;) {
+        uint32_t w = wait_flagged(&st[(size_t)p * BINS + d], kSpinLimit, ctl);
+        if (w == 0u) w = kFlagPrefix;  // timed out (error raised): end the look-back
+        excl[r] += w & kValMask;
+        if ((w & ~kValMask) == kFlagPrefix || p == sd.first_tile) break;
+        --p;
+      }
+      st_volatile(&st[(size_t)tile * BINS + d], kFlagPrefix | ((excl[r] + total[r]) & kValMask));
+    }
   }
   // Global start of digit d for this tile: system offset + digits below d in the
   // whole system + the same digit in the system's earlier tiles.
-  const uint32_t* hs = hist + ((size_t)t.sys * kMaxRadixPasses + pass) * kRadixBins;
-  const uint32_t pass_base = block_exclusive_scan_256(hs[d], s_scan);
-  s_glob[d] = sd.off + pass_base + excl - blk_start;
+  const uint32_t* hs = hist + (size_t)t.sys * kHistWords + (size_t)pass * BINS;
+  uint32_t hv[RPT], hloc = 0;
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    hv[r] = hloc;
+    hloc += hs[threadIdx.x * RPT + r];
+  }
+  const uint32_t pass_base = block_exclusive_scan_256(hloc, s_scan);
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const uint32_t d = threadIdx.x * RPT + r;
+    s_glob[d] = sd.off + pass_base + hv[r] + excl[r] - s_blk_start[d];
+  }
   __syncthreads();
 
   // Stage in shared memory at the block-local sorted position.
 #pragma unroll
   for (int j = 0; j < kItemsPerThread; ++j) {
-    const uint32_t dj = static_cast<uint32_t>(key[j] >> shift) & (kRadixBins - 1);
+    const uint32_t dj = static_cast<uint32_t>(key[j] >> shift) & (BINS - 1);
     const uint32_t r = s_blk_start[dj] + s_whist[warp][dj] + rank[j];
     s_keys[r] = key[j];
     s_vals[r] = val[j];
@@ -164,7 +200,7 @@ __global__ void __launch_bounds__(kTileThreads) k_onesweep(int pass, const K* __
   const uint32_t count = t.end - t.begin;
   for (uint32_t i = threadIdx.x; i < count; i += kTileThreads) {
     const K k = s_keys[i];
-    const uint32_t dst = s_glob[static_cast<uint32_t>(k >> shift) & (kRadixBins - 1)] + i;
+    const uint32_t dst = s_glob[static_cast<uint32_t>(k >> shift) & (BINS - 1)] + i;
     keys_out[dst] = k;
     vals_out[dst] = s_vals[i];
   }
@@ -177,12 +213,15 @@ constexpr size_t onesweep_smem() {
   return kTile * (sizeof(K) + sizeof(uint32_t));
 }
 
-// keys_in -> (keys_out, vals_out) over `passes` passes; keys_tmp/vals_tmp take the odd
-// passes' outputs (an even pass count lands in keys_out).
-template <typename K>
-void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K* keys_tmp, uint32_t* vals_tmp,
-                const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist, uint32_t* status,
-                uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
+// keys_in -> (keys_out, vals_out) over `passes` passes of BITS-bit digits; keys_in may
+// be keys_out (it is read by the first pass only), the values start as the identity.
+// No pass writes the buffer it reads: with an even pass count the keys alternate
+// keys_tmp, keys_out, ...; with an odd count they go keys_tmp, keys_tmp2, keys_tmp,
+// ..., keys_out. The values alternate so that the last pass writes vals_out.
+template <typename K, int BITS>
+void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K* keys_tmp, K* keys_tmp2,
+                uint32_t* vals_tmp, const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist,
+                uint32_t* status, uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
   // The dynamic shared-memory opt-in is a per-device function attribute, set once per
   // device (handles on several host threads may reach here together).
   static std::mutex mu;
@@ -192,7 +231,7 @@ void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K
   if (dev >= 0 && dev < 64) {
     std::lock_guard<std::mutex> lk(mu);
     if (!attr_set[dev]) {
-      cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_onesweep<K, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(onesweep_smem<K>()));
       attr_set[dev] = true;
     }
@@ -200,11 +239,16 @@ void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K
   const K* kin = keys_in;
   const uint32_t* vin = nullptr;
   for (int p = 0; p < passes; ++p) {
-    const bool to_tmp = (p % 2) == 0;
-    K* kout = to_tmp ? keys_tmp : keys_out;
-    uint32_t* vout = to_tmp ? vals_tmp : vals_out;
-    k_onesweep<K><<<ntiles, kTileThreads, onesweep_smem<K>(), st>>>(p, kin, vin, kout, vout, tiles, sys, hist,
-                                                                     status, counters, ntiles, ctl);
+    K* kout;
+    if (p == passes - 1)
+      kout = keys_out;
+    else if (passes % 2 == 0)
+      kout = (p % 2 == 0) ? keys_tmp : keys_out;
+    else
+      kout = (p % 2 == 0) ? keys_tmp : keys_tmp2;
+    uint32_t* vout = ((passes - 1 - p) % 2 == 0) ? vals_out : vals_tmp;
+    k_onesweep<K, BITS><<<ntiles, kTileThreads, onesweep_smem<K>(), st>>>(p, kin, vin, kout, vout, tiles, sys, hist,
+                                                                           status, counters, ntiles, ctl);
     kin = kout;
     vin = vout;
   }
@@ -212,7 +256,8 @@ void run_passes(int passes, const K* keys_in, K* keys_out, uint32_t* vals_out, K
 
 }  // namespace
 
-// Digit histograms of all passes from keys already in b.codes (stage entry point).
+// Digit histograms of all passes (8-bit digits) from keys already in b.codes (stage
+// entry point).
 __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __restrict__ tiles,
                                                             const uint32_t* __restrict__ codes,
                                                             uint32_t* __restrict__ hist) {
@@ -226,7 +271,7 @@ __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __re
     for (int p = 0; p < kRadixPasses; ++p) atomicAdd(&sh[p * kRadixBins + ((c >> (p * kRadixBits)) & (kRadixBins - 1))], 1u);
   }
   __syncthreads();
-  uint32_t* hs = hist + (size_t)t.sys * kMaxRadixPasses * kRadixBins;
+  uint32_t* hs = hist + (size_t)t.sys * kHistWords;
   for (int i = threadIdx.x; i < kRadixPasses * kRadixBins; i += kTileThreads)
     if (sh[i]) atomicAdd(&hs[i], sh[i]);
 }
@@ -234,8 +279,8 @@ __global__ void __launch_bounds__(kTileThreads) k_code_hist(const TileDesc* __re
 void launch_sort_passes(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_tmp,
                         uint32_t* vals_tmp, const TileDesc* tiles, const SysDesc* sys, const uint32_t* hist,
                         uint32_t* status, uint32_t* counters, uint32_t ntiles, DevCtl* ctl, cudaStream_t st) {
-  run_passes<uint32_t>(kRadixPasses, keys_in, keys_out, vals_out, keys_tmp, vals_tmp, tiles, sys, hist, status,
-                       counters, ntiles, ctl, st);
+  run_passes<uint32_t, kRadixBits>(kRadixPasses, keys_in, keys_out, vals_out, keys_tmp, nullptr, vals_tmp, tiles, sys,
+                                   hist, status, counters, ntiles, ctl, st);
 }
 
 void launch_code_hist(const StepBufs& b, cudaStream_t st) {
@@ -243,14 +288,20 @@ void launch_code_hist(const StepBufs& b, cudaStream_t st) {
 }
 
 void launch_sort(const StepBufs& b, cudaStream_t st) {
-  // (codes, identity) -> (codes sorted, order) through (keys_alt, vals_alt).
+  // (codes, identity) -> (codes sorted, order) through (keys_alt, vals_alt); the 3-pass
+  // sort also uses the upper half of keys_alt (sized for 64-bit keys).
   if (b.key64)
-    run_passes<uint64_t>(kRadixPasses63, reinterpret_cast<const uint64_t*>(b.codes), reinterpret_cast<uint64_t*>(b.codes),
-                         b.order, reinterpret_cast<uint64_t*>(b.keys_alt), b.vals_alt, b.tiles, b.sys, b.hist,
-                         b.sort_status, b.counters, b.ntiles, b.ctl, st);
+    run_passes<uint64_t, kRadixBits>(kRadixPasses63, reinterpret_cast<const uint64_t*>(b.codes),
+                                     reinterpret_cast<uint64_t*>(b.codes), b.order,
+                                     reinterpret_cast<uint64_t*>(b.keys_alt), nullptr, b.vals_alt, b.tiles, b.sys,
+                                     b.hist, b.sort_status, b.counters, b.ntiles, b.ctl, st);
+  else if (b.radix_bits == kRadixBitsWide)
+    run_passes<uint32_t, kRadixBitsWide>(kRadixPassesWide, b.codes, b.codes, b.order, b.keys_alt, b.keys_alt + b.n,
+                                         b.vals_alt, b.tiles, b.sys, b.hist, b.sort_status, b.counters, b.ntiles,
+                                         b.ctl, st);
   else
-    run_passes<uint32_t>(kRadixPasses, b.codes, b.codes, b.order, b.keys_alt, b.vals_alt, b.tiles, b.sys, b.hist,
-                         b.sort_status, b.counters, b.ntiles, b.ctl, st);
+    run_passes<uint32_t, kRadixBits>(kRadixPasses, b.codes, b.codes, b.order, b.keys_alt, nullptr, b.vals_alt,
+                                     b.tiles, b.sys, b.hist, b.sort_status, b.counters, b.ntiles, b.ctl, st);
 }
 
 }  // namespace gx

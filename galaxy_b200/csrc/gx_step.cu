@@ -123,7 +123,7 @@ __device__ __forceinline__ void make_bounds(const unsigned long long* e, Bounds&
 // the tile's contribution to the per-system digit histograms of all radix passes
 // (4 for 30-bit keys, 8 for 63-bit). The tile's system cube is rebuilt from the
 // reduced lo/hi by every CTA (a few flops), and the system's first tile publishes it.
-template <bool K64>
+template <bool K64, int BITS>
 __global__ void __launch_bounds__(kTileThreads) k_morton_hist(const TileDesc* __restrict__ tiles,
                                                               const double* __restrict__ pos,
                                                               const unsigned long long* __restrict__ enc,
@@ -131,11 +131,12 @@ __global__ void __launch_bounds__(kTileThreads) k_morton_hist(const TileDesc* __
                                                               Bounds* __restrict__ bounds, uint32_t* __restrict__ codes,
                                                               uint32_t* __restrict__ lanes_out,
                                                               uint32_t* __restrict__ hist) {
-  constexpr int P = K64 ? kRadixPasses63 : kRadixPasses;
-  __shared__ uint32_t sh[P][kRadixBins];
+  constexpr int BINS = 1 << BITS;
+  constexpr int P = K64 ? (63 + BITS - 1) / BITS : (30 + BITS - 1) / BITS;
+  __shared__ uint32_t sh[P][BINS];
   __shared__ Bounds sb;
   const TileDesc t = tiles[blockIdx.x];
-  for (int i = threadIdx.x; i < P * kRadixBins; i += kTileThreads) (&sh[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < P * BINS; i += kTileThreads) (&sh[0][0])[i] = 0;
   if (threadIdx.x == 0) {
     make_bounds(enc + 6 * (size_t)t.sys, sb);
     if (sys[t.sys].first_tile == blockIdx.x) bounds[t.sys] = sb;
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(kTileThreads) k_morton_hist(const TileDesc* __
       const uint64_t code = morton3_63(quantize_lane21(vx), quantize_lane21(vy), quantize_lane21(vz));
       reinterpret_cast<uint64_t*>(codes)[i] = code;
 #pragma unroll
-      for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(code >> (p * kRadixBits)) & (kRadixBins - 1)], 1u);
+      for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(code >> (p * BITS)) & (BINS - 1)], 1u);
     } else {
       const uint32_t lx = quantize_lane(vx), ly = quantize_lane(vy), lz = quantize_lane(vz);
       const uint32_t code = morton3(lx, ly, lz);
@@ -162,12 +163,12 @@ __global__ void __launch_bounds__(kTileThreads) k_morton_hist(const TileDesc* __
         lanes_out[3 * (size_t)i + 2] = lz;
       }
 #pragma unroll
-      for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(code >> (p * kRadixBits)) & (kRadixBins - 1)], 1u);
+      for (int p = 0; p < P; ++p) atomicAdd(&sh[p][(code >> (p * BITS)) & (BINS - 1)], 1u);
     }
   }
   __syncthreads();
-  uint32_t* hs = hist + (size_t)t.sys * kMaxRadixPasses * kRadixBins;
-  for (int i = threadIdx.x; i < P * kRadixBins; i += kTileThreads) {
+  uint32_t* hs = hist + (size_t)t.sys * kHistWords;
+  for (int i = threadIdx.x; i < P * BINS; i += kTileThreads) {
     const uint32_t c = (&sh[0][0])[i];
     if (c) atomicAdd(&hs[i], c);
   }
@@ -184,11 +185,14 @@ void launch_kick_half(const StepBufs& b, cudaStream_t st) {
 
 void launch_morton_hist(const StepBufs& b, uint32_t* lanes_out, cudaStream_t st) {
   if (b.key64)
-    k_morton_hist<true><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds, b.codes,
-                                                            nullptr, b.hist);
+    k_morton_hist<true, kRadixBits><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds,
+                                                                        b.codes, nullptr, b.hist);
+  else if (b.radix_bits == kRadixBitsWide)
+    k_morton_hist<false, kRadixBitsWide><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys,
+                                                                             b.bounds, b.codes, lanes_out, b.hist);
   else
-    k_morton_hist<false><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds, b.codes,
-                                                             lanes_out, b.hist);
+    k_morton_hist<false, kRadixBits><<<b.ntiles, kTileThreads, 0, st>>>(b.tiles, b.pos, b.bbox_enc, b.sys, b.bounds,
+                                                                         b.codes, lanes_out, b.hist);
 }
 
 }  // namespace gx

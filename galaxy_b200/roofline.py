@@ -4,8 +4,8 @@ stage's roofline fraction is (these bytes / its measured time) / the measured HB
 the walk's is its algorithmic FP32 flops over the FP32 rate (it is issue-bound, see
 ``issue_fraction``).
 
-N particles, N - 1 internal nodes per system; P radix passes (4 with 30-bit keys, 8 with
-63-bit keys); K key bytes (4 or 8).
+N particles, N - 1 internal nodes per system; P radix passes (4 with 30-bit keys and
+8-bit digits, 3 with 10-bit digits, 8 with 63-bit keys); K key bytes (4 or 8).
 """
 
 from __future__ import annotations
@@ -13,25 +13,31 @@ from __future__ import annotations
 # Bytes per particle of each stage.
 KICK_DRIFT_BBOX = 120  # pos, vel, acc read (72) + pos, vel written (48)
 MORTON = 24            # pos read; + K for the code written (see stage_bytes)
-BUILD = 368            # codes + order (8) and the gathered pos/mass (32) read; leaf64 (32),
-#                        kids (8), parent (8), agg64 (80), pair record (80), box centre and
-#                        half extents (32) and the rendezvous slot (8) written; the sibling's
-#                        aggregate read at each fold (80)
+BUILD = 336            # codes + order (8) and the gathered pos/mass (32) read; leaf64 (32),
+#                        kids (8), parent (8), agg64 (80), pair record (80) and the
+#                        rendezvous slot (8) written; the sibling's aggregate read at each
+#                        fold (80)
+BUILD_INSIDE = 32      # theta >= 1/sqrt(3): box centre and half extents (FP32) per internal node
 BUILD_QUAD = 80        # quadrupole: q64 (48) + FP32 copy (32) per internal node
 WALK = 140             # pair record per internal node (80), target leaf (32) and order (4)
 #                        read, acceleration (24) written; each record read once
 
 
-def stage_bytes(n: int, key64: bool = False, quad: bool = False) -> dict:
-    """Algorithmic bytes of each stage of one step for n particles."""
+def sort_passes(key64: bool = False, radix_bits: int = 8) -> int:
+    """Radix passes of the sort: ceil(key bits / digit bits)."""
+    return -(-(63 if key64 else 30) // (8 if key64 else radix_bits))
+
+
+def stage_bytes(n: int, key64: bool = False, quad: bool = False, radix_bits: int = 8, inside: bool = False) -> dict:
+    """Algorithmic bytes of each stage of one step for n particles (inside: theta >= 1/sqrt 3)."""
     kb = 8 if key64 else 4
-    passes = 8 if key64 else 4
+    passes = sort_passes(key64, radix_bits)
     return {
         "kick_drift_bbox": KICK_DRIFT_BBOX * n,
         "morton": (MORTON + kb) * n,
         "sort_pass": 2 * (kb + 4) * n,  # (key, index) read and written once
         "sort": passes * 2 * (kb + 4) * n,
-        "build": (BUILD + (BUILD_QUAD if quad else 0)) * n,
+        "build": (BUILD + (BUILD_QUAD if quad else 0) + (BUILD_INSIDE if inside else 0)) * n,
         "walk": WALK * n,
     }
 

@@ -25,6 +25,7 @@ pub struct GxOptions {
     pub walk_block: u32,
     pub walk_ctas_per_sm: u32,
     pub walk_group: u32,
+    pub radix_bits: u32,
 }
 
 #[repr(C)]

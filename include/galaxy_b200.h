@@ -67,6 +67,9 @@ typedef struct gx_options {
                               table's entry for the system's N, else a rule of N. It changes
                               the order in which the walk sums its terms (never which terms),
                               so FP32 results can differ in their last bits between groups */
+  uint32_t radix_bits;     /* digit width of the radix sort of 30-bit keys: 8 (4 passes) or 10
+                              (3 passes); 0 = the tuning table's entry, else 8. The sort is
+                              exact: the width never changes a result. 63-bit keys use 8 */
 } gx_options;
 
 typedef struct gx_handle gx_handle;
@@ -268,23 +271,27 @@ int gx_sph_hydro(gx_handle* h, size_t n, const double* pos, const double* vel, c
 int gx_sph_cfl(gx_handle* h, size_t n, const double* pos, const double* vel, const double* hsml, const double* u,
                double c_cfl, double* dt_out, double* min_out);
 
-/* ---- autotuning of the walk launch (no counterpart in the reference) -------------
+/* ---- autotuning of the walk launch and the sort (no counterpart in the reference) --
  * The walk's block size, its scheduling (one warp per item over a grid, or a persistent
  * kernel with CTAs per SM stealing items) and, for a single system, its warp grouping
  * (targets per warp) are picked per N bucket (floor(log2 N)) by timing candidates on a
- * resident state: force evaluations only, so the resident state is untouched. Block size
- * and scheduling never change a result; the grouping changes the FP32 walk's summation
- * order only. The winner is recorded in a process-wide table keyed by (device, precision,
- * multipole, Morton key width, single system or batch, N bucket); handles and batches
- * created with walk_block == 0 and walk_ctas_per_sm == 0 use the table's entry for
- * their N, and every system (alone or in a batch) created with walk_group == 0 takes the
- * single-system entry's grouping for its own N, so a system's result in a batch equals
- * its result alone. */
+ * resident state: force evaluations only, so the resident state is untouched. For 30-bit
+ * keys the radix sort's digit width (8 bits, 4 passes; 10 bits, 3 passes) is then picked
+ * by timing the sort stage of each. Block size, scheduling and digit width never change a
+ * result; the grouping changes the FP32 walk's summation order only. The winner is
+ * recorded in a process-wide table keyed by (device, precision, multipole, Morton key
+ * width, single system or batch, N bucket); handles and batches created with
+ * walk_block == 0 and walk_ctas_per_sm == 0 use the table's entry for their N, and every
+ * system (alone or in a batch) created with walk_group == 0 takes the single-system
+ * entry's grouping for its own N, so a system's result in a batch equals its result
+ * alone. */
 typedef struct gx_tuning {
   uint32_t walk_block;       /* threads per block of the walk */
   uint32_t walk_ctas_per_sm; /* 0 = grid of one warp per item; > 0 persistent CTAs per SM */
   uint32_t walk_group;       /* targets per warp (single-system entries; 0 in batch entries) */
+  uint32_t radix_bits;       /* digit width of the sort (8 or 10; 8 with 63-bit keys) */
   float ms;                  /* median device time of one force evaluation with it */
+  float sort_ms;             /* median device time of the sort stage with radix_bits */
 } gx_tuning;
 #define GX_TUNE_MAX_CANDIDATES 24
 /* Time every candidate `repeats` times (median) on the handle's resident state; best

@@ -14,6 +14,9 @@ def test_stage_bytes_scale_and_key_width():
     assert roofline.stage_bytes(2 * n)["build"] == 2 * b30["build"]
     assert roofline.stage_bytes(n, quad=True)["build"] - b30["build"] == 80 * n
     assert b30["walk"] == 140 * n
+    assert roofline.sort_passes() == 4 and roofline.sort_passes(radix_bits=10) == 3
+    assert roofline.sort_passes(key64=True) == 8 and roofline.sort_passes(key64=True, radix_bits=10) == 8
+    assert roofline.stage_bytes(n, radix_bits=10)["sort"] == 3 * 16 * n
 
 
 def test_walk_flops_and_fractions():
