@@ -318,6 +318,27 @@ class GpuGravitySph(GpuLbvh):
                                                    _ptr(acc)))
         return acc
 
+    def accel_and_dudt_active(self, state, active, acc=None, dudt=None):
+        """GravitySph::accel_and_dudt_active (gravity_sph.rs:288-319): (acc, dudt) of the
+        active path; dudt zero except on the refreshed gas rows."""
+        n = len(state)
+        acc = np.empty((n, 3)) if acc is None else acc
+        dudt = np.empty(n) if dudt is None else dudt
+        act = np.ascontiguousarray(active, dtype=np.uint32)
+        self._ck(lib().gx_sph_accel_and_dudt_active(self._h, n, _ptr(state.pos), _ptr(state.vel), _ptr(state.mass),
+                                                    _ptr(state.kind), _ptr(state.u), act.shape[0], _ptr(act),
+                                                    _ptr(acc), _ptr(dudt)))
+        return acc, dudt
+
+    def rebuild_gravity_cache(self, state) -> None:
+        """GravitySph::rebuild_gravity_cache (gravity_sph.rs:321-327) delegates to its
+        gravity solver, Lbvh, which caches nothing."""
+
+    def gravity_active_cached(self, state, active, acc=None, mass=None):
+        """GravitySph::gravity_active_cached (gravity_sph.rs:329-341): the gravity-ONLY walk
+        (no hydro), Lbvh's default -- a fresh pass, here for the active targets."""
+        return GpuLbvh.accelerations_active(self, state, active, acc, mass)
+
     def sf_fields(self, state):
         """GravitySph::sf_fields (gravity_sph.rs:353-382): state-indexed (rho, div_v) from a
         cold-start density solve; zero on collisionless rows."""

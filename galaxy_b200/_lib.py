@@ -226,6 +226,7 @@ SIGNATURES = {
     "gx_sph_accelerations": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gx_sph_accel_and_dudt": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gx_sph_accelerations_active": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp]),
+    "gx_sph_accel_and_dudt_active": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp]),
     "gx_sph_sf_fields": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gx_sph_max_stable_dt": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _d, _vp, C.POINTER(_d)]),
     "gx_sph_coupled_pairs": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _sz, C.POINTER(_sz)]),

@@ -1506,6 +1506,42 @@ int host_sph_setup(gx_handle* h, size_t n, const double* pos, const double* vel,
   return GX_OK;
 }
 
+// max_stable_dt, sf_fields and coupled_pairs are &self in the reference
+// (solvers/src/sph/gravity_sph.rs:351-382): they leave the warm-start smoothing lengths
+// and the individual-timestep path's scratch as they were. Each runs its own cold-start
+// density solve over the device h; the keeper saves h (host copy) before it and puts it
+// back after, with the hint and scratch flags, so the next force call warm-starts and the
+// active path reads its stale neighbours as if no diagnostic had run.
+struct SphScratchKeeper {
+  gx_handle* h;
+  size_t ng, hint, rho_ngas;
+  uint64_t rho_gen, gen;
+  std::vector<double> hs;
+  SphScratchKeeper(gx_handle* h_, size_t ng_)
+      : h(h_), ng(ng_), hint(h_->sph_host_hint_ngas), rho_ngas(h_->sph_rho_scratch_ngas), rho_gen(h_->sph_rho_gen),
+        gen(h_->sph.alloc_gen) {}
+  int save() {
+    if (ng && hint == ng && h->sph.hs && h->sph.cap >= ng) {
+      hs.resize(ng);
+      GX_CK(h, cudaMemcpyAsync(hs.data(), h->sph.hs, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      GX_CK(h, cudaStreamSynchronize(h->stream));
+    }
+    h->sph_host_hint_ngas = 0;  // until restored: a failed diagnostic leaves no stale hint
+    return GX_OK;
+  }
+  int restore() {
+    const bool same = h->sph.alloc_gen == gen && h->sph.n_gas == ng;
+    if (same && !hs.empty()) {
+      GX_CK(h, cudaMemcpyAsync(h->sph.hs, hs.data(), ng * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      GX_CK(h, cudaStreamSynchronize(h->stream));
+      h->sph_host_hint_ngas = hint;
+    }
+    h->sph_rho_scratch_ngas = same ? rho_ngas : 0;
+    h->sph_rho_gen = rho_gen;
+    return GX_OK;
+  }
+};
+
 int put_gas(gx_handle* h, double* dst, const double* src, size_t count) {
   if (src) GX_CK(h, cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   return GX_OK;
@@ -1662,6 +1698,12 @@ int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const doubl
 int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                                 const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
                                 double* acc_out) {
+  return gx_sph_accel_and_dudt_active(h, n, pos, vel, mass, kind, u, n_active, active, acc_out, nullptr);
+}
+
+int gx_sph_accel_and_dudt_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                                 const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
+                                 double* acc_out, double* dudt_out) {
   if (!h) return GX_ERR_INVALID_ARG;
   if (int rc = need_sph(h)) return rc;
   if (n == 0) return GX_OK;
@@ -1680,7 +1722,9 @@ int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const
   const uint64_t gen0 = h->sph.alloc_gen;
   h->sph_host_hint_ngas = 0;
   h->sph_rho_scratch_ngas = 0;
-  rc = host_sph_setup(h, n, pos, vel, mass, &gas, h_set0 && h->sph.p.warm_start, true);
+  // density_adaptive_active always warm-starts from the persistent h (gravity_sph.rs:
+  // 247-286), whatever warm_start says
+  rc = host_sph_setup(h, n, pos, vel, mass, &gas, h_set0, true);
   if (rc) return rc;
   const bool same_alloc = h->sph.alloc_gen == gen0;  // a reallocation loses both scratches
   const bool h_set = h_set0 && same_alloc;
@@ -1716,17 +1760,32 @@ int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const
                                cudaMemcpyHostToDevice, h->stream));
     if (all || !local.empty())
       sph_enqueue_force(h->sph, b.pos, b.vel, b.mass, b.acc, true, true, b.ctl, h->stream, nullptr,
-                        all ? nullptr : h->sph.targets, static_cast<uint32_t>(local.size()));
+                        all ? nullptr : h->sph.targets, static_cast<uint32_t>(local.size()), true);
     GX_CK(h, cudaMemcpyAsync(h->sph.rho_act, h->sph.rho, ng * sizeof(double), cudaMemcpyDeviceToDevice,
                              h->stream));
   }
   GX_CK(h, cudaMemcpyAsync(acc_out, b.acc, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> gdudt;
+  if (dudt_out && ng && (all || !local.empty())) {
+    gdudt.resize(ng);  // per gas-local index; rows of the refreshed targets are current
+    GX_CK(h, cudaMemcpyAsync(gdudt.data(), h->sph.dudt, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
   h->stats.n = n;
   rc = finish(h, stats_on(h));  // also keeps `local` alive until its copy has run
   if (rc != GX_OK) return rc;
   h->sph_host_hint_ngas = ng;
   h->sph_rho_scratch_ngas = ng;
   h->sph_rho_gen = h->sph.alloc_gen;
+  if (dudt_out) {
+    // gravity_sph.rs:288-319: zero on every row, the refreshed gas rows overwritten
+    std::fill(dudt_out, dudt_out + n, 0.0);
+    if (!gdudt.empty()) {
+      if (all)
+        for (size_t k = 0; k < ng; ++k) dudt_out[gas[k]] = gdudt[k];
+      else
+        for (uint32_t k : local) dudt_out[gas[k]] = gdudt[k];
+    }
+  }
   return GX_OK;
 }
 
@@ -1743,7 +1802,8 @@ int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* ve
   std::fill(div_out, div_out + n, 0.0);
   if (gas.empty()) return GX_OK;
   cudaSetDevice(h->device);
-  h->sph_host_hint_ngas = 0;
+  SphScratchKeeper keep(h, gas.size());
+  if ((rc = keep.save())) return rc;
   rc = host_sph_setup(h, n, pos, vel, mass, &gas, false, true);  // a cold-start solve
   if (rc) return rc;
   const StepBufs& b = h->ar.b;
@@ -1755,6 +1815,7 @@ int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* ve
   GX_CK(h, cudaMemcpyAsync(dv.data(), h->sph.dudt, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   rc = finish(h, false);
   if (rc) return rc;
+  if ((rc = keep.restore())) return rc;
   for (size_t k = 0; k < ng; ++k) {
     rho_out[gas[k]] = rho[k];
     div_out[gas[k]] = dv[k];
@@ -1775,7 +1836,8 @@ int gx_sph_max_stable_dt(gx_handle* h, size_t n, const double* pos, const double
   int rc = gas_map(h, n, kind, gas);
   if (rc || gas.empty()) return rc;
   cudaSetDevice(h->device);
-  h->sph_host_hint_ngas = 0;
+  SphScratchKeeper keep(h, gas.size());
+  if ((rc = keep.save())) return rc;
   rc = host_sph_setup(h, n, pos, vel, mass, &gas, false, true);  // cfl.rs:66: a cold-start solve
   if (rc) return rc;
   const size_t ng = gas.size();
@@ -1793,6 +1855,7 @@ int gx_sph_max_stable_dt(gx_handle* h, size_t n, const double* pos, const double
   GX_CK(h, cudaMemcpyAsync(dt.data(), h->sph.dtv, ng * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   rc = finish(h, false);
   if (rc) return rc;
+  if ((rc = keep.restore())) return rc;
   if (dt_out)
     for (size_t k = 0; k < ng; ++k) dt_out[gas[k]] = dt[k];
   if (min_out) *min_out = -dec_max_host(enc);
@@ -1810,7 +1873,8 @@ int gx_sph_coupled_pairs(gx_handle* h, size_t n, const double* pos, const double
   int rc = gas_map(h, n, kind, gas);
   if (rc || gas.empty()) return rc;
   cudaSetDevice(h->device);
-  h->sph_host_hint_ngas = 0;
+  SphScratchKeeper keep(h, gas.size());
+  if ((rc = keep.save())) return rc;
   rc = host_sph_setup(h, n, pos, nullptr, mass, &gas, false, true);
   if (rc) return rc;
   const StepBufs& b = h->ar.b;
@@ -1849,6 +1913,7 @@ int gx_sph_coupled_pairs(gx_handle* h, size_t n, const double* pos, const double
   rc = e == cudaSuccess ? finish(h, false) : fail(h, GX_ERR_CUDA, std::string("coupled pairs: ") + cudaGetErrorString(e));
   release();
   if (rc) return rc;
+  if ((rc = keep.restore())) return rc;
   // ascending (a, b): a runs in order, each run's b's sorted (cfl.rs:216-225)
   size_t w = 0;
   for (size_t a = 0; a < ng; ++a) {

@@ -1001,7 +1001,7 @@ void sph_free(SphState& s) {
 
 void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const double* mass, double* acc,
                        bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density,
-                       const uint32_t* targets, uint32_t n_targets) {
+                       const uint32_t* targets, uint32_t n_targets, bool always_warm) {
   const uint32_t n = static_cast<uint32_t>(s.n_gas);
   if (n == 0) return;
   SphScalars* sc = s.sc;
@@ -1024,7 +1024,7 @@ void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const 
     da.hs = s.hs;
     da.n_ngb = s.p.n_ngb;
     da.tol = s.p.h_tol_rel;
-    da.warm = s.p.warm_start;
+    da.warm = (s.p.warm_start || always_warm) ? 1 : 0;
     da.ctl = ctl;
     da.targets = targets;
     da.n_targets = n_targets;

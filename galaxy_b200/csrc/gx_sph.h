@@ -91,9 +91,12 @@ void sph_free(SphState& s);
 // targets (device, gas-local, n_targets of them; nullptr: every gas particle) restricts
 // the density and hydro passes and the scatter to those particles; the grids, seeds and
 // h_max cover all gas, the others' rho / h are read as they are (the active path).
+// always_warm: the density brackets start from the kept h whenever it is valid, whatever
+// warm_start says (the individual-timestep path: density_adaptive_active always
+// warm-starts from its persistent h).
 void sph_enqueue_force(SphState& s, const double* pos, const double* vel, const double* mass, double* acc,
                        bool density, bool hydro, DevCtl* ctl, cudaStream_t st, cudaEvent_t after_density = nullptr,
-                       const uint32_t* targets = nullptr, uint32_t n_targets = 0);
+                       const uint32_t* targets = nullptr, uint32_t n_targets = 0, bool always_warm = false);
 // The CFL bound per gas particle (dtv) and its minimum (sc->min_dt_enc) at the current
 // velocities, on the hydro grid of the last force evaluation. With rebuild, the gas is
 // gathered and the hydro grid rebuilt from hs first (the caller supplied h).

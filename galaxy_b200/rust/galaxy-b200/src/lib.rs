@@ -76,6 +76,9 @@ extern "C" {
     fn gx_sph_accelerations_active(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64,
                                    mass: *const f64, kind: *const u8, u: *const f64, n_active: usize,
                                    active: *const u32, acc: *mut f64) -> c_int;
+    fn gx_sph_accel_and_dudt_active(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64,
+                                    mass: *const f64, kind: *const u8, u: *const f64, n_active: usize,
+                                    active: *const u32, acc: *mut f64, dudt: *mut f64) -> c_int;
     fn gx_sph_sf_fields(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
                         kind: *const u8, rho: *mut f64, div: *mut f64) -> c_int;
     fn gx_sph_accel_and_dudt(h: *mut GxHandle, n: usize, pos: *const f64, vel: *const f64, mass: *const f64,
@@ -327,6 +330,35 @@ impl ForceSolver for GpuGravitySphB200 {
             gx_sph_accelerations_active(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
                                         state.kind.as_ptr() as *const u8, state.u.as_ptr(), idx.len(), idx.as_ptr(),
                                         acc.as_mut_ptr() as *mut f64)
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    fn accel_and_dudt_active(&mut self, state: &State, active: &[usize], acc: &mut [DVec3], dudt: &mut [f64]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        assert_eq!(dudt.len(), n, "dudt length must match particle count");
+        let idx: Vec<u32> = active.iter().map(|&i| i as u32).collect();
+        let rc = unsafe {
+            gx_sph_accel_and_dudt_active(self.h, n, as_f64(&state.pos), as_f64(&state.vel), state.mass.as_ptr(),
+                                         state.kind.as_ptr() as *const u8, state.u.as_ptr(), idx.len(),
+                                         idx.as_ptr(), acc.as_mut_ptr() as *mut f64, dudt.as_mut_ptr())
+        };
+        assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
+    }
+
+    // GravitySph delegates the cache to its gravity solver; Lbvh caches nothing.
+    fn rebuild_gravity_cache(&mut self, _state: &State) {}
+
+    // The gravity-ONLY active walk (gravity_sph.rs:329-341): Lbvh's default, a fresh pass,
+    // with no hydro added (the driver's |a_grav| for the combined rung dt).
+    fn gravity_active_cached(&mut self, state: &State, active: &[usize], acc: &mut [DVec3]) {
+        let n = state.len();
+        assert_eq!(acc.len(), n, "acc length must match particle count");
+        let idx: Vec<u32> = active.iter().map(|&i| u32::try_from(i).expect("active index fits u32")).collect();
+        let rc = unsafe {
+            gx_accelerations_active(self.h, n, as_f64(&state.pos), state.mass.as_ptr(), idx.len(), idx.as_ptr(),
+                                    acc.as_mut_ptr() as *mut f64)
         };
         assert!(rc == 0, "libgalaxy_b200: {:?}", err(self.h, rc));
     }

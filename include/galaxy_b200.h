@@ -243,7 +243,15 @@ int gx_sph_accel_and_dudt(gx_handle* h, size_t n, const double* pos, const doubl
 int gx_sph_accelerations_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
                                 const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
                                 double* acc_out);
-/* GravitySph::sf_fields (gravity_sph.rs:353-382): rho_out[n] and div_out[n] (velocity
+/* GravitySph::accel_and_dudt_active (gravity_sph.rs:288-319; core/src/traits.rs:63-71):
+ * gx_sph_accelerations_active plus dudt_out[n]: zero on every row, then the du/dt of the
+ * refreshed gas rows (the active gas, or all gas when the scratch was refreshed). */
+int gx_sph_accel_and_dudt_active(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,
+                                 const uint8_t* kind, const double* u, size_t n_active, const uint32_t* active,
+                                 double* acc_out, double* dudt_out);
+/* The three diagnostics below are &self in the reference: each runs its own cold-start
+ * density solve but leaves the warm-start h and the active path's scratch as they were.
+ * GravitySph::sf_fields (gravity_sph.rs:353-382): rho_out[n] and div_out[n] (velocity
  * divergence, divergence.rs:34-72) of the gas rows from a cold-start density solve;
  * collisionless rows 0. */
 int gx_sph_sf_fields(gx_handle* h, size_t n, const double* pos, const double* vel, const double* mass,

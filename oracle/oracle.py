@@ -89,7 +89,7 @@ def lib():
                                        C.c_void_p, C.c_void_p, C.c_void_p, _f64p, C.POINTER(C.c_int), d, u64, i]),
             "or_gravity_sph_accelerations_active": (i, [sz, _f64p, _f64p, _f64p, _u8p, _f64p, d, d, d, i, d, d, d,
                                                         d, d, d, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                                        sz, _u32p, _f64p, i]),
+                                                        sz, _u32p, _f64p, C.c_void_p, i]),
             "or_sph_velocity_divergence": (None, [sz, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, i]),
             "or_sph_sf_fields": (None, [sz, _f64p, _f64p, _f64p, _u8p, d, d, _f64p, _f64p, i]),
             "or_sph_coupled_pairs": (sz, [sz, _f64p, _f64p, _u8p, d, d, _u64p, sz, i]),
@@ -594,6 +594,11 @@ class GravitySph:
     def accelerations_active(self, pos, vel, mass, kind, active, u=None) -> np.ndarray:
         """GravitySph::accelerations_active (gravity_sph.rs:247-286): fresh gravity on all,
         hydro on the active gas targets from the persistent (rho, h) scratch."""
+        return self.accel_and_dudt_active(pos, vel, mass, kind, active, u)[0]
+
+    def accel_and_dudt_active(self, pos, vel, mass, kind, active, u=None):
+        """GravitySph::accel_and_dudt_active (gravity_sph.rs:288-319): (acc, dudt), du/dt
+        set on the active gas rows (all gas when the scratch was refreshed), zero elsewhere."""
         pos, vel = _pos(pos), _pos(vel)
         n = pos.shape[0]
         kind = np.ascontiguousarray(kind, np.uint8)
@@ -603,14 +608,15 @@ class GravitySph:
             self.rho_scratch = np.zeros(max(ng, 1))
             self.rho_valid = C.c_int(0)
         acc = np.zeros((n, 3))
+        dudt = np.zeros(n)
         uu = np.zeros(n) if u is None else np.ascontiguousarray(u, dtype=np.float64)
         act = np.ascontiguousarray(active, dtype=np.uint32)
         lib().or_gravity_sph_accelerations_active(n, pos.reshape(-1), vel.reshape(-1),
                                                   np.ascontiguousarray(mass, np.float64), kind, uu, *self._args(),
                                                   self.h_hint.ctypes.data, C.addressof(self.h_valid),
                                                   self.rho_scratch.ctypes.data, C.addressof(self.rho_valid),
-                                                  act.shape[0], act, acc.reshape(-1), self.threads)
-        return acc
+                                                  act.shape[0], act, acc.reshape(-1), dudt.ctypes.data, self.threads)
+        return acc, dudt
 
     def step_many(self, pos, vel, mass, kind, dt, steps, u=None):
         """LeapfrogKdk (integrator.rs:38-78) driving this composite, in place."""

@@ -610,8 +610,12 @@ int or_gravity_sph_accelerations_active(size_t n, const double* pos, const doubl
                                         double theta, int eos, double eos_param, double alpha, double beta,
                                         double visc_eps2, double n_ngb, double h_tol_rel, double* h_scratch,
                                         int* h_valid, double* rho_scratch, int* rho_valid, size_t n_active,
-                                        const uint32_t* active, double* acc_out, int threads) {
+                                        const uint32_t* active, double* acc_out, double* dudt_out, int threads) {
   if (n == 0) return 0;
+  // accel_and_dudt_active (gravity_sph.rs:288-319): du/dt zero on every row, the active
+  // gas rows overwritten below
+  if (dudt_out)
+    for (size_t i = 0; i < n; ++i) dudt_out[i] = 0.0;
   if (g > 0.0)
     or_lbvh_accelerations(n, pos, mass, g, softening, theta, acc_out, threads, nullptr);
   else
@@ -667,16 +671,15 @@ int or_gravity_sph_accelerations_active(size_t n, const double* pos, const doubl
   H.visc_eps2 = visc_eps2;
   H.setup();
   std::vector<D3> ca(local.size());
+  std::vector<double> cd(local.size());
 #pragma omp parallel for num_threads(threads > 1 ? threads : 1) schedule(dynamic, 64)
-  for (size_t t = 0; t < local.size(); ++t) {
-    double d;
-    H.force_one(local[t], &ca[t], &d);
-  }
+  for (size_t t = 0; t < local.size(); ++t) H.force_one(local[t], &ca[t], &cd[t]);
   for (size_t t = 0; t < local.size(); ++t) {
     const size_t i = gas[local[t]];
     acc_out[3 * i] = acc_out[3 * i] + ca[t].x;
     acc_out[3 * i + 1] = acc_out[3 * i + 1] + ca[t].y;
     acc_out[3 * i + 2] = acc_out[3 * i + 2] + ca[t].z;
+    if (dudt_out) dudt_out[i] = cd[t];
   }
   *h_valid = 1;
   *rho_valid = 1;

@@ -366,3 +366,70 @@ def test_max_stable_dt_per_particle_matches_oracle(oracle):
     m, ref = oracle.sph_max_stable_dt(st.pos, st.vel, st.mass, st.kind, 0.25, per_particle=True)
     assert np.all(np.isinf(dt[st.kind == 0]))
     assert np.array_equal(dt, ref) and s.max_stable_dt(st, 0.25) == m
+
+
+def test_diagnostics_leave_warm_start_and_active_scratch(oracle):
+    # max_stable_dt (+ per particle), sf_fields and coupled_pairs are &self in the
+    # reference (gravity_sph.rs:351-382) and are called between force evaluations by its
+    # block-timestep driver (sim/src/lib.rs): they must leave the warm-start h and the
+    # active path's (rho, h) scratch as they were. A handle that runs them between
+    # accelerations_active calls equals one that does not, bit for bit, and both follow
+    # the oracle's GravitySph over the same sequence.
+    st = mix_state(oracle, 0xBEE, 1500, 3000)
+    quiet = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    busy = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    og = oracle.GravitySph(1.0, 0.05, 0.5)
+    every = np.arange(len(st), dtype=np.uint32)
+    assert np.array_equal(quiet.accelerations_active(st, every), busy.accelerations_active(st, every))
+    og.accelerations_active(st.pos, st.vel, st.mass, st.kind, every)
+    rng = np.random.default_rng(6)
+    for _ in range(3):
+        st.pos += 1e-3 * st.vel
+        busy.max_stable_dt_per_particle(st, 0.25)
+        busy.coupled_pairs(st)
+        busy.sf_fields(st)
+        busy.max_stable_dt(st, 0.25)
+        act = np.sort(rng.choice(len(st), len(st) // 3, replace=False)).astype(np.uint32)
+        a = quiet.accelerations_active(st, act)
+        assert np.array_equal(busy.accelerations_active(st, act), a)
+        r = og.accelerations_active(st.pos, st.vel, st.mass, st.kind, act)
+        err = np.linalg.norm(a - r, axis=1) / np.linalg.norm(r, axis=1)
+        assert (err > 1e-10).sum() <= 1 and err.max() < 1e-2
+    # the full composite's warm start survives them too
+    busy.max_stable_dt(st, 0.25)
+    assert np.array_equal(busy.accelerations(st), quiet.accelerations(st))
+
+
+def test_accel_and_dudt_active_and_gravity_only_walk(oracle):
+    # gravity_sph.rs:288-319 (accel_and_dudt_active) and :329-341 (gravity_active_cached:
+    # gravity only, Lbvh's fresh pass) against the oracle's GravitySph over one sequence.
+    st = mix_state(oracle, 0xD00D, 1500, 3000)
+    s = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    twin = gb.GpuGravitySph(1.0, 0.05, 0.5, precision="f64")
+    og = oracle.GravitySph(1.0, 0.05, 0.5)
+    rng = np.random.default_rng(8)
+    gas = st.gas()
+    for step in range(3):
+        if step:
+            st.pos += 1e-3 * st.vel
+        act = (np.arange(len(st), dtype=np.uint32) if step == 0 else
+               np.sort(rng.choice(len(st), len(st) // 3, replace=False)).astype(np.uint32))
+        a, d = s.accel_and_dudt_active(st, act)
+        assert np.array_equal(a, twin.accelerations_active(st, act))  # the same path, with du/dt
+        ra, rd = og.accel_and_dudt_active(st.pos, st.vel, st.mass, st.kind, act)
+        err = np.linalg.norm(a - ra, axis=1) / np.linalg.norm(ra, axis=1)
+        assert (err > 1e-10).sum() <= 1 and err.max() < 1e-2
+        refreshed = gas if step == 0 else np.intersect1d(gas, act)
+        assert not d[np.setdiff1d(np.arange(len(st)), refreshed)].any()
+        scale = np.sqrt(np.mean(rd[refreshed] ** 2))
+        assert (np.abs(d[refreshed] - rd[refreshed]) > 1e-10 * scale).sum() <= 1
+    # the gravity-only walk: no hydro on the gas rows, the reference's Lbvh pass
+    s.rebuild_gravity_cache(st)
+    idx = np.arange(0, len(st), 3, dtype=np.uint32)
+    g = s.gravity_active_cached(st, idx)
+    ref = oracle.lbvh_accelerations(st.pos, st.mass, 1.0, 0.05, 0.5)
+    assert np.array_equal(g[idx], ref[idx])
+    # and it left the active path's scratch alone
+    act = np.sort(rng.choice(len(st), len(st) // 3, replace=False)).astype(np.uint32)
+    st.pos += 1e-3 * st.vel
+    assert np.array_equal(s.accelerations_active(st, act), twin.accelerations_active(st, act))
