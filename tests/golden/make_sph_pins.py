@@ -1,5 +1,8 @@
-"""Extract the reference's frozen SPH output bits into sph_pins.json (run in a container
-that has the reference checkout; the JSON is what the tests read).
+"""Extract the reference's frozen SPH output bits into sph_pins.json (run where a checkout
+of the reference project exists; the JSON is what the tests read).
+
+    python tests/golden/make_sph_pins.py <reference checkout>
+    GALAXY_REFERENCE=<reference checkout> python tests/golden/make_sph_pins.py
 
 Sources (the reference project's own regression pins):
   solvers/tests/sph_forces.rs `isothermal_regression_pins_pre_e1b_bits`: 8 accelerations
@@ -15,7 +18,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GALAXY_REFERENCE")
+if not REF:
+    sys.exit("usage: make_sph_pins.py <reference checkout> (or set GALAXY_REFERENCE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
