@@ -351,10 +351,17 @@ def measure_mix(args, dist, rank, ws, local, steps: int, warmup: int) -> dict:
     k_plain = max(1, min(steps, 3))
     t_plain = 0.0
     plain_ms = []
-    for _ in range(k_plain):
+    by_bucket = {}  # floor(log2 N): [systems, particles, device ms per pass]
+    for rep in range(k_plain):
         t_pass = 0.0
         for r, m in hs:
-            t_pass += r.step_many_timed(m.dt, 1)
+            t_sys = r.step_many_timed(m.dt, 1)
+            t_pass += t_sys
+            if rep == k_plain - 1:
+                e = by_bucket.setdefault(int(np.log2(len(m.state))), [0, 0, 0.0])
+                e[0] += 1
+                e[1] += len(m.state)
+                e[2] += t_sys
         plain_ms.append(t_pass)
         t_plain += t_pass / 1e3
     t_plain = ranks.max_over_ranks(dist, t_plain, local)
@@ -369,6 +376,10 @@ def measure_mix(args, dist, rank, ws, local, steps: int, warmup: int) -> dict:
             "plain_how": "same systems, one single-system handle each, stepped one after another (device time of "
                          "each step summed)",
             "batched_over_plain": value / plain, "gpu_launches_per_step": 12 if k63 else 8,
+            "batch_ns_per_particle_step": float(np.percentile(ms, 50)) * 1e6 / max(n_tot, 1),
+            "plain_by_log2_n": {str(k): {"systems": v[0], "particles": v[1], "ms": v[2],
+                                         "ns_per_particle_step": v[2] * 1e6 / v[1]}
+                                for k, v in sorted(by_bucket.items())},
             "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm")}}
 
 
@@ -383,10 +394,12 @@ def run_ours(args):
 
     # --- headline: resident steps, CUDA-graph replay, device time (CUDA events) ---
     mp = p["multipole"]
-    r = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], multipole=mp, device=local)
+    r = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], multipole=mp, device=local, walk_group=args.walk_group)
     r.upload(st)
     r.step_many(dt, args.warmup)
     tune = r.autotune(repeats=3)  # walk launch for this N bucket (outside the timed region)
+    if args.walk_group:
+        tune["walk_group"] = args.walk_group  # fixed by the option (the handle keeps it)
     r.step_many(dt, 1)  # re-capture the step graph outside the timed region
     clocks = ClockSampler(local)
     clocks.start()
@@ -403,7 +416,7 @@ def run_ours(args):
 
     # --- e2e: the reference-facing ForceSolver path (LeapfrogKdk on host arrays) ---
     pinned = gb.PinnedState.from_state(st)
-    h = gb.GpuLbvh(1.0, p["eps"], p["theta"], multipole=mp, device=local)
+    h = gb.GpuLbvh(1.0, p["eps"], p["theta"], multipole=mp, device=local, walk_group=args.walk_group)
     primed = h.kdk_step_host(pinned, dt, primed=False)  # prime + one step (warm-up)
     k_e2e = max(1, min(args.steps, 10))
     reps = []
@@ -424,7 +437,8 @@ def run_ours(args):
     del pinned, h
 
     # --- per-stage device times (eager launches with CUDA events on the handle's stream) ---
-    rs = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], multipole=mp, device=local, stage_times=True)
+    rs = gb.GpuResidentLeapfrog(1.0, p["eps"], p["theta"], multipole=mp, device=local, stage_times=True,
+                                walk_group=args.walk_group)
     rs.upload(st)
     stage = {"ms_bbox_morton": 0.0, "ms_sort": 0.0, "ms_build": 0.0, "ms_walk": 0.0}
     k_st = max(1, min(args.steps, 10))
@@ -505,7 +519,8 @@ def run_batched(args):
                                "how": mix["plain_how"]},
                 "batched_over_plain": mix["batched_over_plain"],
                 "gpu_launches": mix["gpu_launches_per_step"] * args.steps, "clocks": clk,
-                "walk_launch": mix["walk_launch"]}
+                "walk_launch": mix["walk_launch"], "batch_ns_per_particle_step": mix["batch_ns_per_particle_step"],
+                "plain_by_log2_n": mix["plain_by_log2_n"]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -553,6 +568,10 @@ def run_serving(args):
     wall = time.perf_counter() - t0
     st = srv.stats()
     clk = clocks.stop()
+    states = [srv.status(rid)[0] for rid in rids]
+    counts = {name: sum(1 for x in states if x == code) for name, code in
+              (("queued", srv.QUEUED), ("running", srv.RUNNING), ("completed", srv.DONE), ("rejected", srv.REJECTED),
+               ("cancelled", srv.CANCELLED))}
     snaps = sum(srv.snapshots_written(rid) for rid in rids) if args.snapshot_every else 0
     srv.close()
     if snap_dir:
@@ -570,7 +589,10 @@ def run_serving(args):
                 "snapshots_written": snaps,
                 "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],
                 "wall_particle_steps_per_s": st["particle_steps"] / wall, "completed": st["completed"],
-                "submitted": len(rids), "max_live": st["max_live"], "queue_s_p50": st["queue_s_p50"],
+                "submitted": len(rids), "admitted": counts["running"] + counts["completed"],
+                "rejected": counts["rejected"], "still_queued": counts["queued"], "request_states": counts,
+                "demand_particle_steps": int(sum(r.n * r.steps for r in reqs)), "wall_s": wall,
+                "max_live": st["max_live"], "queue_s_p50": st["queue_s_p50"],
                 "queue_s_p99": st["queue_s_p99"], "clocks": clk}
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -800,6 +822,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.set_defaults(morton63=True)
     ap.add_argument("--no-batched", action="store_true", help="default workload: skip the batched-mix measurement")
+    ap.add_argument("--walk-group", type=int, default=0, choices=[0, 8, 16, 32],
+                    help="targets per warp of the walk (0: tuned)")
     ap.add_argument("--fp64-steps", type=int, default=100, help="precision: horizon of the FP64 run")
     ap.add_argument("--snapshot-every", type=int, default=0, help="serving: emit GLXYSNAP v4 files every K steps")
     args = ap.parse_args()
