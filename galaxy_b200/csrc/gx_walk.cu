@@ -281,6 +281,23 @@ __device__ __forceinline__ void inside_test(const StepBufs& b, const float xh[3]
   amb = amb || (t && near_face);
 }
 
+// True when internal node gi's AABB (FP32 centre / half extents, rounded from FP64) and
+// the targets' padded box (negated faces nlo, nhi) are apart along some axis by more than
+// the rounding of the FP32 box, so that no target is inside the node.
+__device__ __forceinline__ bool boxes_apart(const StepBufs& b, uint32_t gi, const float2 nlo[3], const float2 nhi[3]) {
+  const float4 nc = __ldg(&b.nodeC[gi]);
+  const float4 nd = __ldg(&b.nodeD[gi]);
+  const float c[3] = {nc.x, nc.y, nc.z}, h[3] = {nd.x, nd.y, nd.z};
+  bool apart = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float m = 0x1p-20f * (fabsf(c[a]) + h[a]) + 1e-30f;
+    const float lo = -nlo[a].x, hi = -nhi[a].x;
+    apart = apart || lo > c[a] + h[a] + m || hi < c[a] - h[a] - m;
+  }
+  return apart;
+}
+
 // FP64 decision of an undecided child with record code c (a leaf is undecided only
 // when massless: skip).
 __device__ __forceinline__ void resolve(const StepBufs& b, uint32_t k, double theta, uint32_t c, bool& take,
@@ -580,9 +597,10 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         const float2 dmax2 = __ffma2_rn(fx, fx, __ffma2_rn(fy, fy, __fmul2_rn(fz, fz)));
         bool accL = act && dmin2.x * kGroupLo > r3.z, accR = act && dmin2.y * kGroupLo > r3.w;
         if (inside_rule) {
-          // the group test does not cover the inside rule: nodes go to the targets' tests
-          accL = accL && (cL & kLeafCode);
-          accR = accR && (cR & kLeafCode);
+          // A target inside a node's box opens it: a node is taken for the whole warp only
+          // when its box and the targets' box are apart along some axis.
+          if (accL && !(cL & kLeafCode)) accL = boxes_apart(b, cL, nlo, nhi);
+          if (accR && !(cR & kLeafCode)) accR = boxes_apart(b, cR, nlo, nhi);
         }
         const bool opnL = act && !accL && dmax2.x * kGroupHi < r4.x;
         const bool opnR = act && !accR && dmax2.y * kGroupHi < r4.y;
