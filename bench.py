@@ -174,7 +174,8 @@ def cpu_sample_step(pos, mass, params, threads: int, n_targets: int, rng) -> flo
     return t_build + max(t_walk, 0.0) * n / n_targets
 
 
-def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict, radix_bits: int = 8) -> dict:
+def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict, radix_bits: int = 8,
+                  walk_group: int = 32) -> dict:
     """Roofline of the dominant kernel (the FP32 walk) and the HBM fractions of the other
     stages: algorithmic flops (or bytes) per launch over the launch's CUDA-event time."""
     quad = p["multipole"] == "quad"
@@ -190,8 +191,9 @@ def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict, radix
     build_gbs = roofline.hbm_fraction(sb["build"], stage["ms_build"], hbm)[0]
     mort_gbs = roofline.hbm_fraction(sb["kick_drift_bbox"] + sb["morton"], stage["ms_bbox_morton"], hbm)[0]
     prof = f"profiles/k_walk_f32_{p['name'].replace('collision-', 'collision_')}.md"
-    traffic = profiled_walk(p["name"], "traffic_bytes_per_launch")
-    inst = profiled_walk(p["name"], "instructions_per_launch")
+    # the capture of the same warp grouping as this run's walk
+    traffic = profiled_walk(p["name"], f"traffic_bytes_per_launch_g{walk_group}")
+    inst = profiled_walk(p["name"], f"instructions_per_launch_g{walk_group}")
     issue = None
     if inst:
         rate, frac = roofline.issue_fraction(inst, stage["ms_walk"], 148, mhz)
@@ -200,8 +202,8 @@ def walk_roofline(p: dict, n: int, stage: dict, counts: dict, peaks: dict, radix
                            f"instruction per scheduler per clock"}
     return {"kernel": "k_walk_f32 (tree walk)", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, {prof}"
-                              if traffic else None,
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch with {walk_group} "
+                              f"targets a warp, {prof}" if traffic else None, "walk_group": walk_group,
             "algorithmic_bytes_per_launch": sb["walk"],
             "peak_source": "nominal FP32 CUDA-core rate 148 SM x 128 lanes x 2 x clocks.max.sm (MEASURED_PEAKS.json "
                            "has no FP32 figure); no tensor-core work in this path",
@@ -455,7 +457,7 @@ def run_ours(args):
     del counts_h
     counts = {"leaf": c["leaf_interactions"], "far": c["far_interactions"], "open": c["nodes_opened"],
               "pair_records": c["warp_node_visits"], "f64_rechecks": c["f64_rechecks"]}
-    roof = walk_roofline(p, n, stage, counts, peaks, tune["radix_bits"])
+    roof = walk_roofline(p, n, stage, counts, peaks, tune["radix_bits"], tune["walk_group"])
 
     # --- the batched mix (BASELINE metric: batched vs plain, p50/p99), default workload ---
     mix = None
