@@ -109,8 +109,8 @@ void launch_gather_acc(const double* acc, const uint32_t* active, uint32_t n_act
 int walk_resident_ctas(const WalkCfg& cfg);
 // Shared memory of one FP32 walk block of `block` threads (quadrupole mode: more).
 size_t walk_smem_bytes(int block, bool quad);
-// Per-device set-up of the walk kernels (shared-memory carveout); call with the device
-// current, before any stream capture.
+// Per-device set-up of the walk kernels (their dynamic shared-memory limit); call with the
+// device current, before any stream capture.
 void walk_prepare();
 // gx_diag.cu
 void launch_direct_sum_f64(uint32_t n, const double* pos, const double* mass, double g, double eps,

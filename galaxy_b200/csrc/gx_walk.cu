@@ -917,18 +917,17 @@ int resident(K kern, int block, size_t smem) {
   return n > 0 ? n : 1;
 }
 
-// The FP32 walk's blocks take (block / 32) x (sizeof(WarpLists) [+ sizeof(WarpQuads)]) of
-// shared memory: ask for the largest shared-memory carveout, and let quadrupole blocks
-// go past the default 48 KB.
+// Quadrupole blocks take more than the default 48 KB of dynamic shared memory. (No
+// carveout preference is set: the driver sizes the L1 / shared split per launch, which
+// leaves the L1 of the kernels that follow the walk in a step as large as they need.)
 template <class K>
 void smem_attrs(K kern, bool quad) {
-  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(walk_smem_bytes(kWalkThreads, quad)));
 }
 
 template <bool QUAD, bool KAHAN, bool LIST>
-void carveout_f32() {
+void smem_f32() {
   smem_attrs(k_walk_f32<QUAD, KAHAN, false, false, LIST>, QUAD);
   smem_attrs(k_walk_f32<QUAD, KAHAN, false, true, LIST>, QUAD);
   smem_attrs(k_walk_f32<QUAD, KAHAN, true, false, LIST>, QUAD);
@@ -938,14 +937,14 @@ void carveout_f32() {
 }  // namespace
 
 void walk_prepare() {
-  carveout_f32<false, false, false>();
-  carveout_f32<false, true, false>();
-  carveout_f32<true, false, false>();
-  carveout_f32<true, true, false>();
-  carveout_f32<false, false, true>();
-  carveout_f32<false, true, true>();
-  carveout_f32<true, false, true>();
-  carveout_f32<true, true, true>();
+  smem_f32<false, false, false>();
+  smem_f32<false, true, false>();
+  smem_f32<true, false, false>();
+  smem_f32<true, true, false>();
+  smem_f32<false, false, true>();
+  smem_f32<false, true, true>();
+  smem_f32<true, false, true>();
+  smem_f32<true, true, true>();
 }
 
 int walk_resident_ctas(const WalkCfg& cfg) {
