@@ -74,6 +74,7 @@ void prepare_device(int dev) {
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 0 || dev >= 64 || (done >> dev) & 1u) return;
   walk_prepare();
+  build_prepare();
   done |= 1ull << dev;
 }
 

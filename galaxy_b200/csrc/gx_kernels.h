@@ -89,6 +89,9 @@ void launch_sort_passes(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* v
 void launch_code_hist(const StepBufs& b, cudaStream_t st);
 // gx_build.cu: gather leaves + bottom-up Karras build and aggregation
 void launch_build(const StepBufs& b, int quad, int f64_records, cudaStream_t st);
+// Per-device set-up of the build kernels (their dynamic shared-memory limit); call with the
+// device current, before any stream capture.
+void build_prepare();
 // gx_walk.cu: tree walk, acc in original order
 void launch_walk(const StepBufs& b, const WalkCfg& cfg, cudaStream_t st);
 // gx_diag.cu: one bounded wait on a word nothing sets (failure-detection self-test)

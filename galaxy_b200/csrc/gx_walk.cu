@@ -244,23 +244,6 @@ namespace {
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-// FP32 term of one taken internal child's quadrupole (r = x - com = -d):
-// a += Q r / r^5 - 2.5 (r.Q r) r / r^7, with r^2 softened like the monopole.
-__device__ __forceinline__ void quad_term(const float4& qa, const float4& qb, float dx, float dy, float dz, float inv,
-                                          float t[3]) {
-  const float inv2 = inv * inv;
-  const float inv5 = inv2 * inv2 * inv;
-  const float rx = -dx, ry = -dy, rz = -dz;
-  const float qx = qa.x * rx + qa.y * ry + qa.z * rz;
-  const float qy = qa.y * rx + qa.w * ry + qb.x * rz;
-  const float qz = qa.z * rx + qb.x * ry + qb.y * rz;
-  const float rqr = rx * qx + ry * qy + rz * qz;
-  const float c7 = 2.5f * rqr * inv5 * inv2;
-  t[0] += qx * inv5 - rx * c7;
-  t[1] += qy * inv5 - ry * c7;
-  t[2] += qz * inv5 - rz * c7;
-}
-
 // Opening test for theta >= 1/sqrt(3): the target inside the child's AABB must open it.
 // Returns the adjusted (take, open, amb) of a child whose distance test said "take".
 __device__ __forceinline__ void inside_test(const StepBufs& b, const float xh[3], uint32_t gi, bool& take, bool& open,
@@ -380,13 +363,15 @@ struct WarpLists {
 // 2 + 33, and then the depth-first growth adds at most one entry per tree level.
 static_assert(kWalkDeep + 32 + (kWalkList - 1) + 35 + kMaxDepth <= kWalkStack, "walk stack bound");
 
-// Quadrupole mode: each listed internal node's traceless moments (xx, xy, xz, yy), (yz, zz),
-// fetched once by the lane that lists it.
+// Quadrupole mode: each listed internal node's traceless moments, fetched once by the lane
+// that lists it and stored with the two entries of a pair side by side, as the packed
+// evaluation reads them: a = (xx, xx', xy, xy'), b = (xz, xz', yy, yy'), c = (yz, yz', zz, zz').
+// Slots of leaf entries are never written: the evaluation gives them a zero inverse
+// distance, and the arrays are cleared at the kernel's start so that every slot holds
+// finite values.
 struct WarpQuads {
-  float4 dqa[kWalkList];
-  float2 dqb[kWalkList];
-  float4 uqa[kWalkList];
-  float2 uqb[kWalkList];
+  float4 dqa[kWalkList / 2], dqb[kWalkList / 2], dqc[kWalkList / 2];
+  float4 uqa[kWalkList / 2], uqb[kWalkList / 2], uqc[kWalkList / 2];
 };
 
 size_t walk_smem_bytes(int block, bool quad) {
@@ -412,6 +397,40 @@ __device__ __forceinline__ void mono2(float2 dx, float2 dy, float2 dz, float2 m,
   tx = __ffma2_rn(dx, f, tx);
   ty = __ffma2_rn(dy, f, ty);
   tz = __ffma2_rn(dz, f, tz);
+}
+
+// Stores entry e's moments (xx, xy, xz, yy), (yz, zz) into the pair layout of WarpQuads.
+__device__ __forceinline__ void put_quad(float4* qa, float4* qb, float4* qc, int e, const float4& a, const float4& c) {
+  const int p = e >> 1, h = e & 1;
+  float* A = reinterpret_cast<float*>(qa + p) + h;
+  float* B = reinterpret_cast<float*>(qb + p) + h;
+  float* C = reinterpret_cast<float*>(qc + p) + h;
+  A[0] = a.x;
+  A[2] = a.y;
+  B[0] = a.z;
+  B[2] = a.w;
+  C[0] = c.x;
+  C[2] = c.y;
+}
+
+// Quadrupole terms of the two entries of a pair for one target, packed FP32, added to the
+// monopole accumulator: with r = x - com = -d, a += Q r / r^5 - 2.5 (r.Q r) r / r^7
+// = -(Q d) / r^5 + 2.5 (d.Q d) d / r^7, r^2 softened like the monopole. inv is the
+// inverse distance of an entry the target takes as an internal node, else 0.
+__device__ __forceinline__ void quad2(float2 dx, float2 dy, float2 dz, float2 inv, const float4& qa, const float4& qb,
+                                      const float4& qc, float2& tx, float2& ty, float2& tz) {
+  const float2 xx = f2(qa.x, qa.y), xy = f2(qa.z, qa.w), xz = f2(qb.x, qb.y);
+  const float2 yy = f2(qb.z, qb.w), yz = f2(qc.x, qc.y), zz = f2(qc.z, qc.w);
+  const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
+  const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
+  const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
+  const float2 dqd = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
+  const float2 inv2 = __fmul2_rn(inv, inv);
+  const float2 ninv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), f2(-inv.x, -inv.y));      // -1 / r^5
+  const float2 c7 = __fmul2_rn(__fmul2_rn(f2(-2.5f, -2.5f), dqd), __fmul2_rn(ninv5, inv2));  // 2.5 dQd / r^7
+  tx = __ffma2_rn(dx, c7, __ffma2_rn(qx, ninv5, tx));
+  ty = __ffma2_rn(dy, c7, __ffma2_rn(qy, ninv5, ty));
+  tz = __ffma2_rn(dz, c7, __ffma2_rn(qz, ninv5, tz));
 }
 
 }  // namespace
@@ -452,6 +471,11 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
   uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_total = b.n;
   const float4* __restrict__ pairs = b.pairs;
+  if (QUAD) {
+    float4* z = reinterpret_cast<float4*>(&Q);
+    for (int i = lane; i < static_cast<int>(sizeof(WarpQuads) / sizeof(float4)); i += 32) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+  }
   while (item < b.nitems) {
     const WalkItem it = b.items[item];
     const SysDesc sd = b.sys[it.sys];
@@ -622,22 +646,10 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
             qaR = __ldg(&b.nodeQ[2 * (size_t)cR]);
             qbR = __ldg(&b.nodeQ[2 * (size_t)cR + 1]);
           }
-          if (qL && accL) {
-            Q.dqa[eAL] = qaL;
-            Q.dqb[eAL] = make_float2(qbL.x, qbL.y);
-          }
-          if (qL && undL) {
-            Q.uqa[eUL] = qaL;
-            Q.uqb[eUL] = make_float2(qbL.x, qbL.y);
-          }
-          if (qR && accR) {
-            Q.dqa[eAR] = qaR;
-            Q.dqb[eAR] = make_float2(qbR.x, qbR.y);
-          }
-          if (qR && undR) {
-            Q.uqa[eUR] = qaR;
-            Q.uqb[eUR] = make_float2(qbR.x, qbR.y);
-          }
+          if (qL && accL) put_quad(Q.dqa, Q.dqb, Q.dqc, eAL, qaL, qbL);
+          if (qL && undL) put_quad(Q.uqa, Q.uqb, Q.uqc, eUL, qaL, qbL);
+          if (qR && accR) put_quad(Q.dqa, Q.dqb, Q.dqc, eAR, qaR, qbR);
+          if (qR && undR) put_quad(Q.uqa, Q.uqb, Q.uqc, eUR, qaR, qbR);
         }
         if (accL || accR) {
           // dense entries relative to the box centre: (c_hi - o) + c_lo
@@ -679,18 +691,8 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         if (QUAD || STATS) {
           const uint32_t c0 = L.dcode[2 * p], c1 = L.dcode[2 * p + 1];
           if (QUAD) {
-            float tq[3] = {0.f, 0.f, 0.f};
-            if (t0 && !(c0 & kLeafCode)) {
-              const float2 qb = Q.dqb[2 * p];
-              quad_term(Q.dqa[2 * p], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
-            }
-            if (t1 && !(c1 & kLeafCode)) {
-              const float2 qb = Q.dqb[2 * p + 1];
-              quad_term(Q.dqa[2 * p + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
-            }
-            tx.x += tq[0];
-            ty.x += tq[1];
-            tz.x += tq[2];
+            const float2 iq = f2(t0 && !(c0 & kLeafCode) ? i0 : 0.f, t1 && !(c1 & kLeafCode) ? i1 : 0.f);
+            quad2(dx, dy, dz, iq, Q.dqa[p], Q.dqb[p], Q.dqc[p], tx, ty, tz);
           }
           if (STATS) {
             const uint32_t self = kLeafCode | k;
@@ -741,18 +743,8 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         float i0, i1;
         mono2(dx, dy, dz, f2(B.z, B.w), eps2, tL, tR, tx, ty, tz, i0, i1);
         if (QUAD) {
-          float tq[3] = {0.f, 0.f, 0.f};
-          if (tL && !(cL & kLeafCode)) {
-            const float2 qb = Q.uqb[2 * p];
-            quad_term(Q.uqa[2 * p], make_float4(qb.x, qb.y, 0.f, 0.f), dx.x, dy.x, dz.x, i0, tq);
-          }
-          if (tR && !(cR & kLeafCode)) {
-            const float2 qb = Q.uqb[2 * p + 1];
-            quad_term(Q.uqa[2 * p + 1], make_float4(qb.x, qb.y, 0.f, 0.f), dx.y, dy.y, dz.y, i1, tq);
-          }
-          tx.x += tq[0];
-          ty.x += tq[1];
-          tz.x += tq[2];
+          const float2 iq = f2(tL && !(cL & kLeafCode) ? i0 : 0.f, tR && !(cR & kLeafCode) ? i1 : 0.f);
+          quad2(dx, dy, dz, iq, Q.uqa[p], Q.uqb[p], Q.uqc[p], tx, ty, tz);
         }
         if (STATS) {
           const uint32_t self = kLeafCode | k;
