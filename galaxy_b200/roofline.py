@@ -13,10 +13,10 @@ from __future__ import annotations
 # Bytes per particle of each stage.
 KICK_DRIFT_BBOX = 120  # pos, vel, acc read (72) + pos, vel written (48)
 MORTON = 24            # pos read; + K for the code written (see stage_bytes)
-BUILD = 336            # codes + order (8) and the gathered pos/mass (32) read; leaf64 (32),
-#                        kids (8), parent (8), agg64 (80), pair record (80) and the
-#                        rendezvous slot (8) written; the sibling's aggregate read at each
-#                        fold (80)
+BUILD = 256            # codes + order (8) and the gathered pos/mass (32) read; leaf64 (32),
+#                        kids (8), parent links (8), agg64 (80), pair record (80) and the
+#                        exchange word (8) written (siblings' aggregates are read from
+#                        shared memory below each 256-leaf block, from L2 above it)
 BUILD_INSIDE = 32      # theta >= 1/sqrt(3): box centre and half extents (FP32) per internal node
 BUILD_QUAD = 80        # quadrupole: q64 (48) + FP32 copy (32) per internal node
 WALK = 140             # pair record per internal node (80), target leaf (32) and order (4)
