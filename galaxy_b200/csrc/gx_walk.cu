@@ -355,7 +355,13 @@ struct WarpLists {
   uint32_t dcode[kWalkList];                    // child codes (quadrupole terms, statistics)
   float4 ua[kWalkList / 2], ub[kWalkList / 2], uc[kWalkList / 2], ud[kWalkList / 2], ue[kWalkList / 2],
       uf[kWalkList / 2];  // (xh,yh) (zh,m) (xl,yl) (zl,take) (open,code) (mask,opened)
+  // The targets' padded box as negated faces (lo, hi) and its negated centre o, each
+  // duplicated for packed pairs: warp-uniform, read by the rounds only (kept here rather
+  // than in 18 registers of every lane).
+  float2 nlo[3], nhi[3], no[3];
+  float2 pad;
 };
+static_assert(sizeof(WarpLists) % 16 == 0, "warp lists keep 16-byte alignment");
 
 // Bound of the stack: a normal round starts at most kWalkDeep entries high and pushes at
 // most one entry per popped one (2 children each, <= 32 popped), an undecided evaluation
@@ -523,7 +529,6 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
       // target that is not finite turns the box into all of space: no group decisions.
       const bool fin = isfinite(xh[0]) && isfinite(xh[1]) && isfinite(xh[2]);
       const bool all_fin = __all_sync(0xffffffffu, !valid || fin);
-      float2 nlo[3], nhi[3], no[3];
       float xr[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -533,9 +538,11 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         const float pad = (fabsf(l) + fabsf(h)) * 0x1p-21f + 1e-30f;
         l = all_fin ? l - pad : -INFINITY;
         h = all_fin ? h + pad : INFINITY;
-        nlo[c] = f2(-l, -l);
-        nhi[c] = f2(-h, -h);
-        no[c] = f2(-o, -o);
+        if (lane == 0) {
+          L.nlo[c] = f2(-l, -l);
+          L.nhi[c] = f2(-h, -h);
+          L.no[c] = f2(-o, -o);
+        }
         xr[c] = (xh[c] - o) + xl[c];  // the target relative to o
       }
       const float2 nxr = f2(-xr[0], -xr[0]), nyr = f2(-xr[1], -xr[1]), nzr = f2(-xr[2], -xr[2]);
@@ -604,6 +611,7 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
           r4 = __ldg(pr + 4);
         }
         const uint32_t cL = __float_as_uint(r4.z), cR = __float_as_uint(r4.w);
+        const float2 nlo[3] = {L.nlo[0], L.nlo[1], L.nlo[2]}, nhi[3] = {L.nhi[0], L.nhi[1], L.nhi[2]};
         const float2 chx = f2(r0.x, r0.y), chy = f2(r0.z, r0.w), chz = f2(r1.x, r1.y);
         const float2 clx = f2(r2.x, r2.y), cly = f2(r2.z, r2.w), clz = f2(r3.x, r3.y);
         // c - lo and c - hi per axis, both children at once
@@ -653,9 +661,9 @@ __global__ void __launch_bounds__(kWalkThreads, GX_WALK_MINB) k_walk_f32(StepBuf
         }
         if (accL || accR) {
           // dense entries relative to the box centre: (c_hi - o) + c_lo
-          const float2 rx = __fadd2_rn(__fadd2_rn(chx, no[0]), clx);
-          const float2 ry = __fadd2_rn(__fadd2_rn(chy, no[1]), cly);
-          const float2 rz = __fadd2_rn(__fadd2_rn(chz, no[2]), clz);
+          const float2 rx = __fadd2_rn(__fadd2_rn(chx, L.no[0]), clx);
+          const float2 ry = __fadd2_rn(__fadd2_rn(chy, L.no[1]), cly);
+          const float2 rz = __fadd2_rn(__fadd2_rn(chz, L.no[2]), clz);
           if (accL) put_dense(eAL, rx.x, ry.x, rz.x, r1.z, M, cL);
           if (accR) put_dense(eAR, rx.y, ry.y, rz.y, r1.w, M, cR);
         }
