@@ -1212,8 +1212,10 @@ int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* trie
   const gx_options user = h->opt;
   const uint32_t reps = repeats ? repeats : 3;
   WalkCfg base = walk_cfg(h);
-  // the FP64 walk has one grouping
-  std::vector<gx_tuning> cand = tune_candidates(base, true, h->opt.precision != GX_PREC_F64);
+  // the FP64 walk has one grouping; a grouping fixed by the options is the only one tried
+  std::vector<gx_tuning> cand = tune_candidates(base, true, h->opt.precision != GX_PREC_F64 && user.walk_group == 0);
+  if (user.walk_group)
+    for (gx_tuning& c : cand) c.walk_group = user.walk_group;
   StepBufs& b = h->ar.b;
   const double dt_keep = h->dt_layout;
   int best_i = -1;
@@ -1290,7 +1292,11 @@ int gx_autotune(gx_handle* h, uint32_t repeats, gx_tuning* best, gx_tuning* trie
       return rc;
     }
   }
-  tuned_store(h->device, user, 0, h->n, *best);
+  // A grouping fixed by the options was not tuned: the table's entry leaves it open (0),
+  // so handles of this N bucket with the grouping open keep their default one.
+  gx_tuning rec = *best;
+  if (user.walk_group) rec.walk_group = 0;
+  tuned_store(h->device, user, 0, h->n, rec);
   rc = layout(h, h->n, dt_keep);  // the tuned grouping and digit width (unless the options fix them)
   if (rc) return rc;
   // The resident accelerations are those of the configuration the handle now uses (the

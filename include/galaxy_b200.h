@@ -283,7 +283,8 @@ int gx_sph_cfl(gx_handle* h, size_t n, const double* pos, const double* vel, con
  * The walk's block size, its scheduling (one warp per item over a grid, or a persistent
  * kernel with CTAs per SM stealing items) and, for a single system, its warp grouping
  * (targets per warp) are picked per N bucket (floor(log2 N)) by timing candidates on a
- * resident state: force evaluations only, so the resident state is untouched. For 30-bit
+ * resident state: force evaluations only, so the resident state is untouched. A handle
+ * whose options fix walk_group is tuned at that grouping only. For 30-bit
  * keys the radix sort's digit width (8 bits, 4 passes; 10 bits, 3 passes) is then picked
  * by timing the sort stage of each. Block size, scheduling and digit width never change a
  * result; the grouping changes the FP32 walk's summation order only. The winner is

@@ -71,6 +71,19 @@ def test_autotune_keeps_state_and_records_bucket():
     assert np.array_equal(twin.snapshot().pos, explicit.snapshot().pos)
 
 
+def test_autotune_keeps_a_fixed_grouping():
+    st = gb.ic.collision(40_000, 13)
+    r = gb.GpuResidentLeapfrog(1.0, 0.02, 0.5, walk_group=16)
+    r.upload(st)
+    r.step_many(5e-4, 2)
+    best = r.autotune(repeats=1)
+    assert best["walk_group"] == 16
+    assert {t["walk_group"] for t in best["tried"]} == {16}
+    # the table's entry leaves the grouping open for handles that do not fix it
+    rec = gb.tuning_lookup(40_000)
+    assert rec is not None and rec["walk_group"] == 0
+
+
 def test_batch_autotune_keeps_state():
     sts = [gb.ic.plummer(20_000 + 5_000 * i, 90 + i) for i in range(3)]
     b = gb.Batch()
