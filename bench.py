@@ -248,7 +248,9 @@ def run_reference_sph(args, threads: int):
             "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"gas-star-mix-{args.gas}+{args.gas}", "sample_particles": n, "gas": ng,
-                       "eps": 0.01, "theta": 0.5, "dt": 1e-4},
+                       "eps": 0.01, "theta": 0.5, "dt": 1e-4,
+                       "sampled": f"the rate is per particle-step of a {ng}+{ng} sample of the workload "
+                                  f"(the full size does not fit the run's time on the host)"},
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
