@@ -379,7 +379,7 @@ def measure_mix(args, dist, rank, ws, local, steps: int, warmup: int) -> dict:
             "plain_pass_ms_p50": float(np.percentile(plain_ms, 50)),
             "plain_how": "same systems, one single-system handle each, stepped one after another (device time of "
                          "each step summed)",
-            "batched_over_plain": value / plain, "gpu_launches_per_step": 12 if k63 else 8,
+            "batched_over_plain": value / plain, "gpu_launches_per_step": 13 if k63 else 9,
             "batch_ns_per_particle_step": float(np.percentile(ms, 50)) * 1e6 / max(n_tot, 1),
             "plain_by_log2_n": {str(k): {"systems": v[0], "particles": v[1], "ms": v[2],
                                          "ns_per_particle_step": v[2] * 1e6 / v[1]}
@@ -489,7 +489,7 @@ def run_ours(args):
                                                                         "walk_group")},
                                    "sort": {"radix_bits": tune["radix_bits"], "sort_ms": tune["sort_ms"]}},
                 "step_ms_p50": float(np.percentile(lat, 50)), "step_ms_p99": float(np.percentile(lat, 99)),
-                "e2e": e2e, "gpu_launches": (4 + roofline.sort_passes(False, tune["radix_bits"])) * args.steps,
+                "e2e": e2e, "gpu_launches": (5 + roofline.sort_passes(False, tune["radix_bits"])) * args.steps,
                 "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "walk_counts": counts}
         if mix is not None:
@@ -677,7 +677,7 @@ def run_precision(args):
         dist.destroy_process_group()
 
 
-# Kernels a gas-mode step adds to the 8 of the gravity step: gather, scalars, 3 grids
+# Kernels a gas-mode step adds to the 9 of the gravity step: gather, scalars, 3 grids
 # (keys, histogram, 4 sort passes, fill, mixed flags), seeds, density cell, density, h_max,
 # hydro cell, pack, hydro, scatter.
 SPH_LAUNCHES_PER_STEP = 2 + 3 * 8 + 8
@@ -801,7 +801,7 @@ def run_sph(args):
                            "l2": f"working set ~{900 * n / 1e6:.0f} MB > 126 MB L2 (no flush needed)",
                            "walk_launch": {k: tune[k] for k in ("walk_block", "walk_ctas_per_sm", "walk_group")}},
                 "gas_particle_steps_per_s": ng * ws * args.steps / (ms_max / 1e3),
-                "e2e": e2e, "gpu_launches": (8 + SPH_LAUNCHES_PER_STEP) * args.steps, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": (9 + SPH_LAUNCHES_PER_STEP) * args.steps, "cpu_baseline": cpu,
                 "clocks": clk, "stage_ms": stage, "sph_share_of_step": gas_frac, "min_stable_dt_c0.25": cfl,
                 "roofline": sph_roofline(ng, stage, peaks)}
         print(json.dumps(line), flush=True)
