@@ -1,5 +1,6 @@
 // gx_build.cu -- leaf gather + bottom-up Karras radix-tree build + FP64 aggregation
-// in two passes, one thread per leaf, no waiting.
+// in two passes, one thread per leaf; no thread spins on another's progress (pass 1's
+// rounds meet at block barriers).
 //
 // Reference: solvers/src/lbvh.rs:153-306 (delta, karras_node, reference_karras),
 // :329-379 and :623-636 (reference_aggregate, fold_agg), :560-614 (the node
@@ -17,8 +18,8 @@
 // root is internal node 0. The fold is fold_agg's exact f64 sequence in fixed (left,
 // right) order, so every aggregate is bit-identical to reference_aggregate's.
 //
-// Pass 1 (k_build_local) does every split whose parent lies inside one block's 256
-// leaves with shared-memory exchange words and aggregates; pass 2 (k_build_top)
+// Pass 1 (k_build_local) does every split whose parent lies inside one block's
+// kBuildLeaves (256) leaves with shared-memory exchange words and aggregates; pass 2 (k_build_top)
 // continues the few climbs that leave a block through device-scope exchange words. A
 // one-pass climb through global memory spends a device-scope round trip on every level
 // and keeps a block resident until its highest climber reaches the top; here almost all
