@@ -144,6 +144,15 @@ def test_build_topology_degenerate_codes(h, oracle):
         _check_build(h, oracle, codes.astype(np.uint32), pos, np.ones(n))
 
 
+@pytest.mark.parametrize("n", [255, 256, 257, 511, 513, 4095, 4097])
+def test_build_block_and_tile_edges(h, oracle, n):
+    # systems ending just inside, at and just past a 256-leaf block (the per-block pass
+    # and the cross-block climbs) and a 4096-particle tile
+    pos = oracle.fixture_cloud(0x5EED + n, n, 2.0)
+    mass = oracle.fixture_masses(0xD00D + n, n)
+    _check_build(h, oracle, *_sorted_inputs(oracle, pos, mass))
+
+
 def test_build_large(h, oracle):
     pos = oracle.fixture_cloud(0xBEEF, 65_536, 5.0)
     _check_build(h, oracle, *_sorted_inputs(oracle, pos, np.ones(65_536)))
